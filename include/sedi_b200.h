@@ -1,0 +1,150 @@
+/*
+ * sedi_b200 -- B200 (sm_100a) implementation of the SEDI estimator hot path.
+ *
+ * C ABI: plain pointers and sizes, no C++ or torch types.  Every grid is a
+ * dense n1*n2*n3 array of doubles, i1 fastest, then i2, then i3 -- the element
+ * order of the reference's Grid3d::rank_cells (Slice3d.hpp:30-32) without its
+ * ghost layer; the zero ghost layer of the reference (Cg.hpp:57-62) is applied
+ * inside the kernels.
+ *
+ * Reference interfaces replaced (paths relative to the reference checkout):
+ *   sedi_create          <- {Cg,PipelinedCg,BiCgStab}(DomainDecomposition&, long nghost, int mode, Timers*)
+ *                           Cg.hpp:48-68, PipelinedCg.hpp:48-70, BiCgStab.hpp:55-75, plus
+ *                           Stencil(a,b,c) Stencil.hpp:18-19 and the solver typedef chosen by
+ *                           -DSOLVER in stochastic-estimator.cc:134-142
+ *   sedi_solve[_dev]     <- solver_t::solve(Stencil&, CommHalo&, Grid3d& x, Grid3d& b, Grid3d& iM,
+ *                           int maxiter, Dtype tol, Dtype* final_err, int* final_iter)
+ *                           Cg.hpp:70-82, PipelinedCg.hpp:72-84, BiCgStab.hpp:77-89
+ *   sedi_solve_batch     <- the same solve() applied to many right-hand sides at once
+ *   sedi_estimate[_probes] <- the probe loop of main(), stochastic-estimator.cc:155-216
+ *                           (RNG fill :165, x=0 :175, solve :176-179, abort unless -i :181-184,
+ *                            t += x.*v :195, q += v.*v :198, D = t./q :216)
+ *   sedi_fill_probe      <- DistrRngStd::fill_plusminusone, DistrRngStd.hpp:22-42
+ *   sedi_stencil_apply   <- Stencil::apply / DistrAsyncStencil at -p 1x1x1, Stencil.hpp:21-54,
+ *                           DistrAsyncStencil.hpp:52-100
+ *
+ * Return values of the solve/estimate entry points are the reference's
+ * result_t values (0 solution found, 1 reached maxiter, 2 BiCGStab rho
+ * breakdown, 3 BiCGStab omega breakdown; Cg.hpp:31-34, BiCgStab.hpp:32-37)
+ * or a negative SEDI_ERR_* code.  A context is not thread-safe (one host
+ * thread per context), like the reference solver objects that share one
+ * CommHalo (Cg.hpp:95-98).
+ */
+#ifndef SEDI_B200_H
+#define SEDI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Solver ids: the reference's -DSOLVER values (stochastic-estimator.cc:134-142). */
+#define SEDI_BICGSTAB 1
+#define SEDI_CG 2
+#define SEDI_PIPELINED_CG 3
+
+/* Arithmetic forms. */
+#define SEDI_PREC_FP64 0  /* the reference method in FP64, kernel by kernel */
+#define SEDI_PREC_MIXED 1 /* FP32 Krylov vectors, FP64 reductions, FP64 reliable update of x and r */
+
+/* Reference result_t values. */
+#define SEDI_SOLUTION_FOUND 0
+#define SEDI_REACHED_MAXITER 1
+#define SEDI_BREAKDOWN_RHO 2
+#define SEDI_BREAKDOWN_OMEGA 3
+
+/* Errors (negative). */
+#define SEDI_ERR_ARG (-1)     /* invalid argument (sizes, solver id, NULL pointer) */
+#define SEDI_ERR_CUDA (-2)    /* a CUDA call failed; see sedi_ctx_error() */
+#define SEDI_ERR_NOMEM (-3)   /* device allocation failed */
+#define SEDI_ERR_NODEV (-4)   /* no CUDA device / kernels not loadable */
+#define SEDI_ERR_UNSUPPORTED (-5)
+
+/* Mode bits (Cg.hpp:36-40).  At one GPU there is no halo exchange or
+ * allreduce to overlap, so both bits are accepted and have no numerical
+ * effect, exactly as at -p 1x1x1 in the reference. */
+#define SEDI_MODE_SYNC_STENCIL 1
+#define SEDI_MODE_SYNC_DOTPROD 2
+
+typedef struct sedi_ctx sedi_ctx;
+
+/*
+ * Create a solver context on the current CUDA device.
+ *   solver     SEDI_CG / SEDI_PIPELINED_CG / SEDI_BICGSTAB
+ *   n1,n2,n3   grid (every dimension >= 1)
+ *   a,b,c      stencil coefficients: y = a*x_c - c*(x_{i-1}+...) - b*(x_{i+1}+...)
+ *   mode       SEDI_MODE_* bits (accepted, no effect on one GPU)
+ *   precision  SEDI_PREC_FP64 or SEDI_PREC_MIXED
+ *   batch      right-hand sides in flight per launch (1 = single-vector form)
+ *   err        out: 0 or a negative SEDI_ERR_* (may be NULL)
+ * Returns NULL on error.
+ */
+sedi_ctx *sedi_create(int solver, long n1, long n2, long n3, double a, double b, double c, int mode,
+                      int precision, int batch, int *err);
+void sedi_destroy(sedi_ctx *ctx);
+/* Message for the last failure on this context ("" if none). */
+const char *sedi_ctx_error(const sedi_ctx *ctx);
+
+/*
+ * Solve A x = b for one right-hand side (host buffers, n1*n2*n3 doubles).
+ * x: in first guess, out solution.  iM: inverse-diagonal preconditioner as a
+ * vector, or NULL for the constant 1/a the reference uses
+ * (stochastic-estimator.cc:101-103).  final_err, final_iter: as the reference.
+ */
+int sedi_solve(sedi_ctx *ctx, const double *b, double *x, const double *iM, int maxiter, double tol,
+               double *final_err, int *final_iter);
+/* Same with device pointers (already resident in HBM); runs on the context's stream. */
+int sedi_solve_dev(sedi_ctx *ctx, const double *b_dev, double *x_dev, const double *iM_dev, int maxiter,
+                   double tol, double *final_err, int *final_iter);
+
+/*
+ * nrhs right-hand sides (host buffers; right-hand side k at offset k*n).
+ * Per right-hand side: results[k] (result_t), final_err[k], final_iter[k].
+ * Returns the largest result_t seen, or a negative error.
+ */
+int sedi_solve_batch(sedi_ctx *ctx, int nrhs, const double *b, double *x, int maxiter, double tol,
+                     double *final_err, int *final_iter, int *results);
+
+/*
+ * The estimator loop of stochastic-estimator.cc:155-216 on the GPU.
+ * Probe k is DistrRngStd's ±1 vector from std::mt19937(seed + k).
+ *   D           out: t ./ q (n doubles)
+ *   t, q        out, may be NULL: the accumulators
+ *   iters, errs, results   out, may be NULL: per-probe final_iter, final_err, result_t
+ *   ignore_errors  0: stop at the first probe whose result is not 0 and return
+ *                  that result (the reference aborts with 100+code unless -i)
+ * Returns 0, a positive result_t (first failure, when !ignore_errors), or an error.
+ */
+int sedi_estimate(sedi_ctx *ctx, int samples, uint32_t seed, int maxiter, double tol, int ignore_errors,
+                  double *D, double *t, double *q, int *iters, double *errs, int *results);
+/* Same with caller-provided probes: samples*n doubles in host memory. */
+int sedi_estimate_probes(sedi_ctx *ctx, int samples, const double *probes, int maxiter, double tol,
+                         int ignore_errors, double *D, double *t, double *q, int *iters, double *errs,
+                         int *results);
+
+/* Host probe generator, bit-identical to DistrRngStd with std::mt19937(seed). */
+void sedi_fill_probe(uint32_t seed, long n, double *out);
+
+/* y = A x with zero ghosts (host buffers), the kernel the solvers use. */
+int sedi_stencil_apply(sedi_ctx *ctx, const double *x, double *y);
+
+/*
+ * Per-iteration relative residual of the last single-vector solve:
+ * hist[0] is the initial err, hist[i] the err printed by the reference after
+ * iteration i (Cg.hpp:192, PipelinedCg.hpp:228, BiCgStab.hpp:228).
+ * Returns the number of entries written.
+ */
+int sedi_last_history(sedi_ctx *ctx, double *hist, int len);
+
+/* Kernel launches issued by this context since creation (for benchmarks). */
+long long sedi_launch_count(const sedi_ctx *ctx);
+
+/* Library version string. */
+const char *sedi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

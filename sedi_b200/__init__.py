@@ -1,0 +1,286 @@
+"""sedi_b200 -- B200-native SEDI estimator hot path (host-side Python mirror).
+
+The compute path is the CUDA library ``sedi_b200/_lib/libsedi_b200.so``
+(C ABI in ``include/sedi_b200.h``); this module binds it with ctypes and
+mirrors the reference solver interface so a caller written against the
+reference reads the same:
+
+    reference (C++)                                   here
+    Stencil<real_t> stencil(6.0, 1.0, 1.0)            Stencil(6.0, 1.0, 1.0)
+    Cg<real_t> solver(dd, nghost, mode, &timers)      Cg((n1, n2, n3), nghost=1, mode=0)
+    solver.solve(stencil, comm_halo, x, b, iM,        res, err, it = solver.solve(stencil, None, x, b, iM,
+                 maxiter, tol, &final_err, &iter)                               maxiter, tol)
+
+(Cg.hpp:48-82, PipelinedCg.hpp:48-84, BiCgStab.hpp:55-89).  ``x``, ``b``,
+``iM`` are dense n1*n2*n3 float64 arrays, i1 fastest (numpy arrays, or torch
+CUDA tensors for the device-pointer path); ``iM`` may be None for the
+constant 1/a of stochastic-estimator.cc:103.  ``x`` is updated in place.
+Result codes are the reference's result_t values.
+
+There is no CPU fallback: if the native library is missing or no CUDA device
+is present, calls raise ``SediError``.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = [
+    "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "estimate", "fill_probe",
+    "library_path", "load", "SOLVER_IDS", "FP64", "MIXED",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_lib", "libsedi_b200.so")
+
+BICGSTAB, CG, PIPELINED_CG = 1, 2, 3
+SOLVER_IDS = {"bicgstab": BICGSTAB, "cg": CG, "pcg": PIPELINED_CG, "pipelined_cg": PIPELINED_CG}
+FP64, MIXED = 0, 1
+
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "device out of memory", -4: "no CUDA device",
+          -5: "unsupported"}
+
+_lib = None
+
+
+class SediError(RuntimeError):
+    def __init__(self, code, msg=""):
+        self.code = code
+        super().__init__(f"sedi_b200 error {code} ({ERRORS.get(code, '?')}){': ' + msg if msg else ''}")
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def load():
+    """Load the native library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise SediError(-4, f"native library missing: {_LIB_PATH} (run python -m sedi_b200.build)")
+    lib = ctypes.CDLL(_LIB_PATH)
+    c_int, c_long, c_double, vp = ctypes.c_int, ctypes.c_long, ctypes.c_double, ctypes.c_void_p
+    pi, pd = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    lib.sedi_create.restype = vp
+    lib.sedi_create.argtypes = [c_int, c_long, c_long, c_long, c_double, c_double, c_double, c_int, c_int, c_int, pi]
+    lib.sedi_destroy.argtypes = [vp]
+    lib.sedi_destroy.restype = None
+    lib.sedi_ctx_error.argtypes = [vp]
+    lib.sedi_ctx_error.restype = ctypes.c_char_p
+    lib.sedi_solve.argtypes = [vp, vp, vp, vp, c_int, c_double, pd, pi]
+    lib.sedi_solve_dev.argtypes = [vp, vp, vp, vp, c_int, c_double, pd, pi]
+    lib.sedi_solve_batch.argtypes = [vp, c_int, vp, vp, c_int, c_double, vp, vp, vp]
+    lib.sedi_estimate.argtypes = [vp, c_int, ctypes.c_uint32, c_int, c_double, c_int, vp, vp, vp, vp, vp, vp]
+    lib.sedi_estimate_probes.argtypes = [vp, c_int, vp, c_int, c_double, c_int, vp, vp, vp, vp, vp, vp]
+    lib.sedi_fill_probe.argtypes = [ctypes.c_uint32, c_long, vp]
+    lib.sedi_fill_probe.restype = None
+    lib.sedi_stencil_apply.argtypes = [vp, vp, vp]
+    lib.sedi_last_history.argtypes = [vp, vp, c_int]
+    lib.sedi_launch_count.argtypes = [vp]
+    lib.sedi_launch_count.restype = ctypes.c_longlong
+    lib.sedi_version.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(ctypes.c_void_p)
+    return ctypes.c_void_p(int(a.data_ptr()))  # torch tensor
+
+
+def _host_f64(a, n, name):
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous or a.size != n:
+        raise ValueError(f"{name} must be a C-contiguous float64 array of {n} elements")
+    return a
+
+
+def _is_device(a):
+    return a is not None and not isinstance(a, np.ndarray) and hasattr(a, "data_ptr") and a.is_cuda
+
+
+def fill_probe(seed, n):
+    """DistrRngStd::fill_plusminusone with std::mt19937(seed) (DistrRngStd.hpp:22-42)."""
+    out = np.empty(int(n), np.float64)
+    load().sedi_fill_probe(int(seed) & 0xFFFFFFFF, int(n), _ptr(out))
+    return out
+
+
+class Stencil:
+    """Stencil<Dtype>(a, b, c) (Stencil.hpp:12-19): y = a x_c - c (x_{i-1}...) - b (x_{i+1}...)."""
+
+    def __init__(self, a=6.0, b=1.0, c=1.0):
+        self.a, self.b, self.c = float(a), float(b), float(c)
+
+
+class Context:
+    """One solver context on the current CUDA device (sedi_create / sedi_destroy)."""
+
+    def __init__(self, solver, dims, stencil=None, mode=0, precision=FP64, batch=1):
+        lib = load()
+        if isinstance(solver, str):
+            solver = SOLVER_IDS[solver.lower()]
+        self.solver = int(solver)
+        self.dims = tuple(int(d) for d in dims)
+        if len(self.dims) != 3:
+            raise ValueError("dims must be (n1, n2, n3)")
+        self.n = self.dims[0] * self.dims[1] * self.dims[2]
+        self.stencil = stencil or Stencil()
+        self.precision = precision
+        self.batch = int(batch)
+        err = ctypes.c_int(0)
+        s = self.stencil
+        self._h = lib.sedi_create(self.solver, *self.dims, s.a, s.b, s.c, int(mode), int(precision), self.batch,
+                                  ctypes.byref(err))
+        if not self._h:
+            raise SediError(err.value, "sedi_create")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().sedi_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc < 0:
+            raise SediError(rc, f"{what}: {load().sedi_ctx_error(self._h).decode()}")
+        return rc
+
+    @property
+    def launches(self):
+        return int(load().sedi_launch_count(self._h))
+
+    def solve(self, x, b, iM=None, maxiter=1000, tol=1e-4):
+        """Returns (result_t, final_err, final_iter); x is overwritten with the solution."""
+        lib = load()
+        fe, fi = ctypes.c_double(0.0), ctypes.c_int(0)
+        if _is_device(x) or _is_device(b):
+            for t, nm in ((x, "x"), (b, "b"), (iM, "iM")):
+                if t is not None and (not _is_device(t) or t.numel() != self.n or not t.is_contiguous()
+                                      or str(t.dtype) != "torch.float64"):
+                    raise ValueError(f"{nm} must be a contiguous float64 CUDA tensor of {self.n} elements")
+            rc = lib.sedi_solve_dev(self._h, _ptr(b), _ptr(x), _ptr(iM), int(maxiter), float(tol),
+                                    ctypes.byref(fe), ctypes.byref(fi))
+        else:
+            _host_f64(x, self.n, "x")
+            _host_f64(b, self.n, "b")
+            if iM is not None:
+                _host_f64(iM, self.n, "iM")
+            rc = lib.sedi_solve(self._h, _ptr(b), _ptr(x), _ptr(iM), int(maxiter), float(tol),
+                                ctypes.byref(fe), ctypes.byref(fi))
+        self._check(rc, "solve")
+        return rc, fe.value, fi.value
+
+    def solve_batch(self, x, b, maxiter=1000, tol=1e-4):
+        """x, b: (nrhs, n) float64.  Returns (results, final_errs, final_iters) arrays."""
+        b = np.ascontiguousarray(b, np.float64).reshape(-1, self.n)
+        if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous
+                and x.size == b.size):
+            raise ValueError("x must be a C-contiguous float64 array shaped like b")
+        nrhs = b.shape[0]
+        res = np.zeros(nrhs, np.int32)
+        fe = np.zeros(nrhs, np.float64)
+        fi = np.zeros(nrhs, np.int32)
+        rc = load().sedi_solve_batch(self._h, nrhs, _ptr(b), _ptr(x), int(maxiter), float(tol), _ptr(fe),
+                                     _ptr(fi), _ptr(res))
+        self._check(rc, "solve_batch")
+        return res, fe, fi
+
+    def estimate(self, samples, seed=1234, maxiter=1000, tol=1e-4, ignore_errors=True, probes=None):
+        """Estimator loop; returns dict(D, t, q, iters, errs, results, rc)."""
+        n = self.n
+        D, t, q = np.empty(n), np.empty(n), np.empty(n)
+        iters = np.zeros(samples, np.int32)
+        errs = np.zeros(samples, np.float64)
+        results = np.zeros(samples, np.int32)
+        lib = load()
+        if probes is None:
+            rc = lib.sedi_estimate(self._h, int(samples), int(seed) & 0xFFFFFFFF, int(maxiter), float(tol),
+                                   int(bool(ignore_errors)), _ptr(D), _ptr(t), _ptr(q), _ptr(iters), _ptr(errs),
+                                   _ptr(results))
+        else:
+            probes = np.ascontiguousarray(probes, np.float64).reshape(samples, n)
+            rc = lib.sedi_estimate_probes(self._h, int(samples), _ptr(probes), int(maxiter), float(tol),
+                                          int(bool(ignore_errors)), _ptr(D), _ptr(t), _ptr(q), _ptr(iters),
+                                          _ptr(errs), _ptr(results))
+        self._check(rc, "estimate")
+        return dict(D=D, t=t, q=q, iters=iters, errs=errs, results=results, rc=rc)
+
+    def stencil_apply(self, x):
+        x = _host_f64(np.ascontiguousarray(x, np.float64).reshape(-1), self.n, "x")
+        y = np.empty_like(x)
+        self._check(load().sedi_stencil_apply(self._h, _ptr(x), _ptr(y)), "stencil_apply")
+        return y
+
+    def history(self, length=None):
+        length = length or 100000
+        h = np.empty(length, np.float64)
+        k = self._check(load().sedi_last_history(self._h, _ptr(h), length), "history")
+        return h[:k].copy()
+
+
+class _SolverBase:
+    """Shared shape of Cg / PipelinedCg / BiCgStab (reference ctor + solve)."""
+    SOLVER = CG
+
+    def __init__(self, dims, nghost=1, mode=0, timers=None, precision=FP64, batch=1):
+        if nghost != 1:
+            raise ValueError("the reference stencil needs exactly one ghost layer")
+        self.dims = tuple(dims)
+        self.mode = mode
+        self.precision = precision
+        self.batch = batch
+        self._ctx = {}
+
+    def _context(self, A):
+        key = (A.a, A.b, A.c)
+        if key not in self._ctx:
+            self._ctx[key] = Context(self.SOLVER, self.dims, A, self.mode, self.precision, self.batch)
+        return self._ctx[key]
+
+    def solve(self, A, comm_halo, x, b, iM, maxiter, tol):
+        """solve(Stencil&, CommHalo&, x, b, iM, maxiter, tol) -> (result_t, final_err, final_iter).
+
+        comm_halo is accepted for signature parity and ignored: on one GPU the
+        zero ghost layer is applied inside the kernels."""
+        return self._context(A).solve(x, b, iM, maxiter, tol)
+
+
+class Cg(_SolverBase):
+    SOLVER = CG
+    CG_SOLUTION_FOUND, CG_REACHED_MAXITER = 0, 1
+    CG_ASYNCHRONOUS, CG_SYNCHRONOUS_STENCIL, CG_SYNCHRONOUS_DOTPROD = 0, 1, 2
+
+
+class PipelinedCg(_SolverBase):
+    SOLVER = PIPELINED_CG
+    PLCG_SOLUTION_FOUND, PLCG_REACHED_MAXITER = 0, 1
+    PLCG_ASYNCHRONOUS, PLCG_SYNCHRONOUS_STENCIL, PLCG_SYNCHRONOUS_DOTPROD = 0, 1, 2
+
+
+class BiCgStab(_SolverBase):
+    SOLVER = BICGSTAB
+    BICGSTAB_SOLUTION_FOUND, BICGSTAB_REACHED_MAXITER, BICGSTAB_BREAKDOWN_RHO, BICGSTAB_BREAKDOWN_OMEGA = 0, 1, 2, 3
+    BICGSTAB_ASYNCHRONOUS, BICGSTAB_SYNCHRONOUS_STENCIL, BICGSTAB_SYNCHRONOUS_DOTPROD = 0, 1, 2
+
+
+def estimate(solver, dims, samples, seed=1234, maxiter=1000, tol=1e-4, ignore_errors=True, stencil=None,
+             precision=FP64, batch=1, probes=None):
+    """The estimator loop of stochastic-estimator.cc:155-216 (one call)."""
+    with Context(solver, dims, stencil, 0, precision, batch) as ctx:
+        return ctx.estimate(samples, seed, maxiter, tol, ignore_errors, probes)

@@ -1,0 +1,107 @@
+// Internal declarations shared by the sedi_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "sedi_common.cuh"
+#include "../../include/sedi_b200.h"
+
+namespace sedi {
+
+// Stop reasons recorded by the device when a solve leaves its loop.
+enum StopReason : int {
+	STOP_NONE = 0,
+	STOP_EARLY = 1,      // initial residual below tol (iteration 0)
+	STOP_CONVERGED = 2,  // err <= tol inside the loop
+	STOP_MAXITER = 3,    // loop ran to maxiter
+	STOP_RHO = 4,        // BiCGStab rho == 0 at the top of an iteration
+	STOP_OMEGA = 5,      // BiCGStab omega == 0
+	STOP_SNORM = 6,      // BiCGStab ||s||^2 < tol^2 early exit
+};
+
+// Scalar state of one single-vector solve, resident in device memory.  All
+// Krylov scalars are computed on the device (last block of each reduction),
+// so an iteration needs no host round trip.
+struct SolveState {
+	// inputs
+	double tol;
+	int maxiter;
+	// common
+	double bb;       // <b,b> (1 if 0)
+	double rr;       // <r,r>
+	double err;      // sqrt(rr/bb)
+	int iter;        // iteration the next launch executes (1-based)
+	int done;        // loop left
+	int exit_iter;   // value of the reference's loop variable when the loop was left
+	int reason;      // StopReason
+	int wsel;        // ping-pong selector for stencil inputs
+	int pad0;
+	// CG
+	double ru, ru_new, sp, alpha, beta;
+	// pipelined CG
+	double gamma, gamma_old, delta, rr_top;
+	// BiCGStab
+	double rho, rho_prev, omega, vr, s_norm2, ts, tt;
+	int s_exit;
+	int pad1;
+};
+
+struct Ctx {
+	int solver, precision, batch, mode;
+	Geo g;
+	Coef k;
+	int device;
+	cudaStream_t stream;
+	int nblocks;
+
+	// single-vector FP64 buffers (n doubles each)
+	double *x, *b, *iM, *r, *rhat, *p[2], *v[2], *w[2], *u, *q, *s, *z;
+	double *partials;
+	unsigned int *ticket;
+	SolveState *st;        // device
+	SolveState *st_host;   // pinned mirror
+	double *hist;          // device, maxiter_cap+1
+	int hist_cap;
+	int hist_len;
+	cudaGraphExec_t chunk_graph[2];  // [iM is a vector]
+	int chunk_iters;
+
+	// estimator accumulators (n doubles)
+	double *t_acc, *q_acc;
+
+	void *batched;  // batched-form state (batched.cu)
+
+	long long launches;
+	std::string error;
+};
+
+int set_cuda_error(Ctx *c, cudaError_t e, const char *where);
+
+// plain.cu
+int plain_alloc(Ctx *c);
+void plain_free(Ctx *c);
+int plain_solve_dev(Ctx *c, const double *b, double *x, const double *iM, int maxiter, double tol,
+                    double *final_err, int *final_iter);
+int plain_solve_resident(Ctx *c, bool vim, int maxiter, double tol, double *final_err, int *final_iter);
+int plain_history(Ctx *c, double *out, int len);
+int plain_stencil(Ctx *c, const double *x_dev, double *y_dev);
+int plain_accumulate(Ctx *c, const double *x_dev, const double *v_dev, int reset);
+int plain_divide(Ctx *c, double *D_dev);
+
+// batched.cu
+int batched_alloc(Ctx *c);
+void batched_free(Ctx *c);
+int batched_solve_dev(Ctx *c, int nrhs, const double *b, double *x, int maxiter, double tol, double *final_err,
+                      int *final_iter, int *results);
+int batched_estimate_dev(Ctx *c, int samples, const double *probes_dev, int maxiter, double tol,
+                         int ignore_errors, double *D_dev, double *t_dev, double *q_dev, int *iters,
+                         double *errs, int *results);
+
+// rng.cu
+void host_fill_probe(uint32_t seed, long n, double *out);
+
+}  // namespace sedi

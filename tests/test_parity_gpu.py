@@ -1,0 +1,220 @@
+"""Parity of the single-vector FP64 GPU path with the reference (golden
+fixtures produced by the reference sources) and with the CPU oracle.
+
+All calls go through the C ABI (libsedi_b200.so via sedi_b200).  Tolerances
+(relative max-norm, |a-b|max/|b|max):
+  * stencil apply: bit-exact (same seven terms, same order, no FMA);
+  * CG, pipelined CG: 1e-10 at fixed iteration counts and to convergence,
+    identical iteration counts and result codes;
+  * BiCGStab: 1e-10 up to 20 iterations; converged runs 1e-6 with iteration
+    counts within 15% (the reference's own BiCGStab iterates change by 1.5e-3
+    at 32^3 / 50 iterations between a contracted and an uncontracted build).
+"""
+import numpy as np
+import pytest
+
+import _oracle as O
+import sedi_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+SOLVERS = {"cg": 2, "pcg": 3, "bicgstab": 1}
+
+
+def _ctx(solver, dims, coeffs=(6.0, 1.0, 1.0), **kw):
+    return S.Context(solver, dims, S.Stencil(*coeffs), **kw)
+
+
+@pytest.mark.parametrize("dims", [(5, 7, 9), (1, 1, 1), (1, 13, 1), (11, 1, 1), (16, 3, 2), (32, 32, 32),
+                                  (33, 17, 9)])
+@pytest.mark.parametrize("coeffs", [(6.0, 1.0, 1.0), (6.0, 1.3, 0.7), (-2.5, 0.25, -3.0)])
+def test_stencil_bit_exact(dims, coeffs):
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal(int(np.prod(dims)))
+    with _ctx("cg", dims, coeffs) as c:
+        y = c.stencil_apply(x)
+    assert np.array_equal(y, O.stencil(dims, x, coeffs))
+
+
+@pytest.mark.parametrize("solver,K", [("cg", 50), ("pcg", 50), ("bicgstab", 15), ("cg", 200), ("pcg", 200)])
+def test_fixed_iterations_match_oracle(solver, K):
+    dims = (24, 20, 16)
+    n = int(np.prod(dims))
+    b = O.fill_probe(99, n)
+    rc0, fe0, fi0, x0, h0 = O.solve(SOLVERS[solver], dims, b, maxiter=K, tol=0.0)
+    x = np.zeros(n)
+    with _ctx(solver, dims) as c:
+        rc, fe, fi = c.solve(x, b, None, K, 0.0)
+        hist = c.history()
+    assert (rc, fi) == (rc0, fi0)
+    assert O.relmax(x, x0) <= 1e-10
+    assert abs(fe - fe0) <= 1e-10 * fe0 if solver != "bicgstab" else abs(fe - fe0) <= 1e-8 * fe0
+    assert len(hist) == K + 1
+    assert O.relmax(hist[: min(K, 40) + 1], h0[: min(K, 40) + 1]) <= 1e-10
+
+
+def _run_golden(name, ctx_kw=None):
+    g = O.golden(name)
+    m = g["meta"]
+    with _ctx(m["solver"], m["grid"], m["coeffs"], mode=m.get("mode", 0), **(ctx_kw or {})) as c:
+        r = c.estimate(m["samples"], m["seed"], m["maxiter"], m["tol"], ignore_errors=True)
+    return g, m, r
+
+
+def _check_golden(name, tol_D, iter_slack=0.0, tol_err=None):
+    g, m, r = _run_golden(name)
+    assert O.relmax(r["D"], g["D"]) <= tol_D, O.relmax(r["D"], g["D"])
+    assert O.relmax(r["t"], g["t"]) <= tol_D
+    assert np.array_equal(r["q"], g["q"])
+    assert np.array_equal(r["results"], g["results"])
+    if iter_slack:
+        assert np.all(np.abs(r["iters"] - g["iters"]) <= np.ceil(iter_slack * g["iters"]) + 1)
+    else:
+        assert np.array_equal(r["iters"], g["iters"]), (r["iters"], g["iters"])
+        rtol = tol_err or tol_D
+        assert np.all(np.abs(r["errs"] - g["errs"]) <= rtol * np.abs(g["errs"]) + 1e-15)
+
+
+def test_config1_cg_32_vs_reference():
+    # CG, 32^3, 5 probes mt19937(1234+k), tol 1e-9, maxiter 50, -i.
+    _check_golden("cfg1_cg_32", 1e-10)
+
+
+def test_pcg_32_fixed_50_vs_reference():
+    _check_golden("pcg_32_m50", 1e-10)
+
+
+def test_bicgstab_32_fixed_20_vs_reference():
+    _check_golden("bicgstab_32_m20", 1e-10, tol_err=1e-8)
+
+
+@pytest.mark.parametrize("solver", ["cg", "pcg"])
+def test_converged_vs_reference(solver):
+    _check_golden(f"conv_{solver}_24x20x16", 1e-10)
+
+
+def test_converged_bicgstab_vs_reference():
+    _check_golden("conv_bicgstab_24x20x16", 1e-6, iter_slack=0.15)
+
+
+@pytest.mark.parametrize("name", O.golden_names("odd_") + O.golden_names("tiny_") + O.golden_names("line_"))
+def test_small_shapes_vs_reference(name):
+    _check_golden(name, 1e-9, iter_slack=0.15 if "bicgstab" in name else 0.0)
+
+
+def test_nonsymmetric_bicgstab_vs_reference():
+    _check_golden("nonsym_bicgstab_12x10x8", 1e-6, iter_slack=0.15)
+
+
+def test_maxiter_code_vs_reference():
+    _check_golden("maxiter_cg_16", 1e-10)
+
+
+@pytest.mark.parametrize("solver", ["cg", "pcg", "bicgstab"])
+def test_full_128_checksums_vs_reference(solver):
+    """128^3, 64 probes, tol 1e-9 to convergence (the drop-in configuration):
+    per-probe iteration counts, result codes, a strided sample of D and its
+    checksums against the reference run (8 single-rank processes)."""
+    import os
+    name = f"full_{solver}_128"
+    if not os.path.exists(os.path.join(O.GOLDEN, name + ".npz")):
+        pytest.skip("fixture not generated")
+    g = O.golden(name)
+    m = g["meta"]
+    with _ctx(m["solver"], m["grid"]) as c:
+        r = c.estimate(m["samples"], m["seed"], m["maxiter"], m["tol"], ignore_errors=True)
+    stride = m["sample_stride"]
+    assert np.array_equal(r["results"], g["results"])
+    if solver == "bicgstab":
+        assert np.all(np.abs(r["iters"] - g["iters"]) <= np.ceil(0.15 * g["iters"]) + 1)
+        tol = 1e-6
+    else:
+        assert np.array_equal(r["iters"], g["iters"])
+        tol = 1e-10
+    assert O.relmax(r["D"][::stride], g["D_sample"]) <= tol
+    assert abs(r["D"].sum() - float(g["D_sum"])) <= tol * abs(float(g["D_sum"]))
+
+
+def test_vector_preconditioner_matches_constant_and_oracle():
+    dims = (12, 11, 10)
+    n = int(np.prod(dims))
+    b = O.fill_probe(5, n)
+    iM_const = np.full(n, 1.0 / 6.0)
+    rng = np.random.default_rng(3)
+    iM_var = 1.0 / (6.0 + rng.random(n))
+    for solver in ("cg", "pcg", "bicgstab"):
+        with _ctx(solver, dims) as c:
+            x1 = np.zeros(n)
+            r1 = c.solve(x1, b, None, 30, 0.0)
+            x2 = np.zeros(n)
+            r2 = c.solve(x2, b, iM_const, 30, 0.0)
+            assert r1 == r2 and np.array_equal(x1, x2)
+            x3 = np.zeros(n)
+            rc, fe, fi = c.solve(x3, b, iM_var, 25 if solver != "bicgstab" else 12, 0.0)
+        rc0, fe0, fi0, x0, _ = O.solve(SOLVERS[solver], dims, b, iM=iM_var, maxiter=25 if solver != "bicgstab" else 12,
+                                       tol=0.0)
+        assert (rc, fi) == (rc0, fi0)
+        assert O.relmax(x3, x0) <= 1e-10
+
+
+def test_nonzero_initial_guess_and_early_exit():
+    dims = (10, 9, 8)
+    n = int(np.prod(dims))
+    b = O.fill_probe(17, n)
+    x0 = np.linspace(-1, 1, n)
+    for solver in ("cg", "pcg", "bicgstab"):
+        K = 20 if solver != "bicgstab" else 10
+        with _ctx(solver, dims) as c:
+            x = x0.copy()
+            rc, fe, fi = c.solve(x, b, None, K, 0.0)
+            # zero right-hand side: <b,b> is replaced by 1, r = 0, err = 0 < tol -> iteration 0
+            z = np.zeros(n)
+            xz = np.zeros(n)
+            assert c.solve(xz, z, None, 10, 1e-9) == (0, 0.0, 0)
+            # maxiter 0: the loop does not run; result 1 with final_iter 0
+            x_m0 = np.zeros(n)
+            rm = c.solve(x_m0, b, None, 0, 1e-9)
+        rc0, fe0, fi0, xo, _ = O.solve(SOLVERS[solver], dims, b, x0=x0, maxiter=K, tol=0.0)
+        assert (rc, fi) == (rc0, fi0) and O.relmax(x, xo) <= 1e-10
+        r0 = O.solve(SOLVERS[solver], dims, b, maxiter=0, tol=1e-9)
+        assert rm == (r0[0], r0[1], r0[2])
+
+
+def test_device_pointer_path():
+    torch = pytest.importorskip("torch")
+    dims = (16, 16, 16)
+    n = int(np.prod(dims))
+    b = O.fill_probe(1, n)
+    with _ctx("cg", dims) as c:
+        xh = np.zeros(n)
+        rh = c.solve(xh, b, None, 40, 0.0)
+        xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        bd = torch.from_numpy(b).cuda()
+        rd = c.solve(xd, bd, None, 40, 0.0)
+    assert rh == rd
+    assert np.array_equal(xd.cpu().numpy(), xh)
+
+
+def test_reference_interface_classes():
+    dims = (8, 8, 8)
+    n = 512
+    b = O.fill_probe(1234, n)
+    for cls, sid in ((S.Cg, 2), (S.PipelinedCg, 3), (S.BiCgStab, 1)):
+        solver = cls(dims, 1, 0)
+        x = np.zeros(n)
+        res = solver.solve(S.Stencil(6.0, 1.0, 1.0), None, x, b, None, 500, 1e-10)
+        r0 = O.solve(sid, dims, b, maxiter=500, tol=1e-10)
+        assert res[0] == r0[0] == 0
+        assert O.relmax(x, r0[3]) <= 1e-8
+
+
+def test_results_deterministic_run_to_run():
+    dims = (40, 30, 20)
+    n = int(np.prod(dims))
+    b = O.fill_probe(8, n)
+    outs = []
+    for _ in range(2):
+        with _ctx("cg", dims) as c:
+            x = np.zeros(n)
+            outs.append((c.solve(x, b, None, 60, 0.0), x))
+    assert outs[0][0] == outs[1][0] and np.array_equal(outs[0][1], outs[1][1])
