@@ -123,6 +123,29 @@ int sedi_estimate_probes(sedi_ctx *ctx, int samples, const double *probes, int m
                          int ignore_errors, double *D, double *t, double *q, int *iters, double *errs,
                          int *results);
 
+/* Same with device pointers: probes (samples*n doubles) already resident in
+ * HBM, D/t/q device outputs (t, q may be NULL); per-probe arrays on the host.
+ * Runs on the context's stream (see sedi_set_stream). */
+int sedi_estimate_dev(sedi_ctx *ctx, int samples, const double *probes_dev, int maxiter, double tol,
+                      int ignore_errors, double *D_dev, double *t_dev, double *q_dev, int *iters, double *errs,
+                      int *results);
+
+/* Run the context's work on the caller's CUDA stream (a cudaStream_t passed as
+ * void*); NULL restores the context's own stream. */
+int sedi_set_stream(sedi_ctx *ctx, void *stream);
+
+/*
+ * Time the context's per-iteration stencil kernels in isolation: each of the
+ * solver's per-iteration kernels is launched `reps` times back to back on the
+ * context's stream between CUDA events (after one warm-up launch), on the
+ * context's current buffers and a state with every right-hand side active.
+ * Outputs per kernel k < *count: ms[k] average duration of one launch,
+ * bytes[k] its algorithmic DRAM bytes per launch (compulsory reads + writes
+ * of the Krylov vectors it streams), names (count*32 chars, NUL-terminated
+ * slots).  The buffers' contents are scratch afterwards.  Returns 0 or error.
+ */
+int sedi_time_kernels(sedi_ctx *ctx, int reps, double *ms, double *bytes, char *names, int *count);
+
 /* Host probe generator, bit-identical to DistrRngStd with std::mt19937(seed). */
 void sedi_fill_probe(uint32_t seed, long n, double *out);
 

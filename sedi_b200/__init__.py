@@ -81,6 +81,9 @@ def load():
     lib.sedi_launch_count.argtypes = [vp]
     lib.sedi_launch_count.restype = ctypes.c_longlong
     lib.sedi_version.restype = ctypes.c_char_p
+    lib.sedi_estimate_dev.argtypes = [vp, c_int, vp, c_int, c_double, c_int, vp, vp, vp, vp, vp, vp]
+    lib.sedi_set_stream.argtypes = [vp, vp]
+    lib.sedi_time_kernels.argtypes = [vp, c_int, vp, vp, vp, vp]
     _lib = lib
     return lib
 
@@ -220,6 +223,34 @@ class Context:
                                           _ptr(errs), _ptr(results))
         self._check(rc, "estimate")
         return dict(D=D, t=t, q=q, iters=iters, errs=errs, results=results, rc=rc)
+
+    def set_stream(self, stream):
+        """Run on a caller stream (torch.cuda.Stream, cudaStream_t int, or None)."""
+        handle = None if stream is None else int(getattr(stream, "cuda_stream", stream))
+        self._check(load().sedi_set_stream(self._h, ctypes.c_void_p(handle) if handle else None), "set_stream")
+
+    def estimate_dev(self, samples, probes, D, t=None, q=None, maxiter=1000, tol=1e-4, ignore_errors=True):
+        """Estimator on device buffers (torch CUDA float64 tensors): probes (samples, n), D (n,)."""
+        iters = np.zeros(samples, np.int32)
+        errs = np.zeros(samples, np.float64)
+        results = np.zeros(samples, np.int32)
+        rc = load().sedi_estimate_dev(self._h, int(samples), _ptr(probes), int(maxiter), float(tol),
+                                      int(bool(ignore_errors)), _ptr(D), _ptr(t), _ptr(q), _ptr(iters), _ptr(errs),
+                                      _ptr(results))
+        self._check(rc, "estimate_dev")
+        return dict(iters=iters, errs=errs, results=results, rc=rc)
+
+    def time_kernels(self, reps=10):
+        """Per-iteration kernels timed in isolation: list of (name, ms per launch, algorithmic bytes)."""
+        ms = np.zeros(8)
+        by = np.zeros(8)
+        names = ctypes.create_string_buffer(8 * 32)
+        cnt = ctypes.c_int(0)
+        self._check(load().sedi_time_kernels(self._h, int(reps), _ptr(ms), _ptr(by), names, ctypes.byref(cnt)),
+                    "time_kernels")
+        raw = names.raw
+        return [(raw[32 * k: 32 * k + 32].split(b"\0")[0].decode(), float(ms[k]), float(by[k]))
+                for k in range(cnt.value)]
 
     def stencil_apply(self, x):
         x = _host_f64(np.ascontiguousarray(x, np.float64).reshape(-1), self.n, "x")

@@ -1,9 +1,1241 @@
-// Batched (RHS-interleaved) forms -- placeholder until the batched kernels land.
+// Batched (RHS-interleaved) forms of the solvers on sm_100a.
+//
+// Layout: element (point i, right-hand side j) of every Krylov vector is at
+// i*R + j -- the R right-hand sides of one grid point are contiguous.  Grid
+// points are i1 fastest, then i2, i3, as in the reference's
+// Grid3d::rank_cells (Slice3d.hpp:30-32).
+//
+// Each stencil sweep is one streaming kernel (stream.cuh): a block owns a
+// point tile, a slice of lanes and a chunk of planes; planes arrive through a
+// TMA/mbarrier ring in shared memory, the stencil input is computed once per
+// halo point, and the epilogue fuses the pointwise updates and the dot
+// products.  Every right-hand side keeps its own Krylov scalars, reduction
+// results and stop state in device arrays; the last block of each reduction
+// computes them for all lanes, so an iteration needs no host round trip.
+// Reductions are per lane over a block -> point assignment that depends only
+// on the grid and the batch width, so a batch's results do not depend on what
+// else runs on the GPU.
+//
+// Forms:
+//   FP64  (T = double): the reference method lane by lane; elementwise values
+//         round exactly as the reference's (no FMA contraction), dot
+//         products differ from the reference only in summation order.
+//   MIXED (T = float): Krylov vectors in FP32, all reductions and scalars in
+//         FP64, x kept as x_hi (FP64) + x_lo (FP32 correction since the last
+//         reliable update).  A reliable update (Sleijpen & van der Vorst
+//         1996; van der Vorst & Ye 2000; as used for mixed-precision GPU
+//         Krylov solvers by Clark et al. 2010) folds x_lo into x_hi and
+//         replaces r by the FP64 true residual b - A x_hi every `period`
+//         iterations and whenever a lane's FP32 residual reaches tol; a lane
+//         stops only when its FP64 true residual satisfies the reference's
+//         test err = sqrt(<r,r>/<b,b>) <= tol (Cg.hpp:191-193).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
 #include "sedi_internal.h"
+#include "stream.cuh"
 
 namespace sedi {
-int batched_alloc(Ctx *c) { c->error = "batched form not built"; return SEDI_ERR_UNSUPPORTED; }
-void batched_free(Ctx *) {}
-int batched_solve_dev(Ctx *, int, const double *, double *, int, double, double *, int *, int *) { return SEDI_ERR_UNSUPPORTED; }
-int batched_estimate_dev(Ctx *, int, const double *, int, double, int, double *, double *, double *, int *, double *, int *) { return SEDI_ERR_UNSUPPORTED; }
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Per-lane solver state (device).
+// ---------------------------------------------------------------------------
+struct LaneState {
+	double *bb, *rr, *err, *ru, *ru_new, *sp, *alpha, *beta;  // CG
+	double *gamma, *gamma_old, *delta, *rr_top;                 // pipelined CG
+	double *rho, *rho_prev, *omega, *s_norm2, *ts, *tt;         // BiCGStab
+	int *done, *exit_iter, *reason, *pending, *s_exit;
+};
+
+struct Global {
+	int iter;       // iteration the next launch executes
+	int active;     // lanes still iterating
+	int maxiter;
+	int ru_due;     // a reliable update runs after this iteration
+	double tol;
+	int period;     // reliable-update period (mixed)
+	int nrhs;
+	int err;        // a bounded wait timed out
+	int pad;
+};
+
+// Arithmetic: FP64 keeps the reference's operator-by-operator rounding (no
+// contraction); FP32 lets the compiler fuse.
+__device__ __forceinline__ double amul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double aadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double asub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float amul(float a, float b) { return a * b; }
+__device__ __forceinline__ float aadd(float a, float b) { return a + b; }
+__device__ __forceinline__ float asub(float a, float b) { return a - b; }
+
+template <class T>
+__device__ __forceinline__ T st7(T a, T b, T c, T xc, T xm1, T xm2, T xm3, T xp1, T xp2, T xp3) {
+	T y = amul(a, xc);  // Stencil.hpp:43-50 term order
+	y = asub(y, amul(c, xm1));
+	y = asub(y, amul(c, xm2));
+	y = asub(y, amul(c, xm3));
+	y = asub(y, amul(b, xp1));
+	y = asub(y, amul(b, xp2));
+	y = asub(y, amul(b, xp3));
+	return y;
+}
+
+template <class T>
+__device__ __forceinline__ void dacc(double &acc, T a, T b) {
+	acc = fma((double)a, (double)b, acc);
+}
+
+// Map slots (Maps::m) for the per-type descriptor sets.
+enum { MT_R_HALO = 0, MT_P0_HALO, MT_P1_HALO, MT_X_INT, MT_R_INT };  // fields of type T
+enum { MD_X_HALO = 0, MD_B_INT };                                     // FP64 fields
+
+// ---------------------------------------------------------------------------
+// The streaming kernel.
+// Op provides: NS, NQ, ND, ka/kb/kc; enabled(gl); begin(gl, ls, lane);
+// src_map(s); q_map(q); src(raw[NS]) -> stencil input; out(o, c, y, q[NQ],
+// raw_c[NS], part); fin(lane, tot[ND], gl, ls).
+// ---------------------------------------------------------------------------
+template <class C, class Op>
+__global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_constant__ Maps maps, Op op,
+                                                       double *partials, unsigned *ticket, Global *gl, LaneState ls) {
+	typedef typename C::type T;
+	constexpr int V = C::V, LG = C::LG, RB = C::RB, P1 = C::P1, H1 = C::H1, HALO = C::HALO, INT = C::INT,
+	              NPS = C::NPS, KC = C::KC, KO = C::KO;
+	constexpr int NS = Op::NS, NQ = Op::NQ, ND = Op::ND;
+	constexpr bool IDENT = Op::IDENT;
+	typedef Layout<C, NS, NQ, ND, IDENT> Lay;
+	constexpr int NST = Lay::NST, KEEP = Lay::KEEP;
+	extern __shared__ __align__(128) unsigned char smem[];
+	if (gl->active == 0 || !op.enabled(gl)) return;
+
+	T *const stage0 = reinterpret_cast<T *>(smem);
+	T *const ring = reinterpret_cast<T *>(smem + Lay::OFF_RING);
+	uint64_t *const bar = reinterpret_cast<uint64_t *>(smem + Lay::OFF_BAR);
+	constexpr int SE = (int)(Lay::STAGE_PAD / sizeof(T));
+	constexpr int HE = (int)Lay::HALO_ELEMS, IE = (int)Lay::INT_ELEMS;
+
+	const int t = threadIdx.x, lg = t % LG, ps = t / LG;
+	const int tile = blockIdx.x;
+	const int i1_0 = (tile % g.tiles1) * P1, i2_0 = (tile / g.tiles1) * C::P2;
+	const int slice = blockIdx.y, lane0 = slice * RB;
+	const int zoff = slice * g.n3;  // plane offset of this slice in the 4-D map
+	const int z0 = blockIdx.z * g.zc, z1 = min(z0 + g.zc, g.n3);
+	const int np = z1 - z0 + 2;  // planes z0-1 .. z1 (relative index j = p - z0 + 1)
+	const int lo = lg * V;
+	op.begin(gl, ls, lane0 + lo);
+
+	// Per-thread work, identical in every plane: halo vectors (stencil input)
+	// and output points, with their shared-memory offsets and grid validity.
+	int hoff[KC];
+	unsigned hval = 0;
+#pragma unroll
+	for (int k = 0; k < KC; k++) {
+		const int e = t + k * C::THREADS;
+		const int h = e / LG;
+		const int gi1 = i1_0 - 1 + h % H1, gi2 = i2_0 - 1 + h / H1;
+		hoff[k] = e < HALO * LG ? h * RB + lo : -1;
+		if (e < HALO * LG && gi1 >= 0 && gi1 < g.n1 && gi2 >= 0 && gi2 < g.n2) hval |= 1u << k;
+	}
+	int ooff[KO], qoff[KO];
+	long long obase[KO];
+	unsigned oval = 0;
+#pragma unroll
+	for (int k = 0; k < KO; k++) {
+		const int q = ps + k * NPS;
+		const int q1 = q % P1, q2 = q / P1;
+		const int gi1 = i1_0 + q1, gi2 = i2_0 + q2;
+		ooff[k] = ((q2 + 1) * H1 + (q1 + 1)) * RB + lo;
+		qoff[k] = q * RB + lo;
+		obase[k] = (long long)gi2 * g.n1 + gi1;
+		if (q < INT && gi1 < g.n1 && gi2 < g.n2) oval |= 1u << k;
+	}
+	const long long plane = (long long)g.n1 * g.n2;
+
+	if (t == 0) {
+		for (int s = 0; s < NST; s++) mbar_init(&bar[s], 1);
+		mbar_init_fence();
+	}
+	__syncthreads();
+
+	auto issue = [&](int j) {  // thread 0
+		const int p = z0 - 1 + j;
+		uint64_t *b = &bar[j % NST];
+		T *st = stage0 + (j % NST) * SE;
+		if (p < 0 || p >= g.n3) {
+			mbar_arrive(b);  // ghost plane: completes the phase without data
+			return;
+		}
+		fence_async_smem();
+		mbar_arrive_tx(b, Lay::TX);
+#pragma unroll
+		for (int s = 0; s < NS; s++)
+			tma_load3(st + s * HE, &maps.m[op.src_map(s)], b, (i1_0 - 1) * RB, i2_0 - 1, zoff + p);
+#pragma unroll
+		for (int q = 0; q < NQ; q++) tma_load3(st + NS * HE + q * IE, &maps.m[op.q_map(q)], b, i1_0 * RB, i2_0, zoff + p);
+	};
+	int issued = 0;
+	if (t == 0)
+		for (; issued < NST && issued < np; issued++) issue(issued);
+
+	constexpr int NDX = ND > 0 ? ND : 1;
+	double part[NDX][V];
+#pragma unroll
+	for (int d = 0; d < NDX; d++)
+#pragma unroll
+		for (int e = 0; e < V; e++) part[d][e] = 0.0;
+
+	bool failed = false;
+	int waited = 0;  // planes whose stage has arrived
+	int sj = 0;      // stage slot of plane j (j mod NST)
+	unsigned par = 0;  // barrier parity of plane j ((j / NST) & 1)
+	for (int j = 0; j <= np; j++, sj = (sj + 1 == NST) ? 0 : sj + 1, par ^= (sj == 0)) {
+		if (j < np) {
+			const bool ok = mbar_wait(&bar[sj], par);
+			if (__syncthreads_or(!ok)) {
+				failed = true;
+				break;
+			}
+			waited = j + 1;
+		}
+		// Phase 1: stencil input of plane j (transforming ops only).
+		if (!IDENT && j < np) {
+			const int p = z0 - 1 + j;
+			T *cr = ring + (j & 3) * HE;
+			const T *st = stage0 + sj * SE;
+			const bool pin = p >= 0 && p < g.n3;
+#pragma unroll
+			for (int k = 0; k < KC; k++) {
+				if (hoff[k] < 0) continue;
+				Vec<T> cv;
+				if (pin && (hval >> k & 1u)) {
+					Vec<T> raw[NS];
+#pragma unroll
+					for (int s = 0; s < NS; s++) raw[s] = lds(st + s * HE + hoff[k]);
+					cv = op.src(raw);
+				} else {
+					cv = vzero<T>();  // zero ghost layer
+				}
+				sts(cr + hoff[k], cv);
+			}
+		}
+		// Phase 2: outputs of plane m = j-2 from planes m-1, m, m+1.
+		if (j >= 3) {
+			const int m = j - 2;
+			const int z = z0 - 1 + m;
+			// Stage slots of planes m-1, m, m+1 (sj is the slot of plane j = m+2).
+			const int sm1 = sj >= 3 ? sj - 3 : sj - 3 + NST;
+			const int s0 = sj >= 2 ? sj - 2 : sj - 2 + NST;
+			const int sp1 = sj >= 1 ? sj - 1 : sj - 1 + NST;
+			const T *stz = stage0 + s0 * SE;
+			const T *cm, *c0, *cp;
+			bool zm = true, zp = true;  // planes m-1, m+1 inside the grid
+			if (IDENT) {
+				cm = stage0 + sm1 * SE;
+				c0 = stz;
+				cp = stage0 + sp1 * SE;
+				zm = z - 1 >= 0;
+				zp = z + 1 < g.n3;
+			} else {
+				cm = ring + ((m - 1) & 3) * HE;
+				c0 = ring + (m & 3) * HE;
+				cp = ring + ((m + 1) & 3) * HE;
+			}
+#pragma unroll
+			for (int k = 0; k < KO; k++) {
+				if (!(oval >> k & 1u)) continue;
+				const int hc = ooff[k];
+				const Vec<T> xc = lds(c0 + hc);
+				const Vec<T> xm1 = lds(c0 + hc - RB);
+				const Vec<T> xp1 = lds(c0 + hc + RB);
+				const Vec<T> xm2 = lds(c0 + hc - H1 * RB);
+				const Vec<T> xp2 = lds(c0 + hc + H1 * RB);
+				const Vec<T> xm3 = zm ? lds(cm + hc) : vzero<T>();
+				const Vec<T> xp3 = zp ? lds(cp + hc) : vzero<T>();
+				Vec<T> y;
+#pragma unroll
+				for (int e = 0; e < V; e++)
+					y.v[e] = st7<T>(op.ka, op.kb, op.kc, xc.v[e], xm1.v[e], xm2.v[e], xm3.v[e], xp1.v[e], xp2.v[e],
+					                xp3.v[e]);
+				Vec<T> qv[NQ > 0 ? NQ : 1];
+#pragma unroll
+				for (int qq = 0; qq < NQ; qq++) qv[qq] = lds(stz + NS * HE + qq * IE + qoff[k]);
+				Vec<T> rc[NS];
+				if (Op::USES_RAW_CENTER && op.raw_center()) {
+#pragma unroll
+					for (int s = 0; s < NS; s++) rc[s] = lds(stz + s * HE + hc);
+				}
+				const long long pidx = (long long)z * plane + obase[k];
+				const long long o = ((long long)slice * g.npts + pidx) * RB + lo;
+				op.out(o, pidx, lane0 + lo, xc, y, qv, rc, part);
+			}
+		}
+		__syncthreads();
+		// The stage of plane j-KEEP has been read for the last time.
+		if (t == 0 && j >= KEEP && issued < np) {
+			issue(issued);
+			issued++;
+		}
+	}
+	if (failed) {
+		// Timed out: flag the error and wait (bounded) for the copies still in
+		// flight.  The block still takes part in the reduction ticket below so
+		// the next kernel's last-block detection stays consistent; the host
+		// sees the flag and reports the solve as failed.
+		if (t == 0) {
+			atomicExch(&gl->err, 1);
+			for (int jj = waited; jj < issued; jj++) mbar_wait(&bar[jj % NST], (unsigned)((jj / NST) & 1));
+		}
+		__syncthreads();
+	}
+	if (ND == 0) return;
+
+	// Per-lane block reduction over point slots (scratch in the dead stages),
+	// then across blocks.
+	double *const red = reinterpret_cast<double *>(smem);
+	const int R = g.R;
+#pragma unroll
+	for (int d = 0; d < NDX; d++)
+#pragma unroll
+		for (int e = 0; e < V; e++) red[((size_t)d * NPS + ps) * RB + lo + e] = part[d][e];
+	__syncthreads();
+	const unsigned pb = blockIdx.x + gridDim.x * blockIdx.z;
+	const unsigned npb = gridDim.x * gridDim.z;
+	for (int u = t; u < ND * RB; u += C::THREADS) {
+		const int d = u / RB, l = u % RB;
+		double s = 0.0;
+		for (int q = 0; q < NPS; q++) s += red[((size_t)d * NPS + q) * RB + l];
+		partials[((size_t)pb * ND + d) * R + lane0 + l] = s;
+	}
+	__shared__ bool last;
+	__threadfence();
+	__syncthreads();
+	if (t == 0) last = (atomicAdd(ticket, 1u) == gridDim.x * gridDim.y * gridDim.z - 1);
+	__syncthreads();
+	if (!last) return;
+	__threadfence();
+	const int parts = C::THREADS / R > 0 ? C::THREADS / R : 1;
+	double *acc = red;  // [parts][ND][R]
+	for (int u = t; u < parts * R; u += C::THREADS) {
+		const int pid = u / R, lane = u % R;
+		for (int d = 0; d < ND; d++) {
+			double s = 0.0;
+			for (unsigned b = pid; b < npb; b += parts) s += __ldcg(&partials[((size_t)b * ND + d) * R + lane]);
+			acc[((size_t)pid * ND + d) * R + lane] = s;
+		}
+	}
+	__syncthreads();
+	for (int lane = t; lane < R; lane += C::THREADS) {
+		double tot[NDX];
+		for (int d = 0; d < ND; d++) {
+			double s = 0.0;
+			for (int q = 0; q < parts; q++) s += acc[((size_t)q * ND + d) * R + lane];
+			tot[d] = s;
+		}
+		op.fin(lane, tot, gl, ls);
+	}
+	__syncthreads();
+	if (t == 0) *ticket = 0u;
+}
+
+template <class T>
+struct OpBase {
+	T ka, kb, kc;
+	__device__ bool enabled(const Global *) const { return true; }
+};
+
+// ---------------------------------------------------------------------------
+// Residual sweep (FP64 stream over x and b): r = b - A x (Cg.hpp:119-123).
+// Setup (ru == 0): <b,b>, <r,r> per lane, initial stop test; r stored as TR,
+// optional r_hat copy, MIXED: x_lo = 0.
+// Reliable update (ru == 1, x = x_hi): true <r,u>, <r,r>; lanes whose true
+// err <= tol stop, the others continue from the replaced residual.
+// ---------------------------------------------------------------------------
+template <class TR>
+struct OpResid : OpBase<double> {
+	static constexpr int NS = 1, NQ = 1, ND = 2;
+	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
+	TR *r, *rhat, *xlo;  // stored in the TR layout (slice width WT)
+	double iMd;
+	int solver, ru, WT;
+	long long npts;
+	int it;
+	int keep[2];
+	__device__ bool enabled(const Global *gl) const { return !ru || gl->ru_due; }
+	__device__ bool raw_center() const { return false; }
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+		for (int e = 0; e < 2; e++) keep[e] = ru ? ls.done[lane + e] : 0;
+	}
+	__device__ int src_map(int) const { return MD_X_HALO; }
+	__device__ int q_map(int) const { return MD_B_INT; }
+	__device__ Vec<double> src(const Vec<double> *raw) const { return raw[0]; }
+	__device__ void out(long long, long long pidx, int lane, const Vec<double> &, const Vec<double> &ax,
+	                    const Vec<double> *q, const Vec<double> *, double (&part)[ND][2]) const {
+		const long long ot = sliced(pidx, lane, WT, npts);  // lanes lane, lane+1 share a TR slice
+#pragma unroll
+		for (int e = 0; e < 2; e++) {
+			const double bi = q[0].v[e];
+			const double ri = aadd(bi, -ax.v[e]);  // combine2(1.0, b, -1.0, r, r)
+			if (!keep[e]) r[ot + e] = (TR)ri;
+			if (rhat) rhat[ot + e] = (TR)ri;
+			if (xlo) xlo[ot + e] = TR(0);
+			if (ru) part[0][e] = fma(ri, ri * iMd, part[0][e]);
+			else part[0][e] = fma(bi, bi, part[0][e]);
+			part[1][e] = fma(ri, ri, part[1][e]);
+		}
+	}
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		const double tol = gl->tol;
+		const int maxiter = gl->maxiter;
+		if (ru) {
+			if (ls.done[lane]) return;
+			const double err = sqrt(tot[1] / ls.bb[lane]);
+			ls.err[lane] = err;
+			ls.rr[lane] = tot[1];
+			ls.pending[lane] = 0;
+			if (err <= tol) {
+				ls.done[lane] = 1;
+				ls.exit_iter[lane] = it;
+				ls.reason[lane] = STOP_CONVERGED;
+				atomicSub(&gl->active, 1);
+			} else if (it >= maxiter) {
+				ls.done[lane] = 1;
+				ls.exit_iter[lane] = maxiter + 1;
+				ls.reason[lane] = STOP_MAXITER;
+				atomicSub(&gl->active, 1);
+			} else {
+				ls.ru_new[lane] = tot[0];  // continue from the replaced residual
+				ls.beta[lane] = tot[0] / ls.ru[lane];
+			}
+			return;
+		}
+		const double bb = tot[0] == 0.0 ? 1.0 : tot[0];  // Cg.hpp:112-115
+		ls.bb[lane] = bb;
+		ls.rr[lane] = tot[1];
+		const double err = sqrt(__ddiv_rn(tot[1], bb));
+		ls.err[lane] = err;
+		ls.alpha[lane] = 0.0;
+		ls.beta[lane] = 0.0;
+		ls.omega[lane] = 1.0;
+		ls.rho[lane] = 0.0;
+		ls.rho_prev[lane] = 0.0;
+		ls.s_norm2[lane] = 0.0;
+		ls.s_exit[lane] = 0;
+		ls.pending[lane] = 0;
+		ls.gamma[lane] = 0.0;
+		ls.gamma_old[lane] = 0.0;
+		int done = 0, reason = STOP_NONE, ex = 0;
+		if (lane >= gl->nrhs) {
+			done = 1;
+		} else if (err < tol) {  // :130-134
+			done = 1;
+			reason = STOP_EARLY;
+		} else if (maxiter < 1) {
+			done = 1;
+			reason = STOP_MAXITER;
+			ex = 1;
+		} else if (solver == 1) {
+			ls.rho[lane] = tot[1];
+			if (tot[1] == 0.0) {
+				done = 1;
+				reason = STOP_RHO;
+				ex = 1;
+			}
+		}
+		ls.done[lane] = done;
+		ls.reason[lane] = reason;
+		ls.exit_iter[lane] = ex;
+		if (!done) atomicAdd(&gl->active, 1);
+	}
+};
+
+// ---------------------------------------------------------------------------
+// CG kernel A: p = u + beta p (u = r .* iM; p = u on iteration 1), s = A p,
+// <s,p> (and <r,u> on iteration 1); alpha = <r,u>/<s,p>  (Cg.hpp:150-166, :188).
+// ---------------------------------------------------------------------------
+template <class T>
+struct OpCgA : OpBase<T> {
+	static constexpr int NS = 2, NQ = 0, ND = 2;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr int V = Vec<T>::V;
+	T iMc;
+	T *p0, *p1;
+	T *pout;  // p buffer written this iteration
+	int it;
+	bool first;
+	T beta[V];
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+		first = (it == 1);
+		pout = (it & 1) ? p1 : p0;
+#pragma unroll
+		for (int e = 0; e < V; e++) beta[e] = (T)ls.beta[lane + e];
+	}
+	__device__ bool raw_center() const { return first; }  // <r,u> is only needed on iteration 1
+	__device__ int src_map(int s) const { return s == 0 ? MT_R_HALO : ((it & 1) ? MT_P0_HALO : MT_P1_HALO); }
+	__device__ int q_map(int) const { return 0; }
+	__device__ Vec<T> src(const Vec<T> *raw) const {
+		// 1.0*u == u and (-1.0)*v == -v exactly, so the reference's
+		// combine2(1.0, u, beta, p) rounds as u + round(beta*p).
+		Vec<T> o;
+		if (first) {
+#pragma unroll
+			for (int e = 0; e < V; e++) o.v[e] = amul(raw[0].v[e], iMc);
+		} else {
+#pragma unroll
+			for (int e = 0; e < V; e++) o.v[e] = aadd(amul(raw[0].v[e], iMc), amul(beta[e], raw[1].v[e]));
+		}
+		return o;
+	}
+	__device__ void out(long long o, long long, int, const Vec<T> &pc, const Vec<T> &s, const Vec<T> *,
+	                    const Vec<T> *rc, double (&part)[ND][V]) const {
+		stg(pout + o, pc);
+#pragma unroll
+		for (int e = 0; e < V; e++) dacc(part[0][e], s.v[e], pc.v[e]);
+		if (first) {
+#pragma unroll
+			for (int e = 0; e < V; e++) dacc(part[1][e], rc[0].v[e], amul(rc[0].v[e], iMc));
+		}
+	}
+	__device__ void fin(int lane, const double *tot, Global *, const LaneState &ls) const {
+		if (ls.done[lane]) {
+			ls.alpha[lane] = 0.0;
+			return;
+		}
+		ls.sp[lane] = tot[0];
+		const double ru = first ? tot[1] : ls.ru_new[lane];
+		ls.ru[lane] = ru;
+		ls.alpha[lane] = __ddiv_rn(ru, tot[0]);
+	}
+};
+
+// ---------------------------------------------------------------------------
+// CG kernel B: s = A p, x += alpha p, r -= alpha s, u = r .* iM, <r,u>, <r,r>;
+// beta, err, stop test (Cg.hpp:169-193).
+// ---------------------------------------------------------------------------
+template <class T>
+struct OpCgB : OpBase<T> {
+	static constexpr int NS = 1, NQ = 2, ND = 2;
+	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
+	static constexpr int V = Vec<T>::V;
+	T iMc;
+	T *x, *r;
+	int mixed;
+	int it;
+	T alpha[V];
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+#pragma unroll
+		for (int e = 0; e < V; e++) alpha[e] = (T)ls.alpha[lane + e];
+	}
+	__device__ int src_map(int) const { return (it & 1) ? MT_P1_HALO : MT_P0_HALO; }
+	__device__ int q_map(int q) const { return q == 0 ? MT_X_INT : MT_R_INT; }
+	__device__ bool raw_center() const { return false; }
+	__device__ Vec<T> src(const Vec<T> *raw) const { return raw[0]; }
+	__device__ void out(long long o, long long, int, const Vec<T> &pc, const Vec<T> &s, const Vec<T> *q,
+	                    const Vec<T> *, double (&part)[ND][V]) const {
+		Vec<T> xv = q[0], rv = q[1];
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			xv.v[e] = aadd(xv.v[e], amul(alpha[e], pc.v[e]));  // :169
+			rv.v[e] = aadd(rv.v[e], amul(-alpha[e], s.v[e]));  // :172
+			const T u = amul(rv.v[e], iMc);                                // :175
+			dacc(part[0][e], rv.v[e], u);
+			dacc(part[1][e], rv.v[e], rv.v[e]);
+		}
+		stg(x + o, xv);
+		stg(r + o, rv);
+	}
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		if (ls.done[lane]) return;
+		ls.ru_new[lane] = tot[0];
+		ls.rr[lane] = tot[1];
+		ls.beta[lane] = __ddiv_rn(tot[0], ls.ru[lane]);           // :185
+		const double err = sqrt(__ddiv_rn(tot[1], ls.bb[lane]));  // :191
+		ls.err[lane] = err;
+		const double tol = gl->tol;
+		const int maxiter = gl->maxiter;
+		if (mixed) {
+			// The FP32 recurrence only proposes; the FP64 true residual decides.
+			if (err <= tol || it >= maxiter) {
+				ls.pending[lane] = 1;
+				gl->ru_due = 1;
+			}
+			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = 1;
+		} else if (err <= tol) {  // :193
+			ls.done[lane] = 1;
+			ls.exit_iter[lane] = it;
+			ls.reason[lane] = STOP_CONVERGED;
+			atomicSub(&gl->active, 1);
+		} else if (it >= maxiter) {
+			ls.done[lane] = 1;
+			ls.exit_iter[lane] = maxiter + 1;
+			ls.reason[lane] = STOP_MAXITER;
+			atomicSub(&gl->active, 1);
+		}
+	}
+};
+
+// Iteration bookkeeping between launches.
+__global__ void kb_next_iter(Global *gl) {
+	if (gl->active == 0) return;
+	if (gl->ru_due == 0) gl->iter += 1;
+}
+
+__global__ void kb_ru_done(Global *gl) {
+	if (gl->ru_due) {
+		gl->ru_due = 0;
+		gl->iter += 1;
+	}
+}
+
+// Reliable update (MIXED): x_hi += x_lo, x_lo = 0.  x_hi uses FP64 slices
+// of width WD, x_lo FP32 slices of width WT.
+__global__ void __launch_bounds__(256) kb_ru_fold(long long npts, int R, int WD, int WT, double *__restrict__ xh,
+                                                  float *__restrict__ xl, Global *gl) {
+	if (gl->active == 0 || gl->ru_due == 0) return;
+	const long long pairs = npts * R / 2;
+	for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < pairs;
+	     u += (long long)gridDim.x * blockDim.x) {
+		const long long od = 2 * u;  // FP64 offset
+		const long long sd = od / ((long long)WD * npts);
+		const long long rem = od - sd * WD * npts;
+		const long long i = rem / WD;
+		const int j = (int)(sd * WD + rem % WD);
+		const long long ot = sliced(i, j, WT, npts);
+		const float2 lo = *reinterpret_cast<const float2 *>(xl + ot);
+		double2 hi = *reinterpret_cast<double2 *>(xh + od);
+		hi.x += (double)lo.x;
+		hi.y += (double)lo.y;
+		*reinterpret_cast<double2 *>(xh + od) = hi;
+		*reinterpret_cast<float2 *>(xl + ot) = make_float2(0.f, 0.f);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Estimator accumulation over a batch: t += x .* v, q += v .* v per point,
+// lanes in probe order (stochastic-estimator.cc:195, :198).  x and v are FP64
+// fields in the sliced layout of width W.
+// ---------------------------------------------------------------------------
+__global__ void kb_accumulate(long long npts, int W, int nrhs, const double *__restrict__ x,
+                              const double *__restrict__ v, double *__restrict__ t, double *__restrict__ q, int reset) {
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (long long)gridDim.x * blockDim.x) {
+		double tt = reset ? 0.0 : t[i];
+		double qq = reset ? 0.0 : q[i];
+		for (int j = 0; j < nrhs; j++) {
+			const long long o = sliced(i, j, W, npts);
+			const double vj = v[o];
+			tt = __dadd_rn(tt, __dmul_rn(x[o], vj));
+			qq = __dadd_rn(qq, __dmul_rn(vj, vj));
+		}
+		t[i] = tt;
+		q[i] = qq;
+	}
+}
+
+__global__ void kb_divide(long long n, const double *__restrict__ t, const double *__restrict__ q,
+                          double *__restrict__ D) {
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+		D[i] = __ddiv_rn(t[i], q[i]);
+}
+
+// Dense right-hand sides (k*npts + i) -> sliced FP64 layout of width W over R
+// lanes, zero padding lanes >= nrhs.
+__global__ void kb_interleave(long long npts, int R, int W, int nrhs, const double *__restrict__ src,
+                              double *__restrict__ dst) {
+	const long long total = npts * R;
+	for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (long long)gridDim.x * blockDim.x) {
+		const long long s = u / ((long long)W * npts);
+		const long long rem = u - s * W * npts;
+		const long long i = rem / W;
+		const int j = (int)(s * W + rem % W);
+		dst[u] = j < nrhs ? src[(long long)j * npts + i] : 0.0;
+	}
+}
+
+__global__ void kb_deinterleave(long long npts, int W, int nrhs, const double *__restrict__ src,
+                                double *__restrict__ dst) {
+	const long long total = npts * nrhs;
+	for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (long long)gridDim.x * blockDim.x) {
+		const long long j = u / npts;
+		const long long i = u - j * npts;
+		dst[u] = src[sliced(i, (int)j, W, npts)];
+	}
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side.
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+	static EncodeTiledFn fn = nullptr;
+	if (!fn) {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			fn = (EncodeTiledFn)p;
+		else
+			cudaGetLastError();
+	}
+	return fn;
+}
+
+// 3-D map over a sliced field ([R/W slices][n3][n2][n1][W] of `eb`-byte
+// elements) seen as [n3*slices][n2][n1*W]: one slice row of n1 points is a
+// single contiguous TMA row.  Box W*b1 x b2 x 1; elements outside a row
+// (points i1 < 0 or >= n1) and rows outside the grid read as zero.  Planes
+// are never addressed outside a slice (planes -1 and n3 are handled without
+// loads).
+static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, int W, int b1, int b2) {
+	EncodeTiledFn fn = encode_fn();
+	if (!fn) return false;
+	const cuuint64_t dims[3] = {(cuuint64_t)W * g.n1, (cuuint64_t)g.n2, (cuuint64_t)g.n3 * (R / W)};
+	const cuuint64_t strides[2] = {(cuuint64_t)g.n1 * W * eb, (cuuint64_t)g.n1 * g.n2 * W * eb};
+	const cuuint32_t box[3] = {(cuuint32_t)(W * b1), (cuuint32_t)b2, 1};
+	const cuuint32_t es[3] = {1, 1, 1};
+	return fn(m, eb == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides,
+	          box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+	          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+struct Batched {
+	int R = 0;
+	bool mixed = false;
+	size_t elems = 0;  // npts * R
+	// vectors ([point][R])
+	void *x = nullptr;     // FP64 form: x; MIXED: x_lo (FP32)
+	double *xh = nullptr;  // MIXED x_hi
+	double *b = nullptr;   // right-hand sides (FP64)
+	void *r = nullptr, *p0 = nullptr, *p1 = nullptr;
+	double *partials = nullptr;
+	unsigned *ticket = nullptr;
+	Global *gl = nullptr, *gl_host = nullptr;
+	LaneState ls;
+	double *lane_mem = nullptr;
+	int *lane_int = nullptr;
+	double *t_acc = nullptr, *q_acc = nullptr;
+	int period = 32;
+	int chunk = 16;
+	cudaGraphExec_t graph = nullptr;
+	long long graph_kernels = 0;
+	// launch shapes
+	int rbT = 0, rbD = 0;  // lanes per block slice for T and FP64 streams
+	SGeo gT, gD;
+	dim3 gridT, gridD;
+	Maps mapsT, mapsD;
+};
+
+#define BTRY(expr)                                                            \
+	do {                                                                      \
+		cudaError_t e_ = (expr);                                              \
+		if (e_ != cudaSuccess) return set_cuda_error(c, e_, #expr);           \
+	} while (0)
+
+// Stream configurations per (type, lane slice width).  The full slice is
+// kSliceBytes per point; the point tile gives every block at least THREADS
+// (point, lane group) slots.
+#ifndef SEDI_STREAM_THREADS
+#define SEDI_STREAM_THREADS 512
+#endif
+#ifndef SEDI_SLICE_LANES
+#define SEDI_SLICE_LANES 8
+#endif
+constexpr int kThr = SEDI_STREAM_THREADS, kSliceLanes = SEDI_SLICE_LANES;
+
+// Point tiles: at least THREADS (point, lane group) slots per block, and a
+// merged TMA row W*(P1+2) within the 256-element box limit.
+__host__ __device__ constexpr int tile_p1(int lg) { return lg == 1 ? 32 : 16; }
+__host__ __device__ constexpr int tile_p2(int lg) { return lg >= 4 ? 8 : 16; }
+
+template <class T, int RB>
+struct CfgFor {
+	static constexpr int LG = RB * (int)sizeof(T) / 16;
+	typedef Cfg<T, RB, tile_p1(LG), tile_p2(LG), kThr> type;
+};
+
+static int pick_R(int nrhs, bool mixed) {
+	const int V = mixed ? 4 : 2, full = 8 * V;
+	if (nrhs <= V) return V;
+	if (nrhs <= 2 * V) return 2 * V;
+	if (nrhs <= 4 * V) return 4 * V;
+	return (nrhs + full - 1) / full * full;
+}
+
+static int slice_for(int R, bool) { return R >= kSliceLanes ? kSliceLanes : R; }
+
+static void tile_for(int rb, int eb, int *P1, int *P2) {
+	const int lg = rb * eb / 16;
+	*P1 = tile_p1(lg);
+	*P2 = tile_p2(lg);
+}
+
+static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid) {
+	int P1, P2;
+	tile_for(rb, eb, &P1, &P2);
+	const int t1 = (g.n1 + P1 - 1) / P1, t2 = (g.n2 + P2 - 1) / P2;
+	const int slices = R / rb;
+	// About two blocks' worth of work per SM: split i3 when the tile count is small.
+	const long long want = 148LL * 2;
+	const long long per = (long long)t1 * t2 * slices;
+	long long nz = (want + per - 1) / per;
+	if (nz < 1) nz = 1;
+	if (nz > g.n3) nz = g.n3;
+	int zc = (int)((g.n3 + nz - 1) / nz);
+	if (zc < 4) zc = g.n3 < 4 ? g.n3 : 4;
+	nz = (g.n3 + zc - 1) / zc;
+	sg->n1 = g.n1;
+	sg->n2 = g.n2;
+	sg->n3 = g.n3;
+	sg->R = R;
+	sg->W = rb;
+	sg->npts = g.n;
+	sg->zc = zc;
+	sg->tiles1 = t1;
+	*grid = dim3((unsigned)(t1 * t2), (unsigned)slices, (unsigned)nz);
+}
+
+template <class C, class Op>
+static int launch(Ctx *c, Batched *B, const SGeo &sg, dim3 grid, const Maps &maps, const Op &op, cudaStream_t s) {
+	const size_t sm = Layout<C, Op::NS, Op::NQ, Op::ND, Op::IDENT>::BYTES;
+	static bool attr_set = false;
+	if (!attr_set) {
+		cudaFuncSetAttribute(k_stream<C, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+		attr_set = true;
+	}
+	k_stream<C, Op><<<grid, C::THREADS, sm, s>>>(sg, maps, op, B->partials, B->ticket, B->gl, B->ls);
+	c->launches++;
+	return 0;
+}
+
+int batched_alloc(Ctx *c) {
+	Batched *B = new (std::nothrow) Batched();
+	if (!B) return SEDI_ERR_NOMEM;
+	c->batched = B;
+	B->mixed = c->precision == SEDI_PREC_MIXED;
+	if (c->batch > (B->mixed ? 256 : 128)) {
+		c->error = "batch too large for one context (max 256 FP32 / 128 FP64 right-hand sides)";
+		return SEDI_ERR_ARG;
+	}
+	if (c->solver != 2) {
+		c->error = "batched form implemented for CG";
+		return SEDI_ERR_UNSUPPORTED;
+	}
+	if (!encode_fn()) {
+		c->error = "cuTensorMapEncodeTiled unavailable";
+		return SEDI_ERR_NODEV;
+	}
+	B->R = pick_R(c->batch, B->mixed);
+	B->elems = (size_t)c->g.n * B->R;
+	const int ebT = B->mixed ? 4 : 8;
+	B->rbT = slice_for(B->R, !B->mixed);
+	B->rbD = slice_for(B->R, true);
+	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT);
+	shape(c->g, B->R, B->rbD, 8, &B->gD, &B->gridD);
+	const size_t ts = B->mixed ? sizeof(float) : sizeof(double);
+	const size_t nblkT = (size_t)B->gridT.x * B->gridT.z, nblkD = (size_t)B->gridD.x * B->gridD.z;
+	const size_t nblk = nblkT > nblkD ? nblkT : nblkD;
+	if (cudaMalloc(&B->x, B->elems * ts) != cudaSuccess || cudaMalloc(&B->r, B->elems * ts) != cudaSuccess ||
+	    cudaMalloc(&B->p0, B->elems * ts) != cudaSuccess || cudaMalloc(&B->p1, B->elems * ts) != cudaSuccess ||
+	    cudaMalloc(&B->b, B->elems * sizeof(double)) != cudaSuccess ||
+	    (B->mixed && cudaMalloc(&B->xh, B->elems * sizeof(double)) != cudaSuccess) ||
+	    cudaMalloc(&B->partials, sizeof(double) * nblk * kMaxDots * B->R) != cudaSuccess ||
+	    cudaMalloc(&B->ticket, sizeof(unsigned)) != cudaSuccess || cudaMalloc(&B->gl, sizeof(Global)) != cudaSuccess ||
+	    cudaMallocHost(&B->gl_host, sizeof(Global)) != cudaSuccess ||
+	    cudaMalloc(&B->lane_mem, sizeof(double) * 20 * B->R) != cudaSuccess ||
+	    cudaMalloc(&B->lane_int, sizeof(int) * 5 * B->R) != cudaSuccess ||
+	    cudaMalloc(&B->t_acc, sizeof(double) * c->g.n) != cudaSuccess ||
+	    cudaMalloc(&B->q_acc, sizeof(double) * c->g.n) != cudaSuccess) {
+		cudaGetLastError();
+		c->error = "device allocation failed (batched form)";
+		return SEDI_ERR_NOMEM;
+	}
+	cudaMemset(B->ticket, 0, sizeof(unsigned));
+	cudaMemset(B->x, 0, B->elems * ts);
+	cudaMemset(B->r, 0, B->elems * ts);
+	cudaMemset(B->p0, 0, B->elems * ts);
+	cudaMemset(B->p1, 0, B->elems * ts);
+	const int R = B->R;
+	LaneState &ls = B->ls;
+	double **dp[] = {&ls.bb, &ls.rr, &ls.err, &ls.ru, &ls.ru_new, &ls.sp, &ls.alpha, &ls.beta, &ls.gamma,
+	                 &ls.gamma_old, &ls.delta, &ls.rr_top, &ls.rho, &ls.rho_prev, &ls.omega, &ls.s_norm2, &ls.ts,
+	                 &ls.tt};
+	for (size_t i = 0; i < sizeof(dp) / sizeof(dp[0]); i++) *dp[i] = B->lane_mem + i * R;
+	int **ip[] = {&ls.done, &ls.exit_iter, &ls.reason, &ls.pending, &ls.s_exit};
+	for (size_t i = 0; i < 5; i++) *ip[i] = B->lane_int + i * R;
+	// Tensor maps.
+	int P1, P2;
+	tile_for(B->rbT, ebT, &P1, &P2);
+	bool ok = make_map(&B->mapsT.m[MT_R_HALO], B->r, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
+	          make_map(&B->mapsT.m[MT_P0_HALO], B->p0, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
+	          make_map(&B->mapsT.m[MT_P1_HALO], B->p1, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
+	          make_map(&B->mapsT.m[MT_X_INT], B->x, ebT, c->g, R, B->rbT, P1, P2) &&
+	          make_map(&B->mapsT.m[MT_R_INT], B->r, ebT, c->g, R, B->rbT, P1, P2);
+	tile_for(B->rbD, 8, &P1, &P2);
+	ok = ok && make_map(&B->mapsD.m[MD_X_HALO], B->mixed ? (void *)B->xh : B->x, 8, c->g, R, B->rbD, P1 + 2, P2 + 2) &&
+	     make_map(&B->mapsD.m[MD_B_INT], B->b, 8, c->g, R, B->rbD, P1, P2);
+	if (!ok) {
+		c->error = "tensor map encoding failed";
+		return SEDI_ERR_CUDA;
+	}
+	return 0;
+}
+
+void batched_free(Ctx *c) {
+	Batched *B = (Batched *)c->batched;
+	if (!B) return;
+	void *ptrs[] = {B->x, B->xh, B->b, B->r, B->p0, B->p1, B->partials, B->ticket, B->gl, B->lane_mem, B->lane_int,
+	                B->t_acc, B->q_acc};
+	for (void *p : ptrs)
+		if (p) cudaFree(p);
+	if (B->gl_host) cudaFreeHost(B->gl_host);
+	if (B->graph) cudaGraphExecDestroy(B->graph);
+	delete B;
+	c->batched = nullptr;
+}
+
+template <int RBD>
+static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
+	typedef typename CfgFor<double, RBD>::type CD;
+	cudaStream_t s = c->stream;
+	if (B->mixed) {
+		OpResid<float> op;
+		op.ka = c->k.a;
+		op.kb = c->k.b;
+		op.kc = c->k.c;
+		op.r = (float *)B->r;
+		op.rhat = nullptr;
+		op.xlo = ru ? nullptr : (float *)B->x;
+		op.WT = B->rbT;
+		op.npts = c->g.n;
+		op.iMd = 1.0 / c->k.a;
+		op.solver = c->solver;
+		op.ru = ru ? 1 : 0;
+		launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, s);
+	} else {
+		OpResid<double> op;
+		op.ka = c->k.a;
+		op.kb = c->k.b;
+		op.kc = c->k.c;
+		op.r = (double *)B->r;
+		op.rhat = nullptr;
+		op.xlo = nullptr;
+		op.WT = B->rbT;
+		op.npts = c->g.n;
+		op.iMd = 1.0 / c->k.a;
+		op.solver = c->solver;
+		op.ru = 0;
+		launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, s);
+	}
+}
+
+template <class T, int RBT, int RBD>
+static void enqueue_cg_iteration(Ctx *c, Batched *B) {
+	typedef typename CfgFor<T, RBT>::type C;
+	cudaStream_t s = c->stream;
+	OpCgA<T> a;
+	a.ka = (T)c->k.a;
+	a.kb = (T)c->k.b;
+	a.kc = (T)c->k.c;
+	a.iMc = (T)(1.0 / c->k.a);
+	a.p0 = (T *)B->p0;
+	a.p1 = (T *)B->p1;
+	launch<C>(c, B, B->gT, B->gridT, B->mapsT, a, s);
+	OpCgB<T> bo;
+	bo.ka = (T)c->k.a;
+	bo.kb = (T)c->k.b;
+	bo.kc = (T)c->k.c;
+	bo.iMc = (T)(1.0 / c->k.a);
+	bo.x = (T *)B->x;
+	bo.r = (T *)B->r;
+	bo.mixed = B->mixed ? 1 : 0;
+	launch<C>(c, B, B->gT, B->gridT, B->mapsT, bo, s);
+	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
+	c->launches++;
+	if (B->mixed) {
+		const long long nb = ((long long)B->elems / 2 + 255) / 256;
+		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
+		                                                                 (float *)B->x, B->gl);
+		c->launches++;
+		enqueue_resid<RBD>(c, B, true);
+		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
+		c->launches++;
+	}
+}
+
+template <class T, int RBT, int RBD>
+static int run_batched(Ctx *c, Batched *B, int maxiter, double tol) {
+	cudaStream_t s = c->stream;
+	Global g0 = {};
+	g0.iter = 1;
+	g0.maxiter = maxiter;
+	g0.tol = tol;
+	g0.period = B->period;
+	g0.nrhs = B->gl_host->nrhs;
+	g0.active = 1;  // lets the setup sweep run; its finisher adds one per live lane
+	*B->gl_host = g0;
+	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
+	enqueue_resid<RBD>(c, B, false);
+	BTRY(cudaGetLastError());
+	BTRY(cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s));
+	BTRY(cudaStreamSynchronize(s));
+	if (B->gl_host->err) {
+		c->error = "batched sweep timed out waiting for its data";
+		return SEDI_ERR_CUDA;
+	}
+	B->gl_host->active -= 1;
+	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
+	if (!B->graph) {
+		// The graph bakes in tol/maxiter only through Global (device), so it is reusable.
+		cudaGraph_t graph;
+		const long long before = c->launches;
+		BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+		for (int i = 0; i < B->chunk; i++) enqueue_cg_iteration<T, RBT, RBD>(c, B);
+		BTRY(cudaStreamEndCapture(s, &graph));
+		B->graph_kernels = c->launches - before;
+		c->launches = before;
+		cudaError_t e = cudaGraphInstantiate(&B->graph, graph, 0);
+		cudaGraphDestroy(graph);
+		if (e != cudaSuccess) {
+			B->graph = nullptr;
+			return set_cuda_error(c, e, "cudaGraphInstantiate");
+		}
+	}
+	long long rounds = 0;
+	const long long max_rounds = (long long)maxiter * 2 / B->chunk + 4;
+	while (B->gl_host->active > 0) {
+		BTRY(cudaGraphLaunch(B->graph, s));
+		c->launches += B->graph_kernels;
+		BTRY(cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s));
+		BTRY(cudaStreamSynchronize(s));
+		if (B->gl_host->err) {
+			c->error = "batched sweep timed out waiting for its data";
+			return SEDI_ERR_CUDA;
+		}
+		if (++rounds > max_rounds) {
+			c->error = "batched solver did not stop";
+			return SEDI_ERR_CUDA;
+		}
+	}
+	return 0;
+}
+
+template <class T, int RBT>
+static int dispatch_d(Ctx *c, Batched *B, int maxiter, double tol) {
+	switch (B->rbD) {
+	case 2: return run_batched<T, RBT, 2>(c, B, maxiter, tol);
+	case 4: return run_batched<T, RBT, 4>(c, B, maxiter, tol);
+	default: return run_batched<T, RBT, 8>(c, B, maxiter, tol);
+	}
+}
+
+static int dispatch_run(Ctx *c, Batched *B, int maxiter, double tol) {
+	if (B->mixed) {
+		switch (B->rbT) {
+		case 4: return dispatch_d<float, 4>(c, B, maxiter, tol);
+		default: return dispatch_d<float, 8>(c, B, maxiter, tol);
+		}
+	}
+	switch (B->rbT) {
+	case 2: return run_batched<double, 2, 2>(c, B, maxiter, tol);
+	case 4: return run_batched<double, 4, 4>(c, B, maxiter, tol);
+	default: return run_batched<double, 8, 8>(c, B, maxiter, tol);
+	}
+}
+
+// Result per lane with the reference post-loop logic (Cg.hpp:197-206).
+static int lane_result(int reason, int exit_iter, double err, double tol, int maxiter, double *fe, int *fi) {
+	if (reason == STOP_EARLY) {
+		*fi = 0;
+		*fe = err;
+		return 0;
+	}
+	if (err <= tol) {
+		*fi = exit_iter;
+		*fe = err;
+		return 0;
+	}
+	*fi = maxiter;
+	*fe = err;
+	return 1;
+}
+
+static int batched_run_resident(Ctx *c, int nrhs, int maxiter, double tol, double *final_err, int *final_iter,
+                                int *results) {
+	Batched *B = (Batched *)c->batched;
+	B->gl_host->nrhs = nrhs;
+	int rc = dispatch_run(c, B, maxiter, tol);
+	if (rc) return rc;
+	std::vector<double> err(B->R);
+	std::vector<int> lint(5 * B->R);
+	BTRY(cudaMemcpy(err.data(), B->ls.err, sizeof(double) * B->R, cudaMemcpyDeviceToHost));
+	BTRY(cudaMemcpy(lint.data(), B->lane_int, sizeof(int) * 5 * B->R, cudaMemcpyDeviceToHost));
+	int worst = 0;
+	for (int j = 0; j < nrhs; j++) {
+		const int reason = lint[2 * B->R + j], ex = lint[1 * B->R + j];
+		const int res = lane_result(reason, ex, err[j], tol, maxiter, &final_err[j], &final_iter[j]);
+		if (results) results[j] = res;
+		if (res > worst) worst = res;
+	}
+	return worst;
+}
+
+static int blocks1d(long long n) {
+	long long b = (n + 255) / 256;
+	return (int)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
+}
+
+int batched_solve_dev(Ctx *c, int nrhs, const double *b, double *x, int maxiter, double tol, double *final_err,
+                      int *final_iter, int *results) {
+	Batched *B = (Batched *)c->batched;
+	if (!B || nrhs < 1 || nrhs > c->batch) {
+		c->error = "nrhs outside 1..batch";
+		return SEDI_ERR_ARG;
+	}
+	cudaStream_t s = c->stream;
+	const long long n = c->g.n;
+	kb_interleave<<<blocks1d(n * B->R), 256, 0, s>>>(n, B->R, B->rbD, nrhs, b, B->b);
+	kb_interleave<<<blocks1d(n * B->R), 256, 0, s>>>(n, B->R, B->rbD, nrhs, x, B->mixed ? B->xh : (double *)B->x);
+	c->launches += 2;
+	int rc = batched_run_resident(c, nrhs, maxiter, tol, final_err, final_iter, results);
+	if (rc < 0) return rc;
+	kb_deinterleave<<<blocks1d(n * nrhs), 256, 0, s>>>(n, B->rbD, nrhs, B->mixed ? B->xh : (const double *)B->x, x);
+	c->launches++;
+	BTRY(cudaStreamSynchronize(s));
+	return rc;
+}
+
+// Per-iteration kernels of the batched CG timed in isolation (see
+// sedi_time_kernels): every lane active, no lane stops, no reliable update.
+template <class T, int RBT>
+static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *bytes, char *names, int *count) {
+	typedef typename CfgFor<T, RBT>::type C;
+	cudaStream_t s = c->stream;
+	Global g = {};
+	g.iter = 2;
+	g.active = B->R;
+	g.maxiter = 1 << 30;
+	g.tol = 0.0;
+	g.period = 0;
+	g.nrhs = B->R;
+	*B->gl_host = g;
+	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
+	BTRY(cudaMemsetAsync(B->ls.done, 0, sizeof(int) * B->R, s));
+	BTRY(cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * 20 * B->R, s));
+	OpCgA<T> a;
+	a.ka = (T)c->k.a;
+	a.kb = (T)c->k.b;
+	a.kc = (T)c->k.c;
+	a.iMc = (T)(1.0 / c->k.a);
+	a.p0 = (T *)B->p0;
+	a.p1 = (T *)B->p1;
+	OpCgB<T> bo;
+	bo.ka = (T)c->k.a;
+	bo.kb = (T)c->k.b;
+	bo.kc = (T)c->k.c;
+	bo.iMc = (T)(1.0 / c->k.a);
+	bo.x = (T *)B->x;
+	bo.r = (T *)B->r;
+	bo.mixed = 0;
+	cudaEvent_t e0, e1;
+	BTRY(cudaEventCreate(&e0));
+	BTRY(cudaEventCreate(&e1));
+	const double ts = (double)sizeof(T) * (double)B->elems;
+	for (int k = 0; k < 2; k++) {
+		if (k == 0) launch<C>(c, B, B->gT, B->gridT, B->mapsT, a, s);
+		else launch<C>(c, B, B->gT, B->gridT, B->mapsT, bo, s);
+		BTRY(cudaEventRecord(e0, s));
+		for (int i = 0; i < reps; i++) {
+			if (k == 0) launch<C>(c, B, B->gT, B->gridT, B->mapsT, a, s);
+			else launch<C>(c, B, B->gT, B->gridT, B->mapsT, bo, s);
+		}
+		BTRY(cudaEventRecord(e1, s));
+		BTRY(cudaEventSynchronize(e1));
+		float t = 0.f;
+		BTRY(cudaEventElapsedTime(&t, e0, e1));
+		ms[k] = (double)t / reps;
+		bytes[k] = (k == 0 ? 3.0 : 5.0) * ts;  // A: r, p_old in, p out; B: p, x, r in, x, r out
+		snprintf(names + 32 * k, 32, "%s", k == 0 ? (B->mixed ? "cg_a_fp32" : "cg_a_fp64")
+		                                           : (B->mixed ? "cg_b_fp32" : "cg_b_fp64"));
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	BTRY(cudaGetLastError());
+	if (B->gl_host && cudaMemcpy(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost) == cudaSuccess &&
+	    B->gl_host->err) {
+		c->error = "batched sweep timed out waiting for its data";
+		return SEDI_ERR_CUDA;
+	}
+	*count = 2;
+	return 0;
+}
+
+int batched_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count) {
+	Batched *B = (Batched *)c->batched;
+	if (B->mixed) {
+		switch (B->rbT) {
+		case 4: return time_cg_kernels<float, 4>(c, B, reps, ms, bytes, names, count);
+		default: return time_cg_kernels<float, 8>(c, B, reps, ms, bytes, names, count);
+		}
+	}
+	switch (B->rbT) {
+	case 2: return time_cg_kernels<double, 2>(c, B, reps, ms, bytes, names, count);
+	case 4: return time_cg_kernels<double, 4>(c, B, reps, ms, bytes, names, count);
+	default: return time_cg_kernels<double, 8>(c, B, reps, ms, bytes, names, count);
+	}
+}
+
+int batched_estimate_dev(Ctx *c, int samples, const double *probes_dev, int maxiter, double tol, int ignore_errors,
+                         double *D_dev, double *t_dev, double *q_dev, int *iters, double *errs, int *results) {
+	Batched *B = (Batched *)c->batched;
+	cudaStream_t s = c->stream;
+	const long long n = c->g.n;
+	std::vector<double> fe(B->R);
+	std::vector<int> fi(B->R), res(B->R);
+	int worst = 0;
+	bool first = true;
+	for (int k0 = 0; k0 < samples; k0 += c->batch) {
+		const int nb = samples - k0 < c->batch ? samples - k0 : c->batch;
+		kb_interleave<<<blocks1d(n * B->R), 256, 0, s>>>(n, B->R, B->rbD, nb, probes_dev + (size_t)k0 * n, B->b);
+		BTRY(cudaMemsetAsync(B->mixed ? (void *)B->xh : B->x, 0, B->elems * sizeof(double), s));  // x = 0 (:175)
+		c->launches++;
+		int rc = batched_run_resident(c, nb, maxiter, tol, fe.data(), fi.data(), res.data());
+		if (rc < 0) return rc;
+		for (int j = 0; j < nb; j++) {
+			if (iters) iters[k0 + j] = fi[j];
+			if (errs) errs[k0 + j] = fe[j];
+			if (results) results[k0 + j] = res[j];
+		}
+		kb_accumulate<<<blocks1d(n), 256, 0, s>>>(n, B->rbD, nb, B->mixed ? B->xh : (const double *)B->x, B->b,
+		                                          B->t_acc, B->q_acc, first);
+		c->launches++;
+		first = false;
+		if (rc > worst) worst = rc;
+		if (rc != 0 && !ignore_errors) {
+			for (int j = 0; j < nb; j++)
+				if (res[j] != 0) return res[j];
+		}
+	}
+	if (samples == 0) {
+		BTRY(cudaMemsetAsync(B->t_acc, 0, sizeof(double) * n, s));
+		BTRY(cudaMemsetAsync(B->q_acc, 0, sizeof(double) * n, s));
+	}
+	kb_divide<<<blocks1d(n), 256, 0, s>>>(n, B->t_acc, B->q_acc, D_dev);
+	c->launches++;
+	if (t_dev) BTRY(cudaMemcpyAsync(t_dev, B->t_acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+	if (q_dev) BTRY(cudaMemcpyAsync(q_dev, B->q_acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+	BTRY(cudaStreamSynchronize(s));
+	return worst;
+}
+
 }  // namespace sedi

@@ -70,12 +70,13 @@ sedi_ctx *sedi_create(int solver, long n1, long n2, long n3, double a, double b,
 	c->k.b = b;
 	c->k.c = cc;
 	cudaGetDevice(&c->device);
-	if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+	if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
 		cudaGetLastError();
 		delete h;
 		*err = SEDI_ERR_CUDA;
 		return nullptr;
 	}
+	c->stream = c->own_stream;
 	int rc = plain_form(c) ? plain_alloc(c) : batched_alloc(c);
 	if (rc) {
 		*err = rc;
@@ -90,9 +91,10 @@ void sedi_destroy(sedi_ctx *h) {
 	Ctx *c = &h->c;
 	cudaSetDevice(c->device);
 	if (c->stream) cudaStreamSynchronize(c->stream);
+	if (c->own_stream) cudaStreamSynchronize(c->own_stream);
 	plain_free(c);
 	batched_free(c);
-	if (c->stream) cudaStreamDestroy(c->stream);
+	if (c->own_stream) cudaStreamDestroy(c->own_stream);
 	delete h;
 }
 
@@ -288,6 +290,62 @@ int sedi_estimate_probes(sedi_ctx *h, int samples, const double *probes, int max
 	Ctx *c = &h->c;
 	cudaSetDevice(c->device);
 	return estimate_common(c, samples, 0, probes, maxiter, tol, ignore_errors, D, t, q, iters, errs, results);
+}
+
+int sedi_set_stream(sedi_ctx *h, void *stream) {
+	if (!h) return SEDI_ERR_ARG;
+	Ctx *c = &h->c;
+	c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+	return 0;
+}
+
+int sedi_estimate_dev(sedi_ctx *h, int samples, const double *probes_dev, int maxiter, double tol, int ignore_errors,
+                      double *D_dev, double *t_dev, double *q_dev, int *iters, double *errs, int *results) {
+	if (!h || !D_dev || !probes_dev || samples < 0 || maxiter < 0) return SEDI_ERR_ARG;
+	Ctx *c = &h->c;
+	cudaSetDevice(c->device);
+	if (!plain_form(c))
+		return batched_estimate_dev(c, samples, probes_dev, maxiter, tol, ignore_errors, D_dev, t_dev, q_dev, iters,
+		                            errs, results);
+	const long long n = c->g.n;
+	const size_t bytes = sizeof(double) * (size_t)n;
+	int worst = 0;
+	for (int k = 0; k < samples; k++) {
+		CAPI_TRY(cudaMemcpyAsync(c->b, probes_dev + (size_t)k * n, bytes, cudaMemcpyDeviceToDevice, c->stream));
+		CAPI_TRY(cudaMemsetAsync(c->x, 0, bytes, c->stream));
+		double fe = 0.0;
+		int fi = 0;
+		const int res = plain_solve_resident(c, false, maxiter, tol, &fe, &fi);
+		if (res < 0) return res;
+		if (iters) iters[k] = fi;
+		if (errs) errs[k] = fe;
+		if (results) results[k] = res;
+		int rc = plain_accumulate(c, c->x, c->b, k == 0);
+		if (rc) return rc;
+		if (res != 0 && !ignore_errors) return res;
+		if (res > worst) worst = res;
+	}
+	if (samples == 0) {
+		CAPI_TRY(cudaMemsetAsync(c->t_acc, 0, bytes, c->stream));
+		CAPI_TRY(cudaMemsetAsync(c->q_acc, 0, bytes, c->stream));
+	}
+	int rc = plain_divide(c, D_dev);
+	if (rc) return rc;
+	if (t_dev) CAPI_TRY(cudaMemcpyAsync(t_dev, c->t_acc, bytes, cudaMemcpyDeviceToDevice, c->stream));
+	if (q_dev) CAPI_TRY(cudaMemcpyAsync(q_dev, c->q_acc, bytes, cudaMemcpyDeviceToDevice, c->stream));
+	CAPI_TRY(cudaStreamSynchronize(c->stream));
+	return worst;
+}
+
+int sedi_time_kernels(sedi_ctx *h, int reps, double *ms, double *bytes, char *names, int *count) {
+	if (!h || reps < 1 || !ms || !bytes || !names || !count) return SEDI_ERR_ARG;
+	Ctx *c = &h->c;
+	cudaSetDevice(c->device);
+	if (plain_form(c)) {
+		*count = 0;
+		return SEDI_ERR_UNSUPPORTED;
+	}
+	return batched_time_kernels(c, reps, ms, bytes, names, count);
 }
 
 int sedi_solve_batch(sedi_ctx *h, int nrhs, const double *b, double *x, int maxiter, double tol, double *final_err,

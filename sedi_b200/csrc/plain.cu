@@ -30,26 +30,45 @@ struct IMv {
 __device__ __forceinline__ long long gstride() { return (long long)gridDim.x * blockDim.x; }
 __device__ __forceinline__ long long gstart() { return (long long)blockIdx.x * blockDim.x + threadIdx.x; }
 
+// Sweep launch shape: 32x8 column tiles, i3 split into chunks so that the
+// grid has about 6 blocks per SM.
+struct Launch {
+	dim3 grid;
+	int zc;
+};
+
+static Launch launch_shape(const Geo &g) {
+	const int gx = (g.n1 + kTile1 - 1) / kTile1, gy = (g.n2 + kTile2 - 1) / kTile2;
+	long long want = 148LL * 6;
+	long long nz = (want + (long long)gx * gy - 1) / ((long long)gx * gy);
+	if (nz < 1) nz = 1;
+	if (nz > g.n3) nz = g.n3;
+	const int zc = (int)((g.n3 + nz - 1) / nz);
+	nz = (g.n3 + zc - 1) / zc;
+	Launch l;
+	l.grid = dim3(gx, gy, (unsigned)nz);
+	l.zc = zc;
+	return l;
+}
+
 // ---------------------------------------------------------------------------
 // Setup: r = b - A x (Cg.hpp:119-123), <b,b> (:112-115), <r,r> (:126-129),
 // r_hat = r for BiCGStab (BiCgStab.hpp:153).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_setup(Geo g, Coef k, const double *__restrict__ x,
+__global__ void __launch_bounds__(kThreads) k_setup(Geo g, Coef k, int zc, const double *__restrict__ x,
                                                     const double *__restrict__ b, double *__restrict__ r,
                                                     double *__restrict__ rhat, double *partials, unsigned *ticket,
                                                     SolveState *st, double *hist, double tol, int maxiter,
                                                     int solver) {
 	double v[2] = {0.0, 0.0};
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const Nbr q = neighbours(g, i);
-		const double ax = apply_stencil(k, q, [&](long long j) { return __ldg(x + j); });
+	march(g, k, sweep(g, zc), [&](long long j) { return __ldg(x + j); }, [&](long long i, double, double ax) {
 		const double bi = __ldg(b + i);
-		const double ri = add(mul(1.0, bi), mul(-1.0, ax));  // combine2(1.0, b, -1.0, r, r)
+		const double ri = add(bi, mul(-1.0, ax));  // combine2(1.0, b, -1.0, r, r)
 		r[i] = ri;
 		if (rhat) rhat[i] = ri;
 		v[0] = fma(bi, bi, v[0]);
 		v[1] = fma(ri, ri, v[1]);
-	}
+	});
 	double out[2];
 	if (grid_sum<2>(v, partials, ticket, out) && threadIdx.x == 0) {
 		SolveState s = {};
@@ -91,7 +110,7 @@ __global__ void __launch_bounds__(kThreads) k_setup(Geo g, Coef k, const double 
 // kernel writes the new p.
 // ---------------------------------------------------------------------------
 template <bool VIM>
-__global__ void __launch_bounds__(kThreads) k_cg_a(Geo g, Coef k, IMv<VIM> im, const double *__restrict__ r,
+__global__ void __launch_bounds__(kThreads) k_cg_a(Geo g, Coef k, int zc, IMv<VIM> im, const double *__restrict__ r,
                                                    double *p0, double *p1, double *partials, unsigned *ticket,
                                                    SolveState *st) {
 	if (st->done) return;
@@ -102,20 +121,17 @@ __global__ void __launch_bounds__(kThreads) k_cg_a(Geo g, Coef k, IMv<VIM> im, c
 	double *__restrict__ pnew = (it & 1) ? p1 : p0;
 	auto pn = [&](long long j) {
 		const double uj = mul(__ldg(r + j), im(j));       // u = r .* iM (:175)
-		return first ? uj : add(mul(1.0, uj), mul(beta, __ldg(pold + j)));  // p = 1*u + beta*p (:188)
+		return first ? uj : add(uj, mul(beta, __ldg(pold + j)));  // p = 1*u + beta*p (:188)
 	};
 	double v[2] = {0.0, 0.0};
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const Nbr q = neighbours(g, i);
-		const double pi = pn(i);
-		const double si = apply_stencil(k, q, pn);
+	march(g, k, sweep(g, zc), pn, [&](long long i, double pi, double si) {
 		pnew[i] = pi;
 		v[0] = fma(si, pi, v[0]);
 		if (first) {
 			const double ri = __ldg(r + i);
 			v[1] = fma(ri, mul(ri, im(i)), v[1]);
 		}
-	}
+	});
 	double out[2];
 	if (grid_sum<2>(v, partials, ticket, out) && threadIdx.x == 0) {
 		st->sp = out[0];
@@ -126,7 +142,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_a(Geo g, Coef k, IMv<VIM> im, c
 }
 
 template <bool VIM>
-__global__ void __launch_bounds__(kThreads) k_cg_b(Geo g, Coef k, IMv<VIM> im, double *__restrict__ x,
+__global__ void __launch_bounds__(kThreads) k_cg_b(Geo g, Coef k, int zc, IMv<VIM> im, double *__restrict__ x,
                                                    double *__restrict__ r, const double *p0, const double *p1,
                                                    double *partials, unsigned *ticket, SolveState *st,
                                                    double *hist) {
@@ -135,17 +151,14 @@ __global__ void __launch_bounds__(kThreads) k_cg_b(Geo g, Coef k, IMv<VIM> im, d
 	const double alpha = st->alpha;
 	const double *__restrict__ p = (it & 1) ? p1 : p0;
 	double v[2] = {0.0, 0.0};
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const Nbr q = neighbours(g, i);
-		const double si = apply_stencil(k, q, [&](long long j) { return __ldg(p + j); });
-		const double pi = __ldg(p + i);
-		x[i] = add(mul(1.0, x[i]), mul(alpha, pi));        // :169
-		const double ri = add(mul(1.0, r[i]), mul(-alpha, si));  // :172
+	march(g, k, sweep(g, zc), [&](long long j) { return __ldg(p + j); }, [&](long long i, double pi, double si) {
+		x[i] = add(x[i], mul(alpha, pi));              // :169
+		const double ri = add(r[i], mul(-alpha, si));  // :172
 		r[i] = ri;
-		const double ui = mul(ri, im(i));                  // :175
+		const double ui = mul(ri, im(i));                        // :175
 		v[0] = fma(ri, ui, v[0]);
 		v[1] = fma(ri, ri, v[1]);
-	}
+	});
 	double out[2];
 	if (grid_sum<2>(v, partials, ticket, out) && threadIdx.x == 0) {
 		st->ru_new = out[0];                               // :179-181
@@ -176,18 +189,16 @@ __global__ void __launch_bounds__(kThreads) k_cg_b(Geo g, Coef k, IMv<VIM> im, d
 // ping-pongs (neighbours of w are read while the new w is written).
 // ---------------------------------------------------------------------------
 template <bool VIM>
-__global__ void __launch_bounds__(kThreads) k_pcg_setup(Geo g, Coef k, IMv<VIM> im, const double *__restrict__ r,
-                                                        double *__restrict__ u, double *__restrict__ w,
-                                                        double *__restrict__ zq, double *__restrict__ qq,
-                                                        double *__restrict__ ss, double *__restrict__ pp,
-                                                        double *partials, unsigned *ticket, SolveState *st) {
+__global__ void __launch_bounds__(kThreads) k_pcg_setup(Geo g, Coef k, int zc, IMv<VIM> im,
+                                                        const double *__restrict__ r, double *__restrict__ u,
+                                                        double *__restrict__ w, double *__restrict__ zq,
+                                                        double *__restrict__ qq, double *__restrict__ ss,
+                                                        double *__restrict__ pp, double *partials, unsigned *ticket,
+                                                        SolveState *st) {
 	if (st->done) return;
 	auto uf = [&](long long j) { return mul(__ldg(r + j), im(j)); };
 	double v[3] = {0.0, 0.0, 0.0};
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const Nbr q = neighbours(g, i);
-		const double ui = uf(i);
-		const double wi = apply_stencil(k, q, uf);
+	march(g, k, sweep(g, zc), uf, [&](long long i, double ui, double wi) {
 		const double ri = __ldg(r + i);
 		u[i] = ui;
 		w[i] = wi;
@@ -198,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_setup(Geo g, Coef k, IMv<VIM> 
 		v[0] = fma(ri, ui, v[0]);
 		v[1] = fma(wi, ui, v[1]);
 		v[2] = fma(ri, ri, v[2]);
-	}
+	});
 	double out[3];
 	if (grid_sum<3>(v, partials, ticket, out) && threadIdx.x == 0) {
 		st->gamma = out[0];
@@ -211,7 +222,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_setup(Geo g, Coef k, IMv<VIM> 
 }
 
 template <bool VIM>
-__global__ void __launch_bounds__(kThreads) k_pcg_iter(Geo g, Coef k, IMv<VIM> im, double *__restrict__ x,
+__global__ void __launch_bounds__(kThreads) k_pcg_iter(Geo g, Coef k, int zc, IMv<VIM> im, double *__restrict__ x,
                                                        double *__restrict__ r, double *__restrict__ u, double *w0,
                                                        double *w1, double *__restrict__ qv, double *__restrict__ sv,
                                                        double *__restrict__ pv, double *__restrict__ zv,
@@ -232,20 +243,17 @@ __global__ void __launch_bounds__(kThreads) k_pcg_iter(Geo g, Coef k, IMv<VIM> i
 	double *__restrict__ wn = st->wsel ? w0 : w1;
 	auto mf = [&](long long j) { return mul(__ldg(wc + j), im(j)); };
 	double v[3] = {0.0, 0.0, 0.0};
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const Nbr q = neighbours(g, i);
-		const double ni = apply_stencil(k, q, mf);
+	march(g, k, sweep(g, zc), mf, [&](long long i, double mi, double ni) {
 		const double wi = __ldg(wc + i);
-		const double mi = mul(wi, im(i));
-		const double qi = add(mul(1.0, mi), mul(beta, qv[i]));   // :200
-		const double si = add(mul(1.0, wi), mul(beta, sv[i]));   // :203
+		const double qi = add(mi, mul(beta, qv[i]));   // :200
+		const double si = add(wi, mul(beta, sv[i]));   // :203
 		const double ui0 = u[i];
-		const double pi = add(mul(1.0, ui0), mul(beta, pv[i]));  // :206
-		const double zi = add(mul(1.0, ni), mul(beta, zv[i]));   // :209
-		const double ri = add(mul(1.0, r[i]), mul(-alpha, si));  // :212
-		const double xi = add(mul(1.0, x[i]), mul(alpha, pi));   // :215
-		const double ui = add(mul(1.0, ui0), mul(-alpha, qi));   // :218
-		const double wni = add(mul(1.0, wi), mul(-alpha, zi));   // :221
+		const double pi = add(ui0, mul(beta, pv[i]));  // :206
+		const double zi = add(ni, mul(beta, zv[i]));   // :209
+		const double ri = add(r[i], mul(-alpha, si));  // :212
+		const double xi = add(x[i], mul(alpha, pi));   // :215
+		const double ui = add(ui0, mul(-alpha, qi));   // :218
+		const double wni = add(wi, mul(-alpha, zi));   // :221
 		qv[i] = qi;
 		sv[i] = si;
 		pv[i] = pi;
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(kThreads) k_pcg_iter(Geo g, Coef k, IMv<VIM> i
 		v[0] = fma(ri, ui, v[0]);   // next gamma  = <r,u>
 		v[1] = fma(wni, ui, v[1]);  // next delta  = <w,u>
 		v[2] = fma(ri, ri, v[2]);   // next <r,r>
-	}
+	});
 	double out[3];
 	if (grid_sum<3>(v, partials, ticket, out) && threadIdx.x == 0) {
 		// The stop test uses <r,r> from the top of this iteration (:173, :227).
@@ -297,10 +305,10 @@ __global__ void __launch_bounds__(kThreads) k_pcg_iter(Geo g, Coef k, IMv<VIM> i
 // written).  s, s_hat, t are never stored.
 // ---------------------------------------------------------------------------
 template <bool VIM>
-__global__ void __launch_bounds__(kThreads) k_bicg_1(Geo g, Coef k, IMv<VIM> im, const double *r0, const double *r1,
-                                                     const double *__restrict__ rhat, double *p0, double *p1,
-                                                     double *v0, double *v1, double *partials, unsigned *ticket,
-                                                     SolveState *st) {
+__global__ void __launch_bounds__(kThreads) k_bicg_1(Geo g, Coef k, int zc, IMv<VIM> im, const double *r0,
+                                                     const double *r1, const double *__restrict__ rhat, double *p0,
+                                                     double *p1, double *v0, double *v1, double *partials,
+                                                     unsigned *ticket, SolveState *st) {
 	if (st->done) return;
 	const int it = st->iter;
 	const bool first = (it == 1);
@@ -318,18 +326,15 @@ __global__ void __launch_bounds__(kThreads) k_bicg_1(Geo g, Coef k, IMv<VIM> im,
 	double *__restrict__ vnew = (it & 1) ? v1 : v0;
 	auto pf = [&](long long j) {
 		const double rj = __ldg(r + j);
-		return first ? rj : add(add(mul(1.0, rj), mul(beta, __ldg(pold + j))), mul(bo, __ldg(vold + j)));  // :168
+		return first ? rj : add(add(rj, mul(beta, __ldg(pold + j))), mul(bo, __ldg(vold + j)));  // :168
 	};
 	auto phf = [&](long long j) { return mul(pf(j), im(j)); };  // :175
 	double v[1] = {0.0};
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const Nbr q = neighbours(g, i);
-		const double pi = pf(i);
-		const double vi = apply_stencil(k, q, phf);  // :178-180
-		pnew[i] = pi;
+	march(g, k, sweep(g, zc), phf, [&](long long i, double, double vi) {  // v = A p_hat (:178-180)
+		pnew[i] = pf(i);
 		vnew[i] = vi;
 		v[0] = fma(vi, __ldg(rhat + i), v[0]);
-	}
+	});
 	double out[1];
 	if (grid_sum<1>(v, partials, ticket, out) && threadIdx.x == 0) {
 		st->vr = out[0];
@@ -338,25 +343,23 @@ __global__ void __launch_bounds__(kThreads) k_bicg_1(Geo g, Coef k, IMv<VIM> im,
 }
 
 template <bool VIM>
-__global__ void __launch_bounds__(kThreads) k_bicg_2(Geo g, Coef k, IMv<VIM> im, const double *r0, const double *r1,
-                                                     const double *v0, const double *v1, double *partials,
-                                                     unsigned *ticket, SolveState *st) {
+__global__ void __launch_bounds__(kThreads) k_bicg_2(Geo g, Coef k, int zc, IMv<VIM> im, const double *r0,
+                                                     const double *r1, const double *v0, const double *v1,
+                                                     double *partials, unsigned *ticket, SolveState *st) {
 	if (st->done) return;
 	const int it = st->iter;
 	const double alpha = st->alpha;
 	const double *__restrict__ r = st->wsel ? r1 : r0;
 	const double *__restrict__ vv = (it & 1) ? v1 : v0;
-	auto sf = [&](long long j) { return add(mul(1.0, __ldg(r + j)), mul(-alpha, __ldg(vv + j))); };  // :189
+	auto sf = [&](long long j) { return add(__ldg(r + j), mul(-alpha, __ldg(vv + j))); };  // :189
 	auto shf = [&](long long j) { return mul(sf(j), im(j)); };                                        // :201
 	double v[3] = {0.0, 0.0, 0.0};
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const Nbr q = neighbours(g, i);
+	march(g, k, sweep(g, zc), shf, [&](long long i, double, double ti) {  // t = A s_hat (:204-206)
 		const double si = sf(i);
-		const double ti = apply_stencil(k, q, shf);  // :204-206
 		v[0] = fma(si, si, v[0]);
 		v[1] = fma(ti, si, v[1]);
 		v[2] = fma(ti, ti, v[2]);
-	}
+	});
 	double out[3];
 	if (grid_sum<3>(v, partials, ticket, out) && threadIdx.x == 0) {
 		st->s_norm2 = out[0];  // :192-193
@@ -372,7 +375,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_2(Geo g, Coef k, IMv<VIM> im,
 }
 
 template <bool VIM>
-__global__ void __launch_bounds__(kThreads) k_bicg_3(Geo g, Coef k, IMv<VIM> im, double *__restrict__ x,
+__global__ void __launch_bounds__(kThreads) k_bicg_3(Geo g, Coef k, int zc, IMv<VIM> im, double *__restrict__ x,
                                                      double *r0, double *r1, const double *__restrict__ rhat,
                                                      const double *p0, const double *p1, const double *v0,
                                                      const double *v1, double *partials, unsigned *ticket,
@@ -386,24 +389,21 @@ __global__ void __launch_bounds__(kThreads) k_bicg_3(Geo g, Coef k, IMv<VIM> im,
 	double *__restrict__ rn = sel ? r0 : r1;
 	const double *__restrict__ p = (it & 1) ? p1 : p0;
 	const double *__restrict__ vv = (it & 1) ? v1 : v0;
-	auto sf = [&](long long j) { return add(mul(1.0, __ldg(r + j)), mul(-alpha, __ldg(vv + j))); };
+	auto sf = [&](long long j) { return add(__ldg(r + j), mul(-alpha, __ldg(vv + j))); };
 	auto shf = [&](long long j) { return mul(sf(j), im(j)); };
 	double v[2] = {0.0, 0.0};
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const double phi = mul(__ldg(p + i), im(i));  // p_hat
-		if (s_exit) {
-			x[i] = add(mul(1.0, x[i]), mul(alpha, phi));  // :196
-			continue;
-		}
-		const Nbr q = neighbours(g, i);
-		const double si = sf(i);
-		const double shi = mul(si, im(i));
-		const double ti = apply_stencil(k, q, shf);
-		x[i] = add(add(mul(1.0, x[i]), mul(alpha, phi)), mul(omega, shi));  // :216
-		const double ri = add(mul(1.0, si), mul(-omega, ti));                 // :219
-		rn[i] = ri;
-		v[0] = fma(ri, ri, v[0]);
-		v[1] = fma(ri, __ldg(rhat + i), v[1]);
+	const Sweep w = sweep(g, zc);
+	if (s_exit) {
+		visit(g, w, [&](long long i) { x[i] = add(x[i], mul(alpha, mul(__ldg(p + i), im(i)))); });  // :196
+	} else {
+		march(g, k, w, shf, [&](long long i, double shi, double ti) {
+			const double phi = mul(__ldg(p + i), im(i));                          // p_hat
+			x[i] = add(add(x[i], mul(alpha, phi)), mul(omega, shi));  // :216
+			const double ri = add(sf(i), mul(-omega, ti));            // :219
+			rn[i] = ri;
+			v[0] = fma(ri, ri, v[0]);
+			v[1] = fma(ri, __ldg(rhat + i), v[1]);
+		});
 	}
 	double out[2];
 	if (grid_sum<2>(v, partials, ticket, out) && threadIdx.x == 0) {
@@ -449,12 +449,10 @@ __global__ void __launch_bounds__(kThreads) k_bicg_3(Geo g, Coef k, IMv<VIM> im,
 // Utility kernels: y = A x, accumulators (SliceOps::accumulate_product,
 // SliceOps.hpp:96-108), D = t ./ q (SliceOps::divide, :68-79).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_stencil(Geo g, Coef k, const double *__restrict__ x,
+__global__ void __launch_bounds__(kThreads) k_stencil(Geo g, Coef k, int zc, const double *__restrict__ x,
                                                       double *__restrict__ y) {
-	for (long long i = gstart(); i < g.n; i += gstride()) {
-		const Nbr q = neighbours(g, i);
-		y[i] = apply_stencil(k, q, [&](long long j) { return __ldg(x + j); });
-	}
+	march(g, k, sweep(g, zc), [&](long long j) { return __ldg(x + j); },
+	      [&](long long i, double, double yi) { y[i] = yi; });
 }
 
 __global__ void __launch_bounds__(kThreads) k_accumulate(long long n, const double *__restrict__ x,
@@ -504,7 +502,9 @@ int plain_alloc(Ctx *c) {
 			return SEDI_ERR_NOMEM;
 		}
 	}
-	SEDI_TRY(cudaMalloc(&c->partials, sizeof(double) * kMaxDots * c->nblocks));
+	const Launch l = launch_shape(c->g);
+	const size_t sweep_blocks = (size_t)l.grid.x * l.grid.y * l.grid.z;
+	SEDI_TRY(cudaMalloc(&c->partials, sizeof(double) * kMaxDots * (sweep_blocks > (size_t)c->nblocks ? sweep_blocks : (size_t)c->nblocks)));
 	SEDI_TRY(cudaMalloc(&c->ticket, sizeof(unsigned)));
 	SEDI_TRY(cudaMemset(c->ticket, 0, sizeof(unsigned)));
 	SEDI_TRY(cudaMalloc(&c->st, sizeof(SolveState)));
@@ -530,24 +530,26 @@ void plain_free(Ctx *c) {
 // Enqueue one iteration of the context's solver (kernels early-exit once done).
 template <bool VIM>
 static void enqueue_iteration(Ctx *c, IMv<VIM> im) {
-	const int nb = c->nblocks;
+	const Launch l = launch_shape(c->g);
+	const dim3 nb = l.grid;
+	const int zc = l.zc;
 	cudaStream_t s = c->stream;
 	if (c->solver == 2) {
-		k_cg_a<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, im, c->r, c->p[0], c->p[1], c->partials, c->ticket, c->st);
-		k_cg_b<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, im, c->x, c->r, c->p[0], c->p[1], c->partials, c->ticket,
+		k_cg_a<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, zc, im, c->r, c->p[0], c->p[1], c->partials, c->ticket, c->st);
+		k_cg_b<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, zc, im, c->x, c->r, c->p[0], c->p[1], c->partials, c->ticket,
 		                                     c->st, c->hist);
 		c->launches += 2;
 	} else if (c->solver == 3) {
-		k_pcg_iter<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, im, c->x, c->r, c->u, c->w[0], c->w[1], c->q, c->s,
+		k_pcg_iter<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, zc, im, c->x, c->r, c->u, c->w[0], c->w[1], c->q, c->s,
 		                                         c->p[0], c->z, c->partials, c->ticket, c->st, c->hist);
 		c->launches += 1;
 	} else {
 		// BiCGStab keeps r in r (sel 0) / p[1]-free buffer pair: r0 = c->r, r1 = c->u.
-		k_bicg_1<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, im, c->r, c->u, c->rhat, c->p[0], c->p[1], c->v[0],
+		k_bicg_1<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, zc, im, c->r, c->u, c->rhat, c->p[0], c->p[1], c->v[0],
 		                                       c->v[1], c->partials, c->ticket, c->st);
-		k_bicg_2<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, im, c->r, c->u, c->v[0], c->v[1], c->partials,
+		k_bicg_2<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, zc, im, c->r, c->u, c->v[0], c->v[1], c->partials,
 		                                       c->ticket, c->st);
-		k_bicg_3<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, im, c->x, c->r, c->u, c->rhat, c->p[0], c->p[1],
+		k_bicg_3<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, zc, im, c->x, c->r, c->u, c->rhat, c->p[0], c->p[1],
 		                                       c->v[0], c->v[1], c->partials, c->ticket, c->st, c->hist);
 		c->launches += 3;
 	}
@@ -631,15 +633,17 @@ static int finish_result(const Ctx *c, const SolveState &s, double *final_err, i
 
 template <bool VIM>
 static int solve_impl(Ctx *c, IMv<VIM> im, int maxiter, double tol, double *final_err, int *final_iter) {
-	const int nb = c->nblocks;
+	const Launch l = launch_shape(c->g);
+	const dim3 nb = l.grid;
+	const int zc = l.zc;
 	cudaStream_t s = c->stream;
 	int rc = ensure_hist(c, maxiter);
 	if (rc) return rc;
-	k_setup<<<nb, kThreads, 0, s>>>(c->g, c->k, c->x, c->b, c->r, c->solver == 1 ? c->rhat : nullptr,
+	k_setup<<<nb, kThreads, 0, s>>>(c->g, c->k, zc, c->x, c->b, c->r, c->solver == 1 ? c->rhat : nullptr,
 	                                c->partials, c->ticket, c->st, c->hist, tol, maxiter, c->solver);
 	c->launches++;
 	if (c->solver == 3) {
-		k_pcg_setup<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, im, c->r, c->u, c->w[0], c->z, c->q, c->s, c->p[0],
+		k_pcg_setup<VIM><<<nb, kThreads, 0, s>>>(c->g, c->k, zc, im, c->r, c->u, c->w[0], c->z, c->q, c->s, c->p[0],
 		                                          c->partials, c->ticket, c->st);
 		c->launches++;
 	}
@@ -692,7 +696,8 @@ int plain_solve_dev(Ctx *c, const double *b, double *x, const double *iM, int ma
 }
 
 int plain_stencil(Ctx *c, const double *x_dev, double *y_dev) {
-	k_stencil<<<blocks_for(c->g.n), kThreads, 0, c->stream>>>(c->g, c->k, x_dev, y_dev);
+	const Launch l = launch_shape(c->g);
+	k_stencil<<<l.grid, kThreads, 0, c->stream>>>(c->g, c->k, l.zc, x_dev, y_dev);
 	c->launches++;
 	SEDI_TRY(cudaGetLastError());
 	return 0;

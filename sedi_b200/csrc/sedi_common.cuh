@@ -42,6 +42,65 @@ __device__ __forceinline__ double stencil7(const Coef &k, double xc, double xm1,
 	return y;
 }
 
+// ---------------------------------------------------------------------------
+// 2.5-D sweep.  A block of 256 threads covers a 32 (i1) x 8 (i2) column tile
+// and marches along i3 over [z0, z1); each thread keeps the stencil input at
+// i3-1, i3 and i3+1 of its own column in registers, so per point it loads
+// the i3+1 value and its four in-plane neighbours (L1/L2 hits) and needs no
+// index division.  Block -> work assignment depends only on the grid, so the
+// reductions below are bitwise reproducible.
+// ---------------------------------------------------------------------------
+constexpr int kTile1 = 32, kTile2 = 8;
+
+struct Sweep {
+	int i1, i2, z0, z1;
+	bool active;
+	long long base;  // index of (i1, i2, 0)
+	long long s2, s3;
+};
+
+__device__ __forceinline__ Sweep sweep(const Geo &g, int zchunk) {
+	Sweep w;
+	w.i1 = blockIdx.x * kTile1 + (threadIdx.x & (kTile1 - 1));
+	w.i2 = blockIdx.y * kTile2 + (threadIdx.x / kTile1);
+	w.z0 = blockIdx.z * zchunk;
+	w.z1 = min(w.z0 + zchunk, g.n3);
+	w.active = w.i1 < g.n1 && w.i2 < g.n2 && w.z0 < w.z1;
+	w.s2 = g.n1;
+	w.s3 = (long long)g.n1 * g.n2;
+	w.base = w.i1 + (long long)w.i2 * w.s2;
+	return w;
+}
+
+// Stencil of the field f (value at an in-grid index) over the sweep; calls
+// op(index, f(index), (A f)(index)) at every point of the thread's column.
+template <class F, class Op>
+__device__ __forceinline__ void march(const Geo &g, const Coef &k, const Sweep &w, F f, Op op) {
+	if (!w.active) return;
+	const bool m1 = w.i1 > 0, p1 = w.i1 < g.n1 - 1, m2 = w.i2 > 0, p2 = w.i2 < g.n2 - 1;
+	long long i = w.base + (long long)w.z0 * w.s3;
+	double prev = w.z0 > 0 ? f(i - w.s3) : 0.0;
+	double cur = f(i);
+	for (int i3 = w.z0; i3 < w.z1; i3++, i += w.s3) {
+		const double next = (i3 + 1 < g.n3) ? f(i + w.s3) : 0.0;
+		const double xm1 = m1 ? f(i - 1) : 0.0;
+		const double xm2 = m2 ? f(i - w.s2) : 0.0;
+		const double xp1 = p1 ? f(i + 1) : 0.0;
+		const double xp2 = p2 ? f(i + w.s2) : 0.0;
+		op(i, cur, stencil7(k, cur, xm1, xm2, prev, xp1, xp2, next));
+		prev = cur;
+		cur = next;
+	}
+}
+
+// Pointwise visit of the sweep's column (no stencil).
+template <class Op>
+__device__ __forceinline__ void visit(const Geo &g, const Sweep &w, Op op) {
+	if (!w.active) return;
+	long long i = w.base + (long long)w.z0 * w.s3;
+	for (int i3 = w.z0; i3 < w.z1; i3++, i += w.s3) op(i);
+}
+
 // Point index -> neighbour validity and offsets.
 struct Nbr {
 	long long i;
@@ -120,13 +179,15 @@ template <int ND>
 __device__ bool grid_sum(double (&v)[ND], double *partials, unsigned int *ticket, double (&out)[ND]) {
 	__shared__ double sh[32][ND];
 	__shared__ bool last;
+	const unsigned int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+	const unsigned int nblk = gridDim.x * gridDim.y * gridDim.z;
 	block_sum<ND>(v, sh);
 	if (threadIdx.x == 0) {
 #pragma unroll
-		for (int d = 0; d < ND; d++) partials[(size_t)blockIdx.x * ND + d] = v[d];
+		for (int d = 0; d < ND; d++) partials[(size_t)bid * ND + d] = v[d];
 		__threadfence();
 		const unsigned int t = atomicAdd(ticket, 1u);
-		last = (t == gridDim.x - 1);
+		last = (t == nblk - 1);
 	}
 	__syncthreads();
 	if (!last) return false;
@@ -134,7 +195,7 @@ __device__ bool grid_sum(double (&v)[ND], double *partials, unsigned int *ticket
 	double w[ND];
 #pragma unroll
 	for (int d = 0; d < ND; d++) w[d] = 0.0;
-	for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+	for (unsigned int b = threadIdx.x; b < nblk; b += blockDim.x)
 #pragma unroll
 		for (int d = 0; d < ND; d++) w[d] += __ldcg(&partials[(size_t)b * ND + d]);
 	block_sum<ND>(w, sh);

@@ -55,7 +55,8 @@ struct Ctx {
 	Geo g;
 	Coef k;
 	int device;
-	cudaStream_t stream;
+	cudaStream_t stream;      // stream the context's work runs on
+	cudaStream_t own_stream;  // the context's own stream
 	int nblocks;
 
 	// single-vector FP64 buffers (n doubles each)
@@ -100,6 +101,7 @@ int batched_solve_dev(Ctx *c, int nrhs, const double *b, double *x, int maxiter,
 int batched_estimate_dev(Ctx *c, int samples, const double *probes_dev, int maxiter, double tol,
                          int ignore_errors, double *D_dev, double *t_dev, double *q_dev, int *iters,
                          double *errs, int *results);
+int batched_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count);
 
 // rng.cu
 void host_fill_probe(uint32_t seed, long n, double *out);

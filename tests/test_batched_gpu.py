@@ -1,0 +1,119 @@
+"""Batched (RHS-interleaved) forms through the C ABI.
+
+FP64 batched: the reference method lane by lane -- every right-hand side must
+reproduce the single-vector FP64 path and the reference (same iteration
+counts, x within 1e-10 relative max-norm: elementwise rounding is the
+reference's, only dot-product summation order differs).
+
+MIXED (FP32 vectors + FP64 reliable update): every right-hand side must meet
+the reference's stopping test on its FP64 TRUE residual,
+sqrt(<b-Ax, b-Ax>/<b,b>) <= tol (checked here on the CPU with the oracle's
+stencil), and the estimated diagonal must stay within 1e-8 relative
+max-norm of the FP64 answer on the same probes.
+"""
+import numpy as np
+import pytest
+
+import _oracle as O
+import sedi_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+
+def true_err(dims, x, b):
+    r = b - O.stencil(dims, x)
+    bb = float(b @ b) or 1.0
+    return np.sqrt(float(r @ r) / bb)
+
+
+@pytest.mark.parametrize("nrhs", [1, 3, 16, 64])
+def test_fp64_batch_matches_single_vector(nrhs):
+    dims = (20, 18, 16)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(1234 + k, n) for k in range(nrhs)])
+    X = np.zeros_like(B)
+    with S.Context("cg", dims, batch=nrhs) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=1000, tol=1e-9)
+    for k in range(nrhs):
+        rc0, fe0, fi0, x0, _ = O.solve(2, dims, B[k], maxiter=1000, tol=1e-9)
+        assert (res[k], fi[k]) == (rc0, fi0)
+        assert O.relmax(X[k], x0) <= 1e-10
+        assert abs(fe[k] - fe0) <= 1e-10 * fe0 + 1e-15
+
+
+def test_fp64_batch_fixed_iterations():
+    dims = (24, 20, 16)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(99 + k, n) for k in range(5)])
+    X = np.zeros_like(B)
+    with S.Context("cg", dims, batch=8) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=200, tol=0.0)
+    for k in range(5):
+        rc0, fe0, fi0, x0, _ = O.solve(2, dims, B[k], maxiter=200, tol=0.0)
+        assert (res[k], fi[k]) == (rc0, fi0) == (1, 200)
+        assert O.relmax(X[k], x0) <= 1e-10
+
+
+def test_fp64_batch_estimator_vs_reference():
+    g = O.golden("cfg1_cg_32")
+    m = g["meta"]
+    with S.Context("cg", m["grid"], batch=8) as c:
+        r = c.estimate(m["samples"], m["seed"], m["maxiter"], m["tol"])
+    assert np.array_equal(r["iters"], g["iters"]) and np.array_equal(r["results"], g["results"])
+    assert O.relmax(r["D"], g["D"]) <= 1e-10
+    assert np.array_equal(r["q"], g["q"])
+
+
+@pytest.mark.parametrize("nrhs,tol", [(4, 1e-9), (16, 1e-9), (64, 1e-10), (128, 1e-9)])
+def test_mixed_batch_true_residual(nrhs, tol):
+    dims = (24, 22, 20)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(7 + k, n) for k in range(nrhs)])
+    X = np.zeros_like(B)
+    with S.Context("cg", dims, precision=S.MIXED, batch=nrhs) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=2000, tol=tol)
+    assert np.all(res == 0)
+    fi64 = []
+    for k in range(nrhs):
+        e = true_err(dims, X[k], B[k])
+        assert e <= tol * 1.0000001, (k, e)
+        assert abs(fe[k] - e) <= 1e-3 * e + 1e-16  # reported err is the FP64 true residual
+        if k < 4:
+            fi64.append(O.solve(2, dims, B[k], maxiter=2000, tol=tol)[2])
+    # Mixed precision may need a few more iterations than FP64, not many.
+    assert np.all(fi[: len(fi64)] <= np.array(fi64) * 1.25 + 10)
+
+
+def test_mixed_estimator_diagonal_error():
+    dims = (32, 32, 32)
+    samples = 16
+    with S.Context("cg", dims, batch=samples) as c64:
+        r64 = c64.estimate(samples, 1234, 2000, 1e-9)
+    with S.Context("cg", dims, precision=S.MIXED, batch=samples) as cm:
+        rm = cm.estimate(samples, 1234, 2000, 1e-9)
+    assert np.all(rm["results"] == 0)
+    assert O.relmax(rm["D"], r64["D"]) <= 1e-8, O.relmax(rm["D"], r64["D"])
+
+
+def test_mixed_maxiter_reports_result_1():
+    dims = (16, 16, 16)
+    n = 16 ** 3
+    B = np.stack([O.fill_probe(3 + k, n) for k in range(4)])
+    X = np.zeros_like(B)
+    with S.Context("cg", dims, precision=S.MIXED, batch=4) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=7, tol=1e-14)
+    assert np.all(res == 1) and np.all(fi == 7)
+    for k in range(4):
+        assert abs(fe[k] - true_err(dims, X[k], B[k])) <= 1e-3 * fe[k]
+
+
+def test_batch_padding_lanes_and_zero_rhs():
+    dims = (12, 10, 8)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(11, n), np.zeros(n), O.fill_probe(12, n)])
+    for prec in (S.FP64, S.MIXED):
+        X = np.zeros_like(B)
+        with S.Context("cg", dims, precision=prec, batch=7) as c:
+            res, fe, fi = c.solve_batch(X, B, maxiter=500, tol=1e-10)
+        assert np.all(res == 0)
+        assert fi[1] == 0 and fe[1] == 0.0 and np.all(X[1] == 0.0)
