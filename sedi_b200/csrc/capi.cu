@@ -94,6 +94,8 @@ void sedi_destroy(sedi_ctx *h) {
 	if (c->own_stream) cudaStreamSynchronize(c->own_stream);
 	plain_free(c);
 	batched_free(c);
+	if (c->stage_probes) cudaFree(c->stage_probes);
+	if (c->stage_out) cudaFree(c->stage_out);
 	if (c->own_stream) cudaStreamDestroy(c->own_stream);
 	delete h;
 }
@@ -192,40 +194,43 @@ static int estimate_common(Ctx *c, int samples, uint32_t seed, const double *pro
 	const long long n = c->g.n;
 	const size_t bytes = sizeof(double) * (size_t)n;
 	if (!plain_form(c)) {
-		// Batched form: stage the probes on the device and run them as right-hand sides.
-		double *dprobes = nullptr, *dD = nullptr, *dt = nullptr, *dq = nullptr;
-		int rc = 0;
-		if (cudaMalloc(&dprobes, bytes * (size_t)(samples > 0 ? samples : 1)) != cudaSuccess ||
-		    cudaMalloc(&dD, bytes) != cudaSuccess || cudaMalloc(&dt, bytes) != cudaSuccess ||
-		    cudaMalloc(&dq, bytes) != cudaSuccess) {
-			cudaGetLastError();
-			rc = SEDI_ERR_NOMEM;
-			c->error = "device allocation failed";
-		}
-		std::vector<double> tmp;
-		for (int k = 0; !rc && k < samples; k++) {
-			const double *src = probes ? probes + (size_t)k * n : nullptr;
-			if (!src) {
-				tmp.resize((size_t)n);
-				host_fill_probe(seed + (uint32_t)k, (long)n, tmp.data());
-				src = tmp.data();
+		// Batched form: stage the probes in a context-owned device buffer
+		// (reused across calls), run them as right-hand sides, copy D (t, q) back.
+		const size_t need = bytes * (size_t)(samples > 0 ? samples : 1);
+		if (c->stage_probe_bytes < need) {
+			if (c->stage_probes) cudaFree(c->stage_probes);
+			c->stage_probes = nullptr;
+			c->stage_probe_bytes = 0;
+			if (cudaMalloc(&c->stage_probes, need) != cudaSuccess) {
+				cudaGetLastError();
+				c->error = "device allocation failed (probe staging)";
+				return SEDI_ERR_NOMEM;
 			}
-			if (cudaMemcpy(dprobes + (size_t)k * n, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-				rc = set_cuda_error(c, cudaGetLastError(), "probe upload");
+			c->stage_probe_bytes = need;
 		}
-		if (!rc)
-			rc = batched_estimate_dev(c, samples, dprobes, maxiter, tol, ignore_errors, dD, dt, dq, iters, errs,
-			                          results);
-		if (rc >= 0) {
-			if (cudaMemcpy(D, dD, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
-			    (t && cudaMemcpy(t, dt, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) ||
-			    (q && cudaMemcpy(q, dq, bytes, cudaMemcpyDeviceToHost) != cudaSuccess))
-				rc = set_cuda_error(c, cudaGetLastError(), "result download");
+		if (!c->stage_out && cudaMalloc(&c->stage_out, 3 * bytes) != cudaSuccess) {
+			cudaGetLastError();
+			c->stage_out = nullptr;
+			c->error = "device allocation failed (result staging)";
+			return SEDI_ERR_NOMEM;
 		}
-		cudaFree(dprobes);
-		cudaFree(dD);
-		cudaFree(dt);
-		cudaFree(dq);
+		if (probes) {
+			CAPI_TRY(cudaMemcpyAsync(c->stage_probes, probes, need, cudaMemcpyHostToDevice, c->stream));
+		} else {
+			std::vector<double> tmp((size_t)n);
+			for (int k = 0; k < samples; k++) {
+				host_fill_probe(seed + (uint32_t)k, (long)n, tmp.data());
+				CAPI_TRY(cudaMemcpy(c->stage_probes + (size_t)k * n, tmp.data(), bytes, cudaMemcpyHostToDevice));
+			}
+		}
+		double *dD = c->stage_out, *dt = c->stage_out + n, *dq = c->stage_out + 2 * n;
+		int rc = batched_estimate_dev(c, samples, c->stage_probes, maxiter, tol, ignore_errors, dD, dt, dq, iters,
+		                              errs, results);
+		if (rc < 0) return rc;
+		CAPI_TRY(cudaMemcpyAsync(D, dD, bytes, cudaMemcpyDeviceToHost, c->stream));
+		if (t) CAPI_TRY(cudaMemcpyAsync(t, dt, bytes, cudaMemcpyDeviceToHost, c->stream));
+		if (q) CAPI_TRY(cudaMemcpyAsync(q, dq, bytes, cudaMemcpyDeviceToHost, c->stream));
+		CAPI_TRY(cudaStreamSynchronize(c->stream));
 		return rc;
 	}
 	double *host_probe = nullptr;

@@ -73,6 +73,9 @@ struct Ctx {
 
 	// estimator accumulators (n doubles)
 	double *t_acc, *q_acc;
+	// host-facing estimator staging (batched form): probes, D, t, q on the device
+	double *stage_probes, *stage_out;
+	size_t stage_probe_bytes;
 
 	void *batched;  // batched-form state (batched.cu)
 
