@@ -146,6 +146,27 @@ int sedi_set_stream(sedi_ctx *ctx, void *stream);
  */
 int sedi_time_kernels(sedi_ctx *ctx, int reps, double *ms, double *bytes, char *names, int *count);
 
+/*
+ * Residual without device allocation.  No counterpart in the reference: it
+ * is for callers that cannot allocate device memory where they need a
+ * residual check (memory pools or arenas that own all device memory,
+ * allocation-free serving loops, host frameworks with their own allocator).
+ * Computes r = b - A x with zero ghosts (x_dev, b_dev inputs, r_dev output;
+ * device pointers, n1*n2*n3 doubles, i1 fastest) and *err_out (host) =
+ * sqrt(<r,r>/<b,b>) with <b,b> taken as 1 when it is 0, the solvers' initial
+ * residual test.  Runs on `stream` (a cudaStream_t as void*, NULL = default
+ * stream) and returns after the result is on the host.
+ * Scratch: a fixed device array in the library (about 64 KiB per GPU, held
+ * until the process exits) -- nothing is allocated per call.  Limit: the
+ * grid's sweep may use at most 4096 thread blocks, which holds whenever
+ * ceil(n1/32)*ceil(n2/8) <= 4096 (any n3); larger grids return SEDI_ERR_ARG.
+ * The first call on a device looks up the array's device address, so make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (different streams or threads) race.
+ */
+int sedi_residual_noalloc(long n1, long n2, long n3, double a, double b, double c, const double *x_dev,
+                          const double *b_dev, double *r_dev, double *err_out, void *stream);
+
 /* Host probe generator, bit-identical to DistrRngStd with std::mt19937(seed). */
 void sedi_fill_probe(uint32_t seed, long n, double *out);
 

@@ -84,6 +84,7 @@ def load():
     lib.sedi_estimate_dev.argtypes = [vp, c_int, vp, c_int, c_double, c_int, vp, vp, vp, vp, vp, vp]
     lib.sedi_set_stream.argtypes = [vp, vp]
     lib.sedi_time_kernels.argtypes = [vp, c_int, vp, vp, vp, vp]
+    lib.sedi_residual_noalloc.argtypes = [c_long, c_long, c_long, c_double, c_double, c_double, vp, vp, vp, pd, vp]
     _lib = lib
     return lib
 
