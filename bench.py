@@ -52,7 +52,20 @@ def parse():
     ap.add_argument("--impl", choices=["sedi", "reference"], default="sedi")
     ap.add_argument("--form", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    # Small cases for profiler captures (not the benchmark configuration):
+    ap.add_argument("--grid", default=None, help="override the grid, e.g. 128x128x64")
+    ap.add_argument("--maxiter", type=int, default=None, help="override maxiter (with --tol 0: fixed iterations)")
+    ap.add_argument("--tol", type=float, default=None)
+    ap.add_argument("--no-extras", action="store_true", help="skip e2e, kernel timing, accuracy and other forms")
+    a = ap.parse_args()
+    global GRID, MAXITER, TOL
+    if a.grid:
+        GRID = tuple(int(v) for v in a.grid.split("x"))
+    if a.maxiter is not None:
+        MAXITER = a.maxiter
+    if a.tol is not None:
+        TOL = a.tol
+    return a
 
 
 def dist_env():
@@ -270,7 +283,18 @@ def run_sedi(args):
     ms = float(tmax.item())
     value = world * SAMPLES * args.steps / (ms / 1e3)
     it_all = np.concatenate(iters)
-    assert np.all(res["results"] == 0), "a probe did not converge"
+    if TOL > 0:
+        assert np.all(res["results"] == 0), "a probe did not converge"
+    if args.no_extras:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                              "ms_per_step": ms / args.steps, "grid": list(GRID), "maxiter": MAXITER, "tol": TOL,
+                              "gpu_launches": launches, "note": "profiling case, not the benchmark configuration"}),
+                  flush=True)
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # End to end through the C ABI: pinned host probes in, host D out, per step.
     Dh = np.empty(n)

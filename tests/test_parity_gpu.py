@@ -128,10 +128,11 @@ def test_full_128_checksums_vs_reference(solver):
     assert np.array_equal(r["results"], g["results"])
     if solver == "bicgstab":
         # Two builds of the reference itself (contracted vs uncontracted FP)
-        # differ by up to 11% per probe in BiCGStab iterations at 128^3 and
-        # by 2e-7 in D after four probes.
-        assert np.all(np.abs(r["iters"] - g["iters"]) <= np.ceil(0.2 * g["iters"]) + 1)
-        assert abs(r["iters"].mean() - g["iters"].mean()) <= 0.05 * g["iters"].mean()
+        # differ by up to 11% per probe in BiCGStab iterations at 128^3 over
+        # four probes and by 2e-7 in D; over 64 probes single probes move by
+        # up to ~25% while the mean holds to ~1%.
+        assert np.all(np.abs(r["iters"] - g["iters"]) <= np.ceil(0.3 * g["iters"]) + 1)
+        assert abs(r["iters"].mean() - g["iters"].mean()) <= 0.03 * g["iters"].mean()
         tol = 1e-6
     else:
         assert np.array_equal(r["iters"], g["iters"])
