@@ -181,6 +181,10 @@ int sedi_stencil_apply(sedi_ctx *ctx, const double *x, double *y);
  */
 int sedi_last_history(sedi_ctx *ctx, double *hist, int len);
 
+/* Device memory of the current GPU in MB (used = total - free), the device
+ * counterpart of the reference's resident-set report (stochastic-estimator.cc:31-55). */
+int sedi_device_memory(double *used_mb, double *total_mb);
+
 /* Kernel launches issued by this context since creation (for benchmarks). */
 long long sedi_launch_count(const sedi_ctx *ctx);
 

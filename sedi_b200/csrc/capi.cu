@@ -104,6 +104,18 @@ const char *sedi_ctx_error(const sedi_ctx *h) { return h ? h->c.error.c_str() : 
 
 long long sedi_launch_count(const sedi_ctx *h) { return h ? h->c.launches : 0; }
 
+int sedi_device_memory(double *used_mb, double *total_mb) {
+	if (!used_mb || !total_mb) return SEDI_ERR_ARG;
+	size_t fr = 0, tot = 0;
+	if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+		cudaGetLastError();
+		return SEDI_ERR_NODEV;
+	}
+	*used_mb = (double)(tot - fr) / (1024.0 * 1024.0);
+	*total_mb = (double)tot / (1024.0 * 1024.0);
+	return 0;
+}
+
 void sedi_fill_probe(uint32_t seed, long n, double *out) {
 	if (out && n > 0) host_fill_probe(seed, n, out);
 }

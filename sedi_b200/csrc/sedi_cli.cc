@@ -1,0 +1,308 @@
+// sedi -- command-line driver of the GPU estimator, a drop-in for the
+// reference's stochastic-estimator.{cg,pipelined_cg,bicgstab}.exe.
+//
+// Options are the reference's (CmdLineParser.hpp:43-79): -g N1xN2xN3 and
+// -p P1xP2xP3 mandatory (the whole grid runs on one GPU, so -p must be
+// 1x1x1), -s samples (default 400), -e tol (1e-4), -m maxiter (1000), -i,
+// -f mode, -F, -V archive (solver validation), -E archive (estimator
+// validation).  The reference picks the solver at compile time (-DSOLVER);
+// here --solver bicgstab|cg|pcg (default cg) or the program name suffix
+// (sedi.cg, sedi.pipelined_cg, sedi.bicgstab) selects it.  Extra options:
+// --precision fp64|mixed, --batch B (right-hand sides per launch), --seed S
+// (probe k uses std::mt19937(S + k), default 1234), --quiet (no
+// per-iteration lines), --write-d FILE (the estimate D as raw doubles, i1
+// fastest).
+//
+// Printed lines follow stochastic-estimator.cc, DomainDecomposition.hpp:43-48,
+// the solvers' constructors and per-iteration prints, ValidateSolver.hpp and
+// ValidateEstimator.hpp.  Validation archives use the raw stand-in format
+// (<archive>/<dataset>.raw: "SEDIRAW1", u32 ndims, u32 elem bytes, u64 dims,
+// data in the row-major order of Slice3d::pack_into, i3 fastest).
+#include <getopt.h>
+#include <sys/resource.h>
+#include <sys/time.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sedi_b200.h"
+
+namespace {
+
+[[noreturn]] void usage(const char *prog) {
+	fprintf(stderr, "Usage: %s -g NxNxN -p NxNxN [-s NSAMPLES] [-e TOL] [-m MAXITER] [-i] [-f MODE] [-F]\n", prog);
+	fprintf(stderr, "\t-g NxNxN : size of the global 3D grid\n");
+	fprintf(stderr, "\t-p NxNxN : decomposition into ranks (one GPU: 1x1x1)\n");
+	fprintf(stderr, "\t-s NSAMPLES : number of samples for stochastic estimation\n");
+	fprintf(stderr, "\t-e TOL : solver tolerance\n");
+	fprintf(stderr, "\t-m MAXITER : solver maximum iterations\n");
+	fprintf(stderr, "\t-i : ignore solver convergence errors and keep going\n");
+	fprintf(stderr, "\t-f : [advanced] flag for solver operation mode, see e.g. BiCgStab::mode_t\n");
+	fprintf(stderr, "\t-F : don't enable floating point exceptions (accepted; the GPU does not trap)\n");
+	fprintf(stderr, "\t-V ARCHIVE : enable solver validation mode against a validation archive\n");
+	fprintf(stderr, "\t-E ARCHIVE : enable estimator validation mode against a validation archive\n");
+	fprintf(stderr, "\t--solver cg|pcg|bicgstab  --precision fp64|mixed  --batch B  --seed S  --quiet  --write-d FILE\n");
+	exit(1);
+}
+
+// Raw validation archive (see the file comment).
+bool read_raw(const std::string &archive, const char *name, long n1, long n2, long n3, std::vector<double> &dense) {
+	const std::string path = archive + "/" + name + ".raw";
+	FILE *f = fopen(path.c_str(), "rb");
+	if (!f) return false;
+	char magic[8];
+	uint32_t nd = 0, el = 0;
+	uint64_t dims[3] = {0, 0, 0};
+	bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, "SEDIRAW1", 8) == 0 && fread(&nd, 4, 1, f) == 1 &&
+	          fread(&el, 4, 1, f) == 1 && nd == 3 && el == 8 && fread(dims, 8, 3, f) == 3 &&
+	          (long)dims[0] == n1 && (long)dims[1] == n2 && (long)dims[2] == n3;
+	std::vector<double> buf;
+	if (ok) {
+		buf.resize((size_t)n1 * n2 * n3);
+		ok = fread(buf.data(), 8, buf.size(), f) == buf.size();
+	}
+	fclose(f);
+	if (!ok) return false;
+	// Slice3d::unpack_from (Slice3d.hpp:54-64): file order i1, i2, i3 (i3 fastest).
+	dense.resize(buf.size());
+	size_t idx = 0;
+	for (long i1 = 0; i1 < n1; i1++)
+		for (long i2 = 0; i2 < n2; i2++)
+			for (long i3 = 0; i3 < n3; i3++) dense[(size_t)i1 + (size_t)i2 * n1 + (size_t)i3 * n1 * n2] = buf[idx++];
+	return true;
+}
+
+const char *solver_name(int s) { return s == SEDI_CG ? "Cg" : (s == SEDI_PIPELINED_CG ? "PipelinedCg" : "BiCgStab"); }
+
+}  // namespace
+
+int main(int argc, char **argv) {
+	long ng1 = 0, ng2 = 0, ng3 = 0;
+	int np1 = 0, np2 = 0, np3 = 0;
+	int samples = 400, maxiter = 1000, mode = 0, batch = 1, quiet = 0;
+	double tol = 1e-4;
+	bool ignore = false, have_g = false, have_p = false;
+	int precision = SEDI_PREC_FP64;
+	unsigned seed = 1234;
+	const char *vfile = nullptr, *efile = nullptr, *dout = nullptr;
+	int solver = SEDI_CG;
+	const std::string prog = argv[0];
+	if (prog.find("bicgstab") != std::string::npos) solver = SEDI_BICGSTAB;
+	else if (prog.find("pipelined") != std::string::npos) solver = SEDI_PIPELINED_CG;
+
+	static const option longopts[] = {{"solver", required_argument, nullptr, 1},
+	                                  {"precision", required_argument, nullptr, 2},
+	                                  {"batch", required_argument, nullptr, 3},
+	                                  {"seed", required_argument, nullptr, 4},
+	                                  {"quiet", no_argument, nullptr, 5},
+	                                  {"write-d", required_argument, nullptr, 6},
+	                                  {nullptr, 0, nullptr, 0}};
+	int ch;
+	while ((ch = getopt_long(argc, argv, "g:p:s:e:m:if:FV:E:", longopts, nullptr)) != -1) {
+		switch (ch) {
+		case 'g': have_g = sscanf(optarg, "%ldx%ldx%ld", &ng1, &ng2, &ng3) == 3; if (!have_g) usage(argv[0]); break;
+		case 'p': have_p = sscanf(optarg, "%dx%dx%d", &np1, &np2, &np3) == 3; if (!have_p) usage(argv[0]); break;
+		case 's': if (sscanf(optarg, "%d", &samples) != 1) usage(argv[0]); break;
+		case 'e': if (sscanf(optarg, "%lf", &tol) != 1) usage(argv[0]); break;
+		case 'm': if (sscanf(optarg, "%d", &maxiter) != 1) usage(argv[0]); break;
+		case 'i': ignore = true; break;
+		case 'f': if (sscanf(optarg, "%d", &mode) != 1) usage(argv[0]); break;
+		case 'F': break;
+		case 'V': vfile = optarg; break;
+		case 'E': efile = optarg; break;
+		case 1:
+			if (!strcmp(optarg, "cg")) solver = SEDI_CG;
+			else if (!strcmp(optarg, "pcg") || !strcmp(optarg, "pipelined_cg")) solver = SEDI_PIPELINED_CG;
+			else if (!strcmp(optarg, "bicgstab")) solver = SEDI_BICGSTAB;
+			else usage(argv[0]);
+			break;
+		case 2: precision = !strcmp(optarg, "mixed") ? SEDI_PREC_MIXED : SEDI_PREC_FP64; break;
+		case 3: batch = atoi(optarg); break;
+		case 4: seed = (unsigned)strtoul(optarg, nullptr, 10); break;
+		case 5: quiet = 1; break;
+		case 6: dout = optarg; break;
+		default: usage(argv[0]);
+		}
+	}
+	if (!have_g || !have_p) usage(argv[0]);
+	// DomainDecomposition.hpp:29-36 asserts ranks == np and divisibility; one
+	// GPU holds the whole grid, so the decomposition must be 1x1x1.
+	if (np1 != 1 || np2 != 1 || np3 != 1) {
+		fprintf(stderr, "sedi: the grid runs on one GPU; use -p 1x1x1\n");
+		return 1;
+	}
+	printf("Global grid shape is (%ld, %ld, %ld)\n", ng1, ng2, ng3);
+	printf("Domain decomposition across %d MPI ranks\n", 1);
+	printf("Processor decomposition is (%d, %d, %d)\n", 1, 1, 1);
+	printf("Process block shape is (%ld, %ld, %ld)\n", ng1, ng2, ng3);
+	if (vfile && efile) {  // stochastic-estimator.cc:127-131
+		printf("WARNING: cannot enable both solver and estimator validation mode: disabling both!\n");
+		vfile = efile = nullptr;
+	}
+	const long n = ng1 * ng2 * ng3;
+	std::vector<double> ref_x, ref_v, ref_d;
+	double l2_sol = 0, linf_sol = 0;
+	if (vfile) {  // ValidateSolver.hpp:30-80
+		if (!read_raw(vfile, "x_k", ng1, ng2, ng3, ref_x) || !read_raw(vfile, "v_k", ng1, ng2, ng3, ref_v)) {
+			fprintf(stderr, "sedi: cannot read x_k / v_k from %s\n", vfile);
+			return 2;
+		}
+		for (double x : ref_x) {
+			l2_sol += x * x;
+			linf_sol = fabs(x) > linf_sol ? fabs(x) : linf_sol;
+		}
+		l2_sol = sqrt(l2_sol / n);
+		printf("VALIDATION: rank %d read arrays from %s\n", 0, vfile);
+	}
+	if (efile) {  // ValidateEstimator.hpp:27-58
+		if (!read_raw(efile, "diag_inv", ng1, ng2, ng3, ref_d)) {
+			fprintf(stderr, "sedi: cannot read diag_inv from %s\n", efile);
+			return 2;
+		}
+		printf("VALIDATION_ESTIMATOR: rank %d read arrays from %s\n", 0, efile);
+	}
+	int err = 0;
+	if (batch < 1) batch = 1;
+	sedi_ctx *ctx = sedi_create(solver, ng1, ng2, ng3, 6.0, 1.0, 1.0, mode, precision, batch, &err);
+	if (!ctx) {
+		fprintf(stderr, "sedi: cannot create the GPU solver (error %d)\n", err);
+		return 3;
+	}
+	printf("Initialized %s solver, sync_dotprod=%d, sync_stencil=%d\n", solver_name(solver), (mode & 2) != 0,
+	       (mode & 1) != 0);
+
+	std::vector<double> v(n), x(n), t(n, 0.0), q(n, 0.0), D(n), hist(maxiter + 2);
+	int max_it = 0, min_it = maxiter + 1;
+	double t_rng = 0.0, t_solve = 0.0;
+	const auto T0 = std::chrono::steady_clock::now();
+	// Probes run one at a time (reference order, per-iteration lines) in the
+	// single-vector form, or `batch` at a time through sedi_estimate_probes.
+	const bool one_by_one = (batch == 1 && precision == SEDI_PREC_FP64) || vfile || efile;
+	if (one_by_one) {
+		for (int k = 0; k < samples; k++) {
+			printf("Solving for sample %d/%d...\n", k + 1, samples);
+			auto a = std::chrono::steady_clock::now();
+			if (vfile) {
+				printf("VALIDATION: filling RHS from validation dataset\n");
+				v = ref_v;
+			} else {
+				sedi_fill_probe(seed + (unsigned)k, n, v.data());
+			}
+			auto b = std::chrono::steady_clock::now();
+			t_rng += std::chrono::duration<double>(b - a).count();
+			std::fill(x.begin(), x.end(), 0.0);
+			double fe = 0.0;
+			int fi = 0;
+			int res;
+			if (batch == 1 && precision == SEDI_PREC_FP64) {
+				res = sedi_solve(ctx, v.data(), x.data(), nullptr, maxiter, tol, &fe, &fi);
+				if (!quiet && res >= 0) {
+					const int nh = sedi_last_history(ctx, hist.data(), (int)hist.size());
+					for (int i = 1; i < nh; i++) printf("%s: after iter=%d, err=%.10e\n", solver_name(solver), i, hist[i]);
+				}
+			} else {
+				int r1 = 0;
+				res = sedi_solve_batch(ctx, 1, v.data(), x.data(), maxiter, tol, &fe, &fi, &r1);
+				if (res >= 0) res = r1;
+			}
+			t_solve += std::chrono::duration<double>(std::chrono::steady_clock::now() - b).count();
+			if (res < 0) {
+				fprintf(stderr, "sedi: GPU solve failed (%d): %s\n", res, sedi_ctx_error(ctx));
+				return 4;
+			}
+			if (!ignore && res != 0) {  // stochastic-estimator.cc:181-184
+				fprintf(stderr, "Incomplete convergence in solver, errcode=%d\n", res);
+				return 100 + res;
+			}
+			max_it = fi > max_it ? fi : max_it;
+			min_it = fi < min_it ? fi : min_it;
+			if (vfile) {  // ValidateSolver.hpp:95-113
+				printf("VALIDATION: comparing to ref solution from validation dataset\n");
+				double e2 = 0, einf = 0;
+				for (long i = 0; i < n; i++) {
+					const double d = x[i] - ref_x[i];
+					e2 += d * d;
+					einf = fabs(d) > einf ? fabs(d) : einf;
+				}
+				e2 = sqrt(e2 / n);
+				printf("VALIDATION: rel L2 error=%.4e, rel Linf error=%.4e\n", e2 / l2_sol, einf / linf_sol);
+			}
+			for (long i = 0; i < n; i++) {  // stochastic-estimator.cc:195, :198
+				t[i] = t[i] + x[i] * v[i];
+				q[i] = q[i] + v[i] * v[i];
+			}
+			if (efile) {  // stochastic-estimator.cc:201-205, ValidateEstimator.hpp:70-87
+				double e2 = 0, einf = 0;
+				for (long i = 0; i < n; i++) {
+					const double d = t[i] / q[i] - ref_d[i];
+					e2 += d * d;
+					einf = fabs(d) > einf ? fabs(d) : einf;
+				}
+				printf("VALIDATION_ESTIMATOR: L2 error=%.4e, Linf error=%.4e\n", sqrt(e2 / n), einf);
+			}
+		}
+		for (long i = 0; i < n; i++) D[i] = t[i] / q[i];  // :216
+	} else {
+		std::vector<double> probes((size_t)n * samples);
+		auto a = std::chrono::steady_clock::now();
+		for (int k = 0; k < samples; k++) sedi_fill_probe(seed + (unsigned)k, n, probes.data() + (size_t)k * n);
+		auto b = std::chrono::steady_clock::now();
+		t_rng = std::chrono::duration<double>(b - a).count();
+		std::vector<int> iters(samples), results(samples);
+		std::vector<double> errs(samples);
+		const int rc = sedi_estimate_probes(ctx, samples, probes.data(), maxiter, tol, ignore ? 1 : 0, D.data(),
+		                                    t.data(), q.data(), iters.data(), errs.data(), results.data());
+		t_solve = std::chrono::duration<double>(std::chrono::steady_clock::now() - b).count();
+		if (rc < 0) {
+			fprintf(stderr, "sedi: GPU estimate failed (%d): %s\n", rc, sedi_ctx_error(ctx));
+			return 4;
+		}
+		for (int k = 0; k < samples; k++) {
+			max_it = iters[k] > max_it ? iters[k] : max_it;
+			min_it = iters[k] < min_it ? iters[k] : min_it;
+		}
+		if (!ignore && rc != 0) {
+			fprintf(stderr, "Incomplete convergence in solver, errcode=%d\n", rc);
+			return 100 + rc;
+		}
+	}
+	const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - T0).count();
+	printf("Total solve time: %.4e seconds, iteration count min=%d max=%d\n", total, min_it, max_it);
+	// Timers.hpp:57-70 buckets.  On the GPU the stencil, dot products and
+	// vector updates are fused kernels: their time is reported under
+	// TIMER_COMPUTE_STENCIL_INNER; one GPU has no halo or dot-product comms.
+	printf("===========================================\n");
+	printf("TIMER_GLOBAL                 = %.4e s\n", total);
+	printf("TIMER_COMPUTE_STENCIL_INNER  = %.4e s\n", t_solve);
+	printf("TIMER_COMPUTE_STENCIL_BORDER = %.4e s\n", 0.0);
+	printf("TIMER_COMPUTE_DOTPROD        = %.4e s\n", 0.0);
+	printf("TIMER_COMPUTE_RNG            = %.4e s\n", t_rng);
+	printf("TIMER_COMPUTE_MISC           = %.4e s\n", total - t_solve - t_rng);
+	printf("TIMER_HALO_PACK              = %.4e s\n", 0.0);
+	printf("TIMER_HALO_ISEND_IRECV       = %.4e s\n", 0.0);
+	printf("TIMER_HALO_UNPACK_WAIT       = %.4e s\n", 0.0);
+	printf("TIMER_COMM_DOTPROD           = %.4e s\n", 0.0);
+	printf("===========================================\n");
+	struct rusage usage;
+	getrusage(RUSAGE_SELF, &usage);
+	const double rss = usage.ru_maxrss / 1024.0;
+	printf("Resident set size across ranks [MB]: avg=%.3e, tot=%.3e, min=%.3e, max=%.3e\n", rss, rss, rss, rss);
+	double used = 0, totmb = 0;
+	if (sedi_device_memory(&used, &totmb) == 0) printf("Device memory [MB]: used=%.3e, total=%.3e\n", used, totmb);
+	// The estimate itself, for callers that want it (the reference keeps it in memory).
+	if (dout) {
+		FILE *f = fopen(dout, "wb");
+		if (f) {
+			fwrite(D.data(), sizeof(double), D.size(), f);
+			fclose(f);
+		}
+	}
+	sedi_destroy(ctx);
+	return 0;
+}
