@@ -167,6 +167,11 @@ int sedi_time_kernels(sedi_ctx *ctx, int reps, double *ms, double *bytes, char *
 int sedi_residual_noalloc(long n1, long n2, long n3, double a, double b, double c, const double *x_dev,
                           const double *b_dev, double *r_dev, double *err_out, void *stream);
 
+/* Device probe generator: probes seed, seed+1, ..., seed+nprobes-1 (each
+ * DistrRngStd's +-1 vector from std::mt19937(seed + k), bit-identical to
+ * sedi_fill_probe) into out_dev[k*n + i], on `stream` (cudaStream_t as void*). */
+int sedi_fill_probes_dev(uint32_t seed, int nprobes, long n, double *out_dev, void *stream);
+
 /* Host probe generator, bit-identical to DistrRngStd with std::mt19937(seed). */
 void sedi_fill_probe(uint32_t seed, long n, double *out);
 

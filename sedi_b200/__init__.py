@@ -84,6 +84,7 @@ def load():
     lib.sedi_estimate_dev.argtypes = [vp, c_int, vp, c_int, c_double, c_int, vp, vp, vp, vp, vp, vp]
     lib.sedi_set_stream.argtypes = [vp, vp]
     lib.sedi_time_kernels.argtypes = [vp, c_int, vp, vp, vp, vp]
+    lib.sedi_fill_probes_dev.argtypes = [ctypes.c_uint32, c_int, c_long, vp, vp]
     lib.sedi_residual_noalloc.argtypes = [c_long, c_long, c_long, c_double, c_double, c_double, vp, vp, vp, pd, vp]
     _lib = lib
     return lib
@@ -111,6 +112,18 @@ def fill_probe(seed, n):
     """DistrRngStd::fill_plusminusone with std::mt19937(seed) (DistrRngStd.hpp:22-42)."""
     out = np.empty(int(n), np.float64)
     load().sedi_fill_probe(int(seed) & 0xFFFFFFFF, int(n), _ptr(out))
+    return out
+
+
+def fill_probes_dev(seed, out, stream=None):
+    """Device generator: fills the CUDA float64 tensor out (nprobes, n) with
+    probes seed, seed+1, ... (bit-identical to fill_probe)."""
+    nprobes, n = out.shape
+    handle = None if stream is None else int(getattr(stream, "cuda_stream", stream))
+    rc = load().sedi_fill_probes_dev(int(seed) & 0xFFFFFFFF, int(nprobes), int(n), _ptr(out),
+                                     ctypes.c_void_p(handle) if handle else None)
+    if rc < 0:
+        raise SediError(rc, "fill_probes_dev")
     return out
 
 

@@ -91,7 +91,7 @@ __device__ __forceinline__ void dacc(double &acc, T a, T b) {
 }
 
 // Map slots (Maps::m) for the per-type descriptor sets.
-enum { MT_R_HALO = 0, MT_P0_HALO, MT_P1_HALO, MT_X_INT, MT_R_INT };  // fields of type T
+enum { MT_R_HALO = 0, MT_P0_HALO, MT_P1_HALO, MT_X_INT, MT_R_INT, MT_W0_HALO, MT_W1_HALO, MT_Q_HALO };  // T fields
 enum { MD_X_HALO = 0, MD_B_INT };                                     // FP64 fields
 
 // ---------------------------------------------------------------------------
@@ -362,6 +362,7 @@ struct OpResid : OpBase<double> {
 	TR *r, *rhat, *xlo;  // stored in the TR layout (slice width WT)
 	double iMd;
 	int solver, ru, WT;
+	int pcg;  // reliable update of pipelined CG: the following sweeps rebuild its scalars
 	long long npts;
 	int it;
 	int keep[2];
@@ -408,7 +409,7 @@ struct OpResid : OpBase<double> {
 				ls.exit_iter[lane] = maxiter + 1;
 				ls.reason[lane] = STOP_MAXITER;
 				atomicSub(&gl->active, 1);
-			} else {
+			} else if (!pcg) {
 				ls.ru_new[lane] = tot[0];  // continue from the replaced residual
 				ls.beta[lane] = tot[0] / ls.ru[lane];
 			}
@@ -581,6 +582,207 @@ struct OpCgB : OpBase<T> {
 	}
 };
 
+// ---------------------------------------------------------------------------
+// Pipelined CG (PipelinedCg.hpp:136-230), one sweep per iteration.  The
+// stencil input is m = w .* iM (:158) from the w halo; the seven pointwise
+// fields q, s, p, z, r, x, u are read directly in the epilogue (a TMA ring
+// of eight fields would not fit in shared memory); the eight fused updates
+// (:199-221) and the next iteration's <r,u>, <w,u>, <r,r> (:155) follow.
+// w ping-pongs: iteration it reads W[(it+1)&1] and writes W[it&1].
+// ---------------------------------------------------------------------------
+template <class T>
+struct OpPcg : OpBase<T> {
+	static constexpr int NS = 1, NQ = 0, ND = 3;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr int V = Vec<T>::V;
+	T iMc;
+	T *x, *r, *u, *q, *s, *p, *z, *w0, *w1;
+	T *wn;
+	int it, mixed;
+	T alpha[V], beta[V];
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+		wn = (it & 1) ? w1 : w0;
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const int l = lane + e;
+			const double g = ls.gamma[l], d = ls.delta[l];
+			double al, be;
+			if (it > 1) {  // :175-178
+				be = __ddiv_rn(g, ls.gamma_old[l]);
+				al = __ddiv_rn(1.0, __dsub_rn(__ddiv_rn(d, g), __ddiv_rn(be, ls.alpha[l])));
+			} else {       // :179-181
+				be = 0.0;
+				al = __ddiv_rn(g, d);
+			}
+			if (ls.done[l]) al = be = 0.0;  // finished lanes stay frozen
+			alpha[e] = (T)al;
+			beta[e] = (T)be;
+		}
+	}
+	__device__ bool raw_center() const { return true; }
+	__device__ int src_map(int) const { return (it & 1) ? MT_W0_HALO : MT_W1_HALO; }
+	__device__ int q_map(int) const { return 0; }
+	__device__ Vec<T> src(const Vec<T> *raw) const {
+		Vec<T> o;
+#pragma unroll
+		for (int e = 0; e < V; e++) o.v[e] = amul(raw[0].v[e], iMc);  // m = w .* iM
+		return o;
+	}
+	__device__ void out(long long o, long long, int, const Vec<T> &mc, const Vec<T> &nc, const Vec<T> *,
+	                    const Vec<T> *rc, double (&part)[ND][V]) const {
+		const Vec<T> wv = rc[0];
+		Vec<T> qv = ldg_rw(q + o), sv = ldg_rw(s + o), pv = ldg_rw(p + o), zv = ldg_rw(z + o);
+		Vec<T> rv = ldg_rw(r + o), xv = ldg_rw(x + o), uv = ldg_rw(u + o), wnv;
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			qv.v[e] = aadd(mc.v[e], amul(beta[e], qv.v[e]));       // :200
+			sv.v[e] = aadd(wv.v[e], amul(beta[e], sv.v[e]));       // :203
+			pv.v[e] = aadd(uv.v[e], amul(beta[e], pv.v[e]));       // :206
+			zv.v[e] = aadd(nc.v[e], amul(beta[e], zv.v[e]));       // :209
+			rv.v[e] = aadd(rv.v[e], amul(-alpha[e], sv.v[e]));     // :212
+			xv.v[e] = aadd(xv.v[e], amul(alpha[e], pv.v[e]));      // :215
+			uv.v[e] = aadd(uv.v[e], amul(-alpha[e], qv.v[e]));     // :218
+			wnv.v[e] = aadd(wv.v[e], amul(-alpha[e], zv.v[e]));    // :221
+			dacc(part[0][e], rv.v[e], uv.v[e]);
+			dacc(part[1][e], wnv.v[e], uv.v[e]);
+			dacc(part[2][e], rv.v[e], rv.v[e]);
+		}
+		stg(q + o, qv);
+		stg(s + o, sv);
+		stg(p + o, pv);
+		stg(z + o, zv);
+		stg(r + o, rv);
+		stg(x + o, xv);
+		stg(u + o, uv);
+		stg(wn + o, wnv);
+	}
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		if (ls.done[lane]) return;
+		// The stop test uses <r,r> from the top of this iteration (:173, :227).
+		const double err = sqrt(__ddiv_rn(ls.rr_top[lane], ls.bb[lane]));
+		ls.err[lane] = err;
+		const double g = ls.gamma[lane], d = ls.delta[lane];
+		double al;
+		if (it > 1) {
+			const double be = __ddiv_rn(g, ls.gamma_old[lane]);
+			al = __ddiv_rn(1.0, __dsub_rn(__ddiv_rn(d, g), __ddiv_rn(be, ls.alpha[lane])));
+		} else {
+			al = __ddiv_rn(g, d);
+		}
+		ls.gamma_old[lane] = g;
+		ls.alpha[lane] = al;
+		ls.gamma[lane] = tot[0];
+		ls.delta[lane] = tot[1];
+		ls.rr_top[lane] = tot[2];
+		const double tol = gl->tol;
+		const int maxiter = gl->maxiter;
+		if (mixed) {
+			if (err <= tol || it >= maxiter) {
+				ls.pending[lane] = 1;
+				gl->ru_due = 1;
+			}
+			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = 1;
+		} else if (err <= tol) {
+			ls.done[lane] = 1;
+			ls.exit_iter[lane] = it;
+			ls.reason[lane] = STOP_CONVERGED;
+			atomicSub(&gl->active, 1);
+		} else if (it >= maxiter) {
+			ls.done[lane] = 1;
+			ls.exit_iter[lane] = maxiter + 1;
+			ls.reason[lane] = STOP_MAXITER;
+			atomicSub(&gl->active, 1);
+		}
+	}
+};
+
+// Pipelined CG setup and residual replacement: from r, u = r .* iM (:138)
+// and w = A u (:141-143) into the w buffer the next iteration reads, plus the
+// next iteration's <r,u>, <w,u>, <r,r>.  With `zero`, also q = s = p = z = 0
+// (:146-149).  In a reliable update it runs only when one is due.
+template <class T>
+struct OpPcgUW : OpBase<T> {
+	static constexpr int NS = 1, NQ = 0, ND = 3;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr int V = Vec<T>::V;
+	T iMc;
+	T *u, *w0, *w1, *q, *s, *p, *z;
+	T *wdst;
+	int zero, ru;
+	__device__ bool enabled(const Global *gl) const { return !ru || gl->ru_due; }
+	__device__ void begin(const Global *gl, const LaneState &, int) {
+		// The next iteration (gl->iter + 1 after a reliable update, 1 at setup) reads W[(it+1)&1].
+		const int next = ru ? gl->iter + 1 : 1;
+		wdst = (next & 1) ? w0 : w1;
+	}
+	__device__ bool raw_center() const { return true; }
+	__device__ int src_map(int) const { return MT_R_HALO; }
+	__device__ int q_map(int) const { return 0; }
+	__device__ Vec<T> src(const Vec<T> *raw) const {
+		Vec<T> o;
+#pragma unroll
+		for (int e = 0; e < V; e++) o.v[e] = amul(raw[0].v[e], iMc);
+		return o;
+	}
+	__device__ void out(long long o, long long, int, const Vec<T> &uc, const Vec<T> &wv, const Vec<T> *,
+	                    const Vec<T> *rc, double (&part)[ND][V]) const {
+		stg(u + o, uc);
+		stg(wdst + o, wv);
+		if (zero) {
+			stg(q + o, vzero<T>());
+			stg(s + o, vzero<T>());
+			stg(p + o, vzero<T>());
+			stg(z + o, vzero<T>());
+		}
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			dacc(part[0][e], rc[0].v[e], uc.v[e]);
+			dacc(part[1][e], wv.v[e], uc.v[e]);
+			dacc(part[2][e], rc[0].v[e], rc[0].v[e]);
+		}
+	}
+	__device__ void fin(int lane, const double *tot, Global *, const LaneState &ls) const {
+		if (ru && ls.done[lane]) return;
+		ls.gamma[lane] = tot[0];
+		ls.delta[lane] = tot[1];
+		ls.rr_top[lane] = tot[2];
+		if (!ru) {
+			ls.gamma_old[lane] = 0.0;
+			ls.alpha[lane] = 0.0;
+		}
+	}
+};
+
+// y = A f (+ y2 = y .* iM): the reliable update's s = A p, q = s .* iM and
+// z = A q for pipelined CG.  No reductions.
+template <class T>
+struct OpApply : OpBase<T> {
+	static constexpr int NS = 1, NQ = 0, ND = 0;
+	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
+	static constexpr int V = Vec<T>::V;
+	T iMc;
+	T *y, *y2;
+	int map;
+	__device__ bool enabled(const Global *gl) const { return gl->ru_due != 0; }
+	__device__ void begin(const Global *, const LaneState &, int) {}
+	__device__ bool raw_center() const { return false; }
+	__device__ int src_map(int) const { return map; }
+	__device__ int q_map(int) const { return 0; }
+	__device__ Vec<T> src(const Vec<T> *raw) const { return raw[0]; }
+	__device__ void out(long long o, long long, int, const Vec<T> &, const Vec<T> &yv, const Vec<T> *, const Vec<T> *,
+	                    double (&)[1][V]) const {
+		stg(y + o, yv);
+		if (y2) {
+			Vec<T> t;
+#pragma unroll
+			for (int e = 0; e < V; e++) t.v[e] = amul(yv.v[e], iMc);
+			stg(y2 + o, t);
+		}
+	}
+	__device__ void fin(int, const double *, Global *, const LaneState &) const {}
+};
+
 // Iteration bookkeeping between launches.
 __global__ void kb_next_iter(Global *gl) {
 	if (gl->active == 0) return;
@@ -718,6 +920,7 @@ struct Batched {
 	double *xh = nullptr;  // MIXED x_hi
 	double *b = nullptr;   // right-hand sides (FP64)
 	void *r = nullptr, *p0 = nullptr, *p1 = nullptr;
+	void *w[2] = {nullptr, nullptr}, *u = nullptr, *q = nullptr, *sv = nullptr, *z = nullptr;  // pipelined CG
 	double *partials = nullptr;
 	unsigned *ticket = nullptr;
 	Global *gl = nullptr, *gl_host = nullptr;
@@ -827,8 +1030,8 @@ int batched_alloc(Ctx *c) {
 		c->error = "batch too large for one context (max 256 FP32 / 128 FP64 right-hand sides)";
 		return SEDI_ERR_ARG;
 	}
-	if (c->solver != 2) {
-		c->error = "batched form implemented for CG";
+	if (c->solver == 1) {
+		c->error = "batched form implemented for CG and pipelined CG";
 		return SEDI_ERR_UNSUPPORTED;
 	}
 	if (!encode_fn()) {
@@ -860,6 +1063,17 @@ int batched_alloc(Ctx *c) {
 		c->error = "device allocation failed (batched form)";
 		return SEDI_ERR_NOMEM;
 	}
+	if (c->solver == 3) {
+		void **pv[] = {&B->w[0], &B->w[1], &B->u, &B->q, &B->sv, &B->z};
+		for (void **pp : pv) {
+			if (cudaMalloc(pp, B->elems * ts) != cudaSuccess) {
+				cudaGetLastError();
+				c->error = "device allocation failed (batched pipelined CG)";
+				return SEDI_ERR_NOMEM;
+			}
+			cudaMemset(*pp, 0, B->elems * ts);
+		}
+	}
 	cudaMemset(B->ticket, 0, sizeof(unsigned));
 	cudaMemset(B->x, 0, B->elems * ts);
 	cudaMemset(B->r, 0, B->elems * ts);
@@ -881,6 +1095,10 @@ int batched_alloc(Ctx *c) {
 	          make_map(&B->mapsT.m[MT_P1_HALO], B->p1, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
 	          make_map(&B->mapsT.m[MT_X_INT], B->x, ebT, c->g, R, B->rbT, P1, P2) &&
 	          make_map(&B->mapsT.m[MT_R_INT], B->r, ebT, c->g, R, B->rbT, P1, P2);
+	if (c->solver == 3)
+		ok = ok && make_map(&B->mapsT.m[MT_W0_HALO], B->w[0], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
+		     make_map(&B->mapsT.m[MT_W1_HALO], B->w[1], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
+		     make_map(&B->mapsT.m[MT_Q_HALO], B->q, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2);
 	tile_for(B->rbD, 8, &P1, &P2);
 	ok = ok && make_map(&B->mapsD.m[MD_X_HALO], B->mixed ? (void *)B->xh : B->x, 8, c->g, R, B->rbD, P1 + 2, P2 + 2) &&
 	     make_map(&B->mapsD.m[MD_B_INT], B->b, 8, c->g, R, B->rbD, P1, P2);
@@ -895,7 +1113,7 @@ void batched_free(Ctx *c) {
 	Batched *B = (Batched *)c->batched;
 	if (!B) return;
 	void *ptrs[] = {B->x, B->xh, B->b, B->r, B->p0, B->p1, B->partials, B->ticket, B->gl, B->lane_mem, B->lane_int,
-	                B->t_acc, B->q_acc};
+	                B->t_acc, B->q_acc, B->w[0], B->w[1], B->u, B->q, B->sv, B->z};
 	for (void *p : ptrs)
 		if (p) cudaFree(p);
 	if (B->gl_host) cudaFreeHost(B->gl_host);
@@ -906,6 +1124,7 @@ void batched_free(Ctx *c) {
 
 template <int RBD>
 static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
+	const int pcg = c->solver == 3 ? 1 : 0;
 	typedef typename CfgFor<double, RBD>::type CD;
 	cudaStream_t s = c->stream;
 	if (B->mixed) {
@@ -921,6 +1140,7 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 		op.iMd = 1.0 / c->k.a;
 		op.solver = c->solver;
 		op.ru = ru ? 1 : 0;
+		op.pcg = pcg;
 		launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, s);
 	} else {
 		OpResid<double> op;
@@ -935,6 +1155,7 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 		op.iMd = 1.0 / c->k.a;
 		op.solver = c->solver;
 		op.ru = 0;
+		op.pcg = pcg;
 		launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, s);
 	}
 }
@@ -973,6 +1194,77 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	}
 }
 
+template <class T, int RBT>
+static void enqueue_pcg_uw(Ctx *c, Batched *B, int zero, int ru) {
+	typedef typename CfgFor<T, RBT>::type C;
+	OpPcgUW<T> o;
+	o.ka = (T)c->k.a;
+	o.kb = (T)c->k.b;
+	o.kc = (T)c->k.c;
+	o.iMc = (T)(1.0 / c->k.a);
+	o.u = (T *)B->u;
+	o.w0 = (T *)B->w[0];
+	o.w1 = (T *)B->w[1];
+	o.q = (T *)B->q;
+	o.s = (T *)B->sv;
+	o.p = (T *)B->p0;
+	o.z = (T *)B->z;
+	o.zero = zero;
+	o.ru = ru;
+	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o, c->stream);
+}
+
+template <class T, int RBT, int RBD>
+static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
+	typedef typename CfgFor<T, RBT>::type C;
+	cudaStream_t s = c->stream;
+	OpPcg<T> o;
+	o.ka = (T)c->k.a;
+	o.kb = (T)c->k.b;
+	o.kc = (T)c->k.c;
+	o.iMc = (T)(1.0 / c->k.a);
+	o.x = (T *)B->x;
+	o.r = (T *)B->r;
+	o.u = (T *)B->u;
+	o.q = (T *)B->q;
+	o.s = (T *)B->sv;
+	o.p = (T *)B->p0;
+	o.z = (T *)B->z;
+	o.w0 = (T *)B->w[0];
+	o.w1 = (T *)B->w[1];
+	o.mixed = B->mixed ? 1 : 0;
+	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o, s);
+	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
+	c->launches++;
+	if (B->mixed) {
+		// Residual replacement (reliable update) of pipelined CG: x_hi += x_lo;
+		// r = b - A x_hi (FP64); s = A p, q = s .* iM; z = A q; u = r .* iM,
+		// w = A u and the next iteration's dots.
+		const long long nb = ((long long)B->elems / 2 + 255) / 256;
+		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
+		                                                                 (float *)B->x, B->gl);
+		c->launches++;
+		enqueue_resid<RBD>(c, B, true);
+		OpApply<T> a1;
+		a1.ka = (T)c->k.a;
+		a1.kb = (T)c->k.b;
+		a1.kc = (T)c->k.c;
+		a1.iMc = (T)(1.0 / c->k.a);
+		a1.y = (T *)B->sv;
+		a1.y2 = (T *)B->q;
+		a1.map = MT_P0_HALO;
+		launch<C>(c, B, B->gT, B->gridT, B->mapsT, a1, s);
+		OpApply<T> a2 = a1;
+		a2.y = (T *)B->z;
+		a2.y2 = nullptr;
+		a2.map = MT_Q_HALO;
+		launch<C>(c, B, B->gT, B->gridT, B->mapsT, a2, s);
+		enqueue_pcg_uw<T, RBT>(c, B, 0, 1);
+		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
+		c->launches++;
+	}
+}
+
 template <class T, int RBT, int RBD>
 static int run_batched(Ctx *c, Batched *B, int maxiter, double tol) {
 	cudaStream_t s = c->stream;
@@ -995,12 +1287,16 @@ static int run_batched(Ctx *c, Batched *B, int maxiter, double tol) {
 	}
 	B->gl_host->active -= 1;
 	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
+	if (c->solver == 3 && B->gl_host->active > 0) enqueue_pcg_uw<T, RBT>(c, B, 1, 0);  // :138-149
 	if (!B->graph) {
 		// The graph bakes in tol/maxiter only through Global (device), so it is reusable.
 		cudaGraph_t graph;
 		const long long before = c->launches;
 		BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-		for (int i = 0; i < B->chunk; i++) enqueue_cg_iteration<T, RBT, RBD>(c, B);
+		for (int i = 0; i < B->chunk; i++) {
+			if (c->solver == 3) enqueue_pcg_iteration<T, RBT, RBD>(c, B);
+			else enqueue_cg_iteration<T, RBT, RBD>(c, B);
+		}
 		BTRY(cudaStreamEndCapture(s, &graph));
 		B->graph_kernels = c->launches - before;
 		c->launches = before;
@@ -1151,6 +1447,38 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 	BTRY(cudaEventCreate(&e0));
 	BTRY(cudaEventCreate(&e1));
 	const double ts = (double)sizeof(T) * (double)B->elems;
+	if (c->solver == 3) {
+		OpPcg<T> o;
+		o.ka = (T)c->k.a;
+		o.kb = (T)c->k.b;
+		o.kc = (T)c->k.c;
+		o.iMc = (T)(1.0 / c->k.a);
+		o.x = (T *)B->x;
+		o.r = (T *)B->r;
+		o.u = (T *)B->u;
+		o.q = (T *)B->q;
+		o.s = (T *)B->sv;
+		o.p = (T *)B->p0;
+		o.z = (T *)B->z;
+		o.w0 = (T *)B->w[0];
+		o.w1 = (T *)B->w[1];
+		o.mixed = 0;
+		launch<C>(c, B, B->gT, B->gridT, B->mapsT, o, s);
+		BTRY(cudaEventRecord(e0, s));
+		for (int i = 0; i < reps; i++) launch<C>(c, B, B->gT, B->gridT, B->mapsT, o, s);
+		BTRY(cudaEventRecord(e1, s));
+		BTRY(cudaEventSynchronize(e1));
+		float t = 0.f;
+		BTRY(cudaEventElapsedTime(&t, e0, e1));
+		ms[0] = (double)t / reps;
+		bytes[0] = 16.0 * ts;  // w, q, s, p, z, r, x, u in and out
+		snprintf(names, 32, "%s", B->mixed ? "pcg_fp32" : "pcg_fp64");
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		*count = 1;
+		BTRY(cudaGetLastError());
+		return 0;
+	}
 	for (int k = 0; k < 2; k++) {
 		if (k == 0) launch<C>(c, B, B->gT, B->gridT, B->mapsT, a, s);
 		else launch<C>(c, B, B->gT, B->gridT, B->mapsT, bo, s);
@@ -1197,6 +1525,16 @@ int batched_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *name
 
 int batched_estimate_dev(Ctx *c, int samples, const double *probes_dev, int maxiter, double tol, int ignore_errors,
                          double *D_dev, double *t_dev, double *q_dev, int *iters, double *errs, int *results) {
+	return batched_estimate_src(c, samples, probes_dev, 0u, maxiter, tol, ignore_errors, D_dev, t_dev, q_dev, iters,
+	                            errs, results);
+}
+
+// Probes come from device memory (probes_dev) or, when probes_dev is NULL,
+// from the device generator (probe k = std::mt19937(seed + k)), written
+// straight into the lane-sliced right-hand-side buffer.
+int batched_estimate_src(Ctx *c, int samples, const double *probes_dev, uint32_t seed, int maxiter, double tol,
+                         int ignore_errors, double *D_dev, double *t_dev, double *q_dev, int *iters, double *errs,
+                         int *results) {
 	Batched *B = (Batched *)c->batched;
 	cudaStream_t s = c->stream;
 	const long long n = c->g.n;
@@ -1206,7 +1544,12 @@ int batched_estimate_dev(Ctx *c, int samples, const double *probes_dev, int maxi
 	bool first = true;
 	for (int k0 = 0; k0 < samples; k0 += c->batch) {
 		const int nb = samples - k0 < c->batch ? samples - k0 : c->batch;
-		kb_interleave<<<blocks1d(n * B->R), 256, 0, s>>>(n, B->R, B->rbD, nb, probes_dev + (size_t)k0 * n, B->b);
+		if (probes_dev) {
+			kb_interleave<<<blocks1d(n * B->R), 256, 0, s>>>(n, B->R, B->rbD, nb, probes_dev + (size_t)k0 * n, B->b);
+		} else {
+			if (nb < B->R) BTRY(cudaMemsetAsync(B->b, 0, B->elems * sizeof(double), s));  // padding lanes
+			if (device_fill_probes(seed + (uint32_t)k0, nb, n, B->rbD, B->b, s)) return set_cuda_error(c, cudaGetLastError(), "device probes");
+		}
 		BTRY(cudaMemsetAsync(B->mixed ? (void *)B->xh : B->x, 0, B->elems * sizeof(double), s));  // x = 0 (:175)
 		c->launches++;
 		int rc = batched_run_resident(c, nb, maxiter, tol, fe.data(), fi.data(), res.data());

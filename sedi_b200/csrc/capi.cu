@@ -209,7 +209,7 @@ static int estimate_common(Ctx *c, int samples, uint32_t seed, const double *pro
 		// Batched form: stage the probes in a context-owned device buffer
 		// (reused across calls), run them as right-hand sides, copy D (t, q) back.
 		const size_t need = bytes * (size_t)(samples > 0 ? samples : 1);
-		if (c->stage_probe_bytes < need) {
+		if (probes && c->stage_probe_bytes < need) {
 			if (c->stage_probes) cudaFree(c->stage_probes);
 			c->stage_probes = nullptr;
 			c->stage_probe_bytes = 0;
@@ -226,18 +226,12 @@ static int estimate_common(Ctx *c, int samples, uint32_t seed, const double *pro
 			c->error = "device allocation failed (result staging)";
 			return SEDI_ERR_NOMEM;
 		}
-		if (probes) {
-			CAPI_TRY(cudaMemcpyAsync(c->stage_probes, probes, need, cudaMemcpyHostToDevice, c->stream));
-		} else {
-			std::vector<double> tmp((size_t)n);
-			for (int k = 0; k < samples; k++) {
-				host_fill_probe(seed + (uint32_t)k, (long)n, tmp.data());
-				CAPI_TRY(cudaMemcpy(c->stage_probes + (size_t)k * n, tmp.data(), bytes, cudaMemcpyHostToDevice));
-			}
-		}
+		// Seeded probes are generated on the device (bit-identical to the host
+		// generator); caller probes are uploaded.
+		if (probes) CAPI_TRY(cudaMemcpyAsync(c->stage_probes, probes, need, cudaMemcpyHostToDevice, c->stream));
 		double *dD = c->stage_out, *dt = c->stage_out + n, *dq = c->stage_out + 2 * n;
-		int rc = batched_estimate_dev(c, samples, c->stage_probes, maxiter, tol, ignore_errors, dD, dt, dq, iters,
-		                              errs, results);
+		int rc = batched_estimate_src(c, samples, probes ? c->stage_probes : nullptr, seed, maxiter, tol,
+		                              ignore_errors, dD, dt, dq, iters, errs, results);
 		if (rc < 0) return rc;
 		CAPI_TRY(cudaMemcpyAsync(D, dD, bytes, cudaMemcpyDeviceToHost, c->stream));
 		if (t) CAPI_TRY(cudaMemcpyAsync(t, dt, bytes, cudaMemcpyDeviceToHost, c->stream));

@@ -105,8 +105,13 @@ int batched_estimate_dev(Ctx *c, int samples, const double *probes_dev, int maxi
                          int ignore_errors, double *D_dev, double *t_dev, double *q_dev, int *iters,
                          double *errs, int *results);
 int batched_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count);
+int batched_estimate_src(Ctx *c, int samples, const double *probes_dev, uint32_t seed, int maxiter, double tol,
+                         int ignore_errors, double *D_dev, double *t_dev, double *q_dev, int *iters, double *errs,
+                         int *results);
 
 // rng.cu
 void host_fill_probe(uint32_t seed, long n, double *out);
+// Probes seed..seed+nprobes-1 on the device: lane-sliced (W > 0) or dense (W == 0).
+int device_fill_probes(uint32_t seed, int nprobes, long long npts, int W, double *out, cudaStream_t s);
 
 }  // namespace sedi

@@ -117,3 +117,53 @@ def test_batch_padding_lanes_and_zero_rhs():
             res, fe, fi = c.solve_batch(X, B, maxiter=500, tol=1e-10)
         assert np.all(res == 0)
         assert fi[1] == 0 and fe[1] == 0.0 and np.all(X[1] == 0.0)
+
+
+@pytest.mark.parametrize("nrhs", [1, 5, 16])
+def test_fp64_batch_pcg_matches_single_vector(nrhs):
+    dims = (20, 18, 16)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(555 + k, n) for k in range(nrhs)])
+    X = np.zeros_like(B)
+    with S.Context("pcg", dims, batch=nrhs) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=1000, tol=1e-9)
+    for k in range(nrhs):
+        rc0, fe0, fi0, x0, _ = O.solve(3, dims, B[k], maxiter=1000, tol=1e-9)
+        assert (res[k], fi[k]) == (rc0, fi0)
+        assert O.relmax(X[k], x0) <= 1e-10
+        assert abs(fe[k] - fe0) <= 1e-8 * fe0 + 1e-15
+
+
+def test_fp64_batch_pcg_estimator_vs_reference():
+    g = O.golden("pcg_32_m50")
+    m = g["meta"]
+    with S.Context("pcg", m["grid"], batch=8) as c:
+        r = c.estimate(m["samples"], m["seed"], m["maxiter"], m["tol"])
+    assert np.array_equal(r["iters"], g["iters"]) and np.array_equal(r["results"], g["results"])
+    assert O.relmax(r["D"], g["D"]) <= 1e-10
+
+
+@pytest.mark.parametrize("nrhs,tol", [(4, 1e-9), (32, 1e-10)])
+def test_mixed_batch_pcg_true_residual(nrhs, tol):
+    dims = (24, 22, 20)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(31 + k, n) for k in range(nrhs)])
+    X = np.zeros_like(B)
+    with S.Context("pcg", dims, precision=S.MIXED, batch=nrhs) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=3000, tol=tol)
+    assert np.all(res == 0)
+    for k in range(nrhs):
+        assert true_err(dims, X[k], B[k]) <= tol * 1.0000001, k
+    fi64 = O.solve(3, dims, B[0], maxiter=3000, tol=tol)[2]
+    assert fi[0] <= fi64 * 1.25 + 10
+
+
+def test_mixed_pcg_estimator_diagonal_error():
+    dims = (32, 32, 32)
+    samples = 16
+    with S.Context("pcg", dims, batch=samples) as c64:
+        r64 = c64.estimate(samples, 1234, 3000, 1e-9)
+    with S.Context("pcg", dims, precision=S.MIXED, batch=samples) as cm:
+        rm = cm.estimate(samples, 1234, 3000, 1e-9)
+    assert np.all(rm["results"] == 0)
+    assert O.relmax(rm["D"], r64["D"]) <= 1e-8, O.relmax(rm["D"], r64["D"])
