@@ -91,7 +91,10 @@ __device__ __forceinline__ void dacc(double &acc, T a, T b) {
 }
 
 // Map slots (Maps::m) for the per-type descriptor sets.
-enum { MT_R_HALO = 0, MT_P0_HALO, MT_P1_HALO, MT_X_INT, MT_R_INT, MT_W0_HALO, MT_W1_HALO, MT_Q_HALO };  // T fields
+enum {
+	MT_R_HALO = 0, MT_P0_HALO, MT_P1_HALO, MT_X_INT, MT_R_INT, MT_W0_HALO, MT_W1_HALO, MT_Q_HALO,
+	MT_R1_HALO, MT_V0_HALO, MT_V1_HALO
+};  // fields of type T
 enum { MD_X_HALO = 0, MD_B_INT };                                     // FP64 fields
 
 // ---------------------------------------------------------------------------
@@ -360,17 +363,24 @@ struct OpResid : OpBase<double> {
 	static constexpr int NS = 1, NQ = 1, ND = 2;
 	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
 	TR *r, *rhat, *xlo;  // stored in the TR layout (slice width WT)
+	TR *r_alt;           // BiCGStab reliable update: r buffers by iteration parity
 	double iMd;
 	int solver, ru, WT;
 	int pcg;  // reliable update of pipelined CG: the following sweeps rebuild its scalars
+	TR *rdst;
 	long long npts;
 	int it;
-	int keep[2];
+	int keep[2], restart[2];
 	__device__ bool enabled(const Global *gl) const { return !ru || gl->ru_due; }
 	__device__ bool raw_center() const { return false; }
 	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
 		it = gl->iter;
-		for (int e = 0; e < 2; e++) keep[e] = ru ? ls.done[lane + e] : 0;
+		for (int e = 0; e < 2; e++) {
+			keep[e] = ru ? ls.done[lane + e] : 0;
+			restart[e] = ru && solver == 1 && !keep[e] && ls.s_exit[lane + e] == 2;
+		}
+		// BiCGStab: iteration it+1 reads r from R[(it+1)&1 ? 0 : 1].
+		rdst = (ru && solver == 1) ? (((it + 1) & 1) ? r : r_alt) : r;
 	}
 	__device__ int src_map(int) const { return MD_X_HALO; }
 	__device__ int q_map(int) const { return MD_B_INT; }
@@ -382,11 +392,17 @@ struct OpResid : OpBase<double> {
 		for (int e = 0; e < 2; e++) {
 			const double bi = q[0].v[e];
 			const double ri = aadd(bi, -ax.v[e]);  // combine2(1.0, b, -1.0, r, r)
-			if (!keep[e]) r[ot + e] = (TR)ri;
-			if (rhat) rhat[ot + e] = (TR)ri;
+			const TR rt = (TR)ri;
+			if (!keep[e]) rdst[ot + e] = rt;
 			if (xlo) xlo[ot + e] = TR(0);
-			if (ru) part[0][e] = fma(ri, ri * iMd, part[0][e]);
-			else part[0][e] = fma(bi, bi, part[0][e]);
+			if (ru && solver == 1) {
+				if (restart[e]) rhat[ot + e] = rt;
+				part[0][e] = fma((double)rt, (double)(restart[e] ? rt : rhat[ot + e]), part[0][e]);  // rho = <r, r_hat>
+			} else {
+				if (rhat) rhat[ot + e] = rt;
+				if (ru) part[0][e] = fma(ri, ri * iMd, part[0][e]);
+				else part[0][e] = fma(bi, bi, part[0][e]);
+			}
 			part[1][e] = fma(ri, ri, part[1][e]);
 		}
 	}
@@ -409,6 +425,9 @@ struct OpResid : OpBase<double> {
 				ls.exit_iter[lane] = maxiter + 1;
 				ls.reason[lane] = STOP_MAXITER;
 				atomicSub(&gl->active, 1);
+			} else if (solver == 1) {
+				ls.rho[lane] = tot[0];  // continue from the replaced residual (restart keeps s_exit = 2)
+				if (ls.s_exit[lane] != 2) ls.s_exit[lane] = 0;
 			} else if (!pcg) {
 				ls.ru_new[lane] = tot[0];  // continue from the replaced residual
 				ls.beta[lane] = tot[0] / ls.ru[lane];
@@ -783,6 +802,258 @@ struct OpApply : OpBase<T> {
 	__device__ void fin(int, const double *, Global *, const LaneState &) const {}
 };
 
+// ---------------------------------------------------------------------------
+// BiCGStab (BiCgStab.hpp:157-232), three sweeps per iteration as in the
+// single-vector form.  r, p and v ping-pong by iteration parity (iteration
+// `it` reads R/P/V[(it&1) ? 0 : 1]-indexed as below and writes the other).
+//   1: p = r + beta (p - omega v) (p = r on iteration 1), p_hat = p .* iM,
+//      v = A p_hat, <v, r_hat>; alpha = rho / <v, r_hat>.
+//   2: s = r - alpha v, s_hat = s .* iM, t = A s_hat; <s,s>, <t,s>, <t,t>;
+//      early-exit flag on <s,s> < tol^2 or omega = <t,s>/<t,t>.
+//   3: x += alpha p_hat (+ omega s_hat), r = s - omega t, <r,r>, next rho.
+// Finished lanes are frozen with alpha = omega = 0.
+// ---------------------------------------------------------------------------
+template <class T>
+struct OpBicg1 : OpBase<T> {
+	static constexpr int NS = 3, NQ = 0, ND = 1;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr int V = Vec<T>::V;
+	T iMc;
+	T *p0, *p1, *v0, *v1, *rhat;
+	T *pn, *vn;
+	int it;
+	bool fresh[V];  // p = r: iteration 1, finished lanes, restarted lanes
+	T beta[V], bo[V];
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+		pn = (it & 1) ? p1 : p0;
+		vn = (it & 1) ? v1 : v0;
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const int l = lane + e;
+			fresh[e] = it == 1 || ls.done[l] || ls.s_exit[l] == 2;
+			double be = 0.0, bw = 0.0;
+			if (!fresh[e]) {
+				be = __dmul_rn(__ddiv_rn(ls.rho[l], ls.rho_prev[l]), __ddiv_rn(ls.alpha[l], ls.omega[l]));  // :166
+				bw = __dmul_rn(-be, ls.omega[l]);
+			}
+			beta[e] = (T)be;
+			bo[e] = (T)bw;
+		}
+	}
+	__device__ bool raw_center() const { return true; }
+	__device__ int src_map(int s) const {
+		if (s == 0) return (it & 1) ? MT_R_HALO : MT_R1_HALO;
+		if (s == 1) return (it & 1) ? MT_P0_HALO : MT_P1_HALO;
+		return (it & 1) ? MT_V0_HALO : MT_V1_HALO;
+	}
+	__device__ int q_map(int) const { return 0; }
+	__device__ Vec<T> pval(const Vec<T> *raw) const {
+		Vec<T> o;
+#pragma unroll
+		for (int e = 0; e < V; e++)
+			o.v[e] = fresh[e] ? raw[0].v[e]  // :171
+			                  : aadd(aadd(raw[0].v[e], amul(beta[e], raw[1].v[e])), amul(bo[e], raw[2].v[e]));  // :168
+		return o;
+	}
+	__device__ Vec<T> src(const Vec<T> *raw) const {
+		Vec<T> o = pval(raw);
+#pragma unroll
+		for (int e = 0; e < V; e++) o.v[e] = amul(o.v[e], iMc);  // p_hat (:175)
+		return o;
+	}
+	__device__ void out(long long o, long long, int, const Vec<T> &, const Vec<T> &vv, const Vec<T> *, const Vec<T> *rc,
+	                    double (&part)[ND][V]) const {
+		stg(pn + o, pval(rc));
+		stg(vn + o, vv);
+		const Vec<T> rh = ldg_rw(rhat + o);
+#pragma unroll
+		for (int e = 0; e < V; e++) dacc(part[0][e], vv.v[e], rh.v[e]);
+	}
+	__device__ void fin(int lane, const double *tot, Global *, const LaneState &ls) const {
+		if (ls.done[lane]) {
+			ls.alpha[lane] = 0.0;
+			return;
+		}
+		ls.alpha[lane] = __ddiv_rn(ls.rho[lane], tot[0]);  // :186
+	}
+};
+
+template <class T>
+struct OpBicgS : OpBase<T> {  // sweeps 2 and 3 share s, s_hat, t
+	static constexpr int V = Vec<T>::V;
+	T iMc;
+	int it;
+	T alpha[V];
+	__device__ void load_alpha(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+#pragma unroll
+		for (int e = 0; e < V; e++) alpha[e] = (T)(ls.done[lane + e] ? 0.0 : ls.alpha[lane + e]);
+	}
+	__device__ int src_map(int s) const {
+		if (s == 0) return (it & 1) ? MT_R_HALO : MT_R1_HALO;
+		return (it & 1) ? MT_V1_HALO : MT_V0_HALO;  // v written by sweep 1 of this iteration
+	}
+	__device__ Vec<T> sval(const Vec<T> *raw) const {
+		Vec<T> o;
+#pragma unroll
+		for (int e = 0; e < V; e++) o.v[e] = aadd(raw[0].v[e], amul(-alpha[e], raw[1].v[e]));  // :189
+		return o;
+	}
+	__device__ Vec<T> src(const Vec<T> *raw) const {
+		Vec<T> o = sval(raw);
+#pragma unroll
+		for (int e = 0; e < V; e++) o.v[e] = amul(o.v[e], iMc);  // s_hat (:201)
+		return o;
+	}
+};
+
+template <class T>
+struct OpBicg2 : OpBicgS<T> {
+	static constexpr int NS = 2, NQ = 0, ND = 3;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr int V = Vec<T>::V;
+	__device__ bool enabled(const Global *) const { return true; }
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) { this->load_alpha(gl, ls, lane); }
+	__device__ bool raw_center() const { return true; }
+	__device__ int q_map(int) const { return 0; }
+	__device__ void out(long long, long long, int, const Vec<T> &, const Vec<T> &tv, const Vec<T> *, const Vec<T> *rc,
+	                    double (&part)[ND][V]) const {
+		const Vec<T> sv = this->sval(rc);
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			dacc(part[0][e], sv.v[e], sv.v[e]);
+			dacc(part[1][e], tv.v[e], sv.v[e]);
+			dacc(part[2][e], tv.v[e], tv.v[e]);
+		}
+	}
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		if (ls.done[lane]) return;
+		ls.s_norm2[lane] = tot[0];  // :192-193
+		ls.ts[lane] = tot[1];
+		ls.tt[lane] = tot[2];
+		if (tot[0] < __dmul_rn(gl->tol, gl->tol)) {
+			ls.s_exit[lane] = 1;  // :194
+		} else {
+			ls.s_exit[lane] = 0;
+			ls.omega[lane] = __ddiv_rn(tot[1], tot[2]);  // :212
+		}
+	}
+};
+
+template <class T>
+struct OpBicg3 : OpBicgS<T> {
+	static constexpr int NS = 2, NQ = 0, ND = 2;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr int V = Vec<T>::V;
+	T *x, *r0, *r1, *p0, *p1, *rhat;
+	T *rn, *pc;
+	int mixed;
+	T omega[V];
+	int mode[V];  // 0: full update, 1: early exit on s (x only), 2: finished lane (x, r kept)
+	__device__ bool enabled(const Global *) const { return true; }
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		this->load_alpha(gl, ls, lane);
+		const int it = this->it;
+		rn = (it & 1) ? r1 : r0;
+		pc = (it & 1) ? p1 : p0;
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const int l = lane + e;
+			mode[e] = ls.done[l] ? 2 : (ls.s_exit[l] ? 1 : 0);
+			omega[e] = (T)(mode[e] ? 0.0 : ls.omega[l]);
+		}
+	}
+	__device__ bool raw_center() const { return true; }
+	__device__ int q_map(int) const { return 0; }
+	__device__ void out(long long o, long long, int, const Vec<T> &shv, const Vec<T> &tv, const Vec<T> *, const Vec<T> *rc,
+	                    double (&part)[ND][V]) const {
+		const Vec<T> sv = this->sval(rc);
+		Vec<T> xv = ldg_rw(x + o);
+		const Vec<T> pv = ldg_rw(pc + o), rh = ldg_rw(rhat + o);
+		Vec<T> rv;
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const T ph = amul(pv.v[e], this->iMc);
+			if (mode[e] == 2) {
+				rv.v[e] = rc[0].v[e];
+			} else if (mode[e] == 1) {
+				xv.v[e] = aadd(xv.v[e], amul(this->alpha[e], ph));  // :196
+				rv.v[e] = rc[0].v[e];
+			} else {
+				xv.v[e] = aadd(aadd(xv.v[e], amul(this->alpha[e], ph)), amul(omega[e], shv.v[e]));  // :216
+				rv.v[e] = aadd(sv.v[e], amul(-omega[e], tv.v[e]));                                  // :219
+			}
+			dacc(part[0][e], rv.v[e], rv.v[e]);
+			dacc(part[1][e], rv.v[e], rh.v[e]);
+		}
+		stg(x + o, xv);
+		stg(rn + o, rv);
+	}
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		if (ls.done[lane]) return;
+		const int it = this->it;
+		const double tol = gl->tol;
+		const int maxiter = gl->maxiter;
+		if (ls.s_exit[lane]) {
+			if (mixed) {
+				// The FP64 true residual decides; if it is still above tol the
+				// lane restarts from it (s_exit = 2: r_hat = r, p = r).
+				ls.s_exit[lane] = 2;
+				ls.pending[lane] = 1;
+				gl->ru_due = 1;
+				return;
+			}
+			ls.done[lane] = 1;
+			ls.exit_iter[lane] = it;
+			ls.reason[lane] = STOP_SNORM;
+			atomicSub(&gl->active, 1);
+			return;
+		}
+		ls.rr[lane] = tot[0];
+		const double err = sqrt(__ddiv_rn(tot[0], ls.bb[lane]));  // :226
+		ls.err[lane] = err;
+		const double om = ls.omega[lane];
+		if (mixed) {
+			ls.rho_prev[lane] = ls.rho[lane];
+			ls.rho[lane] = tot[1];
+			if (om == 0.0 || tot[1] == 0.0) ls.s_exit[lane] = 2;  // breakdown: restart unless converged
+			if (err <= tol || it >= maxiter || om == 0.0 || tot[1] == 0.0) {
+				ls.pending[lane] = 1;
+				gl->ru_due = 1;
+			}
+			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = 1;
+			return;
+		}
+		int stop = STOP_NONE, ex = 0;
+		if (err <= tol) {                      // :228
+			stop = STOP_CONVERGED;
+			ex = it;
+		} else if (om == 0.0) {                // :229
+			stop = STOP_OMEGA;
+			ex = it;
+		} else {
+			ls.rho_prev[lane] = ls.rho[lane];  // :231
+			if (it >= maxiter) {
+				stop = STOP_MAXITER;
+				ex = maxiter + 1;
+			} else {
+				ls.rho[lane] = tot[1];           // next iteration :159-160
+				if (tot[1] == 0.0) {             // :162
+					stop = STOP_RHO;
+					ex = it + 1;
+				}
+			}
+		}
+		if (stop != STOP_NONE) {
+			ls.done[lane] = 1;
+			ls.exit_iter[lane] = ex;
+			ls.reason[lane] = stop;
+			atomicSub(&gl->active, 1);
+		}
+	}
+};
+
 // Iteration bookkeeping between launches.
 __global__ void kb_next_iter(Global *gl) {
 	if (gl->active == 0) return;
@@ -921,6 +1192,7 @@ struct Batched {
 	double *b = nullptr;   // right-hand sides (FP64)
 	void *r = nullptr, *p0 = nullptr, *p1 = nullptr;
 	void *w[2] = {nullptr, nullptr}, *u = nullptr, *q = nullptr, *sv = nullptr, *z = nullptr;  // pipelined CG
+	void *r1 = nullptr, *v[2] = {nullptr, nullptr}, *rhat = nullptr;                        // BiCGStab
 	double *partials = nullptr;
 	unsigned *ticket = nullptr;
 	Global *gl = nullptr, *gl_host = nullptr;
@@ -1030,10 +1302,6 @@ int batched_alloc(Ctx *c) {
 		c->error = "batch too large for one context (max 256 FP32 / 128 FP64 right-hand sides)";
 		return SEDI_ERR_ARG;
 	}
-	if (c->solver == 1) {
-		c->error = "batched form implemented for CG and pipelined CG";
-		return SEDI_ERR_UNSUPPORTED;
-	}
 	if (!encode_fn()) {
 		c->error = "cuTensorMapEncodeTiled unavailable";
 		return SEDI_ERR_NODEV;
@@ -1063,15 +1331,18 @@ int batched_alloc(Ctx *c) {
 		c->error = "device allocation failed (batched form)";
 		return SEDI_ERR_NOMEM;
 	}
-	if (c->solver == 3) {
-		void **pv[] = {&B->w[0], &B->w[1], &B->u, &B->q, &B->sv, &B->z};
-		for (void **pp : pv) {
-			if (cudaMalloc(pp, B->elems * ts) != cudaSuccess) {
+	if (c->solver == 3 || c->solver == 1) {
+		void **pcg[] = {&B->w[0], &B->w[1], &B->u, &B->q, &B->sv, &B->z};
+		void **bicg[] = {&B->r1, &B->v[0], &B->v[1], &B->rhat};
+		void ***pv = c->solver == 3 ? pcg : bicg;
+		const int np = c->solver == 3 ? 6 : 4;
+		for (int i = 0; i < np; i++) {
+			if (cudaMalloc(pv[i], B->elems * ts) != cudaSuccess) {
 				cudaGetLastError();
-				c->error = "device allocation failed (batched pipelined CG)";
+				c->error = "device allocation failed (batched solver vectors)";
 				return SEDI_ERR_NOMEM;
 			}
-			cudaMemset(*pp, 0, B->elems * ts);
+			cudaMemset(*pv[i], 0, B->elems * ts);
 		}
 	}
 	cudaMemset(B->ticket, 0, sizeof(unsigned));
@@ -1099,6 +1370,10 @@ int batched_alloc(Ctx *c) {
 		ok = ok && make_map(&B->mapsT.m[MT_W0_HALO], B->w[0], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
 		     make_map(&B->mapsT.m[MT_W1_HALO], B->w[1], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
 		     make_map(&B->mapsT.m[MT_Q_HALO], B->q, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2);
+	if (c->solver == 1)
+		ok = ok && make_map(&B->mapsT.m[MT_R1_HALO], B->r1, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
+		     make_map(&B->mapsT.m[MT_V0_HALO], B->v[0], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
+		     make_map(&B->mapsT.m[MT_V1_HALO], B->v[1], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2);
 	tile_for(B->rbD, 8, &P1, &P2);
 	ok = ok && make_map(&B->mapsD.m[MD_X_HALO], B->mixed ? (void *)B->xh : B->x, 8, c->g, R, B->rbD, P1 + 2, P2 + 2) &&
 	     make_map(&B->mapsD.m[MD_B_INT], B->b, 8, c->g, R, B->rbD, P1, P2);
@@ -1113,7 +1388,8 @@ void batched_free(Ctx *c) {
 	Batched *B = (Batched *)c->batched;
 	if (!B) return;
 	void *ptrs[] = {B->x, B->xh, B->b, B->r, B->p0, B->p1, B->partials, B->ticket, B->gl, B->lane_mem, B->lane_int,
-	                B->t_acc, B->q_acc, B->w[0], B->w[1], B->u, B->q, B->sv, B->z};
+	                B->t_acc, B->q_acc, B->w[0], B->w[1], B->u, B->q, B->sv, B->z, B->r1, B->v[0], B->v[1],
+	                B->rhat};
 	for (void *p : ptrs)
 		if (p) cudaFree(p);
 	if (B->gl_host) cudaFreeHost(B->gl_host);
@@ -1133,7 +1409,8 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 		op.kb = c->k.b;
 		op.kc = c->k.c;
 		op.r = (float *)B->r;
-		op.rhat = nullptr;
+		op.r_alt = (float *)B->r1;
+		op.rhat = (float *)B->rhat;  // BiCGStab only (null otherwise)
 		op.xlo = ru ? nullptr : (float *)B->x;
 		op.WT = B->rbT;
 		op.npts = c->g.n;
@@ -1148,7 +1425,8 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 		op.kb = c->k.b;
 		op.kc = c->k.c;
 		op.r = (double *)B->r;
-		op.rhat = nullptr;
+		op.r_alt = (double *)B->r1;
+		op.rhat = (double *)B->rhat;
 		op.xlo = nullptr;
 		op.WT = B->rbT;
 		op.npts = c->g.n;
@@ -1266,6 +1544,56 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 }
 
 template <class T, int RBT, int RBD>
+static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
+	typedef typename CfgFor<T, RBT>::type C;
+	cudaStream_t s = c->stream;
+	const T ka = (T)c->k.a, kb = (T)c->k.b, kc = (T)c->k.c, iMc = (T)(1.0 / c->k.a);
+	OpBicg1<T> o1;
+	o1.ka = ka;
+	o1.kb = kb;
+	o1.kc = kc;
+	o1.iMc = iMc;
+	o1.p0 = (T *)B->p0;
+	o1.p1 = (T *)B->p1;
+	o1.v0 = (T *)B->v[0];
+	o1.v1 = (T *)B->v[1];
+	o1.rhat = (T *)B->rhat;
+	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o1, s);
+	OpBicg2<T> o2;
+	o2.ka = ka;
+	o2.kb = kb;
+	o2.kc = kc;
+	o2.iMc = iMc;
+	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o2, s);
+	OpBicg3<T> o3;
+	o3.ka = ka;
+	o3.kb = kb;
+	o3.kc = kc;
+	o3.iMc = iMc;
+	o3.x = (T *)B->x;
+	o3.r0 = (T *)B->r;
+	o3.r1 = (T *)B->r1;
+	o3.p0 = (T *)B->p0;
+	o3.p1 = (T *)B->p1;
+	o3.rhat = (T *)B->rhat;
+	o3.mixed = B->mixed ? 1 : 0;
+	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o3, s);
+	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
+	c->launches++;
+	if (B->mixed) {
+		// Reliable update: x_hi += x_lo; r = b - A x_hi (FP64) into the r buffer
+		// the next iteration reads; rho = <r, r_hat> (restarted lanes: r_hat = r).
+		const long long nb = ((long long)B->elems / 2 + 255) / 256;
+		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
+		                                                                 (float *)B->x, B->gl);
+		c->launches++;
+		enqueue_resid<RBD>(c, B, true);
+		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
+		c->launches++;
+	}
+}
+
+template <class T, int RBT, int RBD>
 static int run_batched(Ctx *c, Batched *B, int maxiter, double tol) {
 	cudaStream_t s = c->stream;
 	Global g0 = {};
@@ -1295,6 +1623,7 @@ static int run_batched(Ctx *c, Batched *B, int maxiter, double tol) {
 		BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
 		for (int i = 0; i < B->chunk; i++) {
 			if (c->solver == 3) enqueue_pcg_iteration<T, RBT, RBD>(c, B);
+			else if (c->solver == 1) enqueue_bicg_iteration<T, RBT, RBD>(c, B);
 			else enqueue_cg_iteration<T, RBT, RBD>(c, B);
 		}
 		BTRY(cudaStreamEndCapture(s, &graph));
@@ -1349,20 +1678,45 @@ static int dispatch_run(Ctx *c, Batched *B, int maxiter, double tol) {
 	}
 }
 
-// Result per lane with the reference post-loop logic (Cg.hpp:197-206).
-static int lane_result(int reason, int exit_iter, double err, double tol, int maxiter, double *fe, int *fi) {
-	if (reason == STOP_EARLY) {
+// Per-lane scalars the post-loop logic reads.
+struct LaneOut {
+	int reason, exit_iter;
+	double err, bb, s_norm2, omega, rho;
+};
+
+// Result per lane with the reference post-loop logic (Cg.hpp:197-206,
+// BiCgStab.hpp:234-262; the BiCGStab breakdown branches only in the FP64
+// form: MIXED lanes stop on their FP64 true residual or at maxiter).
+static int lane_result(const LaneOut &l, bool bicg, double tol, int maxiter, double *fe, int *fi) {
+	if (l.reason == STOP_EARLY) {
 		*fi = 0;
-		*fe = err;
+		*fe = l.err;
 		return 0;
 	}
-	if (err <= tol) {
-		*fi = exit_iter;
-		*fe = err;
+	if (l.err <= tol) {
+		*fi = l.exit_iter;
+		*fe = l.err;
 		return 0;
+	}
+	if (bicg) {
+		if (l.s_norm2 <= tol * tol) {
+			*fi = l.exit_iter;
+			*fe = std::sqrt(l.s_norm2 / l.bb);
+			return 0;
+		}
+		if (l.omega == 0.0) {
+			*fi = l.exit_iter;
+			*fe = l.err;
+			return 3;
+		}
+		if (l.rho == 0.0) {
+			*fi = l.exit_iter;
+			*fe = l.err;
+			return 2;
+		}
 	}
 	*fi = maxiter;
-	*fe = err;
+	*fe = l.err;
 	return 1;
 }
 
@@ -1372,14 +1726,24 @@ static int batched_run_resident(Ctx *c, int nrhs, int maxiter, double tol, doubl
 	B->gl_host->nrhs = nrhs;
 	int rc = dispatch_run(c, B, maxiter, tol);
 	if (rc) return rc;
-	std::vector<double> err(B->R);
-	std::vector<int> lint(5 * B->R);
-	BTRY(cudaMemcpy(err.data(), B->ls.err, sizeof(double) * B->R, cudaMemcpyDeviceToHost));
-	BTRY(cudaMemcpy(lint.data(), B->lane_int, sizeof(int) * 5 * B->R, cudaMemcpyDeviceToHost));
+	const int R = B->R;
+	std::vector<double> lm(18 * R);
+	std::vector<int> lint(5 * R);
+	BTRY(cudaMemcpy(lm.data(), B->lane_mem, sizeof(double) * 18 * R, cudaMemcpyDeviceToHost));
+	BTRY(cudaMemcpy(lint.data(), B->lane_int, sizeof(int) * 5 * R, cudaMemcpyDeviceToHost));
+	auto at = [&](const double *dev, int j) { return lm[(size_t)(dev - B->lane_mem) + j]; };
+	const bool bicg = c->solver == 1 && !B->mixed;
 	int worst = 0;
 	for (int j = 0; j < nrhs; j++) {
-		const int reason = lint[2 * B->R + j], ex = lint[1 * B->R + j];
-		const int res = lane_result(reason, ex, err[j], tol, maxiter, &final_err[j], &final_iter[j]);
+		LaneOut l;
+		l.reason = lint[2 * R + j];
+		l.exit_iter = lint[1 * R + j];
+		l.err = at(B->ls.err, j);
+		l.bb = at(B->ls.bb, j);
+		l.s_norm2 = at(B->ls.s_norm2, j);
+		l.omega = at(B->ls.omega, j);
+		l.rho = at(B->ls.rho, j);
+		const int res = lane_result(l, bicg, tol, maxiter, &final_err[j], &final_iter[j]);
 		if (results) results[j] = res;
 		if (res > worst) worst = res;
 	}
@@ -1476,6 +1840,63 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		cudaEventDestroy(e0);
 		cudaEventDestroy(e1);
 		*count = 1;
+		BTRY(cudaGetLastError());
+		return 0;
+	}
+	if (c->solver == 1) {
+		const T ka = (T)c->k.a, kb = (T)c->k.b, kc = (T)c->k.c, iMc = (T)(1.0 / c->k.a);
+		OpBicg1<T> o1;
+		o1.ka = ka;
+		o1.kb = kb;
+		o1.kc = kc;
+		o1.iMc = iMc;
+		o1.p0 = (T *)B->p0;
+		o1.p1 = (T *)B->p1;
+		o1.v0 = (T *)B->v[0];
+		o1.v1 = (T *)B->v[1];
+		o1.rhat = (T *)B->rhat;
+		OpBicg2<T> o2;
+		o2.ka = ka;
+		o2.kb = kb;
+		o2.kc = kc;
+		o2.iMc = iMc;
+		OpBicg3<T> o3;
+		o3.ka = ka;
+		o3.kb = kb;
+		o3.kc = kc;
+		o3.iMc = iMc;
+		o3.x = (T *)B->x;
+		o3.r0 = (T *)B->r;
+		o3.r1 = (T *)B->r1;
+		o3.p0 = (T *)B->p0;
+		o3.p1 = (T *)B->p1;
+		o3.rhat = (T *)B->rhat;
+		o3.mixed = 0;
+		// Lanes run the full update (no early exit) with zero scalars.
+		BTRY(cudaMemsetAsync(B->ls.s_exit, 0, sizeof(int) * B->R, s));
+		const char *nm[3] = {"bicg_1", "bicg_2", "bicg_3"};
+		const double words[3] = {6.0, 2.0, 7.0};  // 1: r, p, v, r_hat in, p, v out; 2: r, v in;
+		                                          // 3: r, v, x, p, r_hat in, x, r out
+		for (int k = 0; k < 3; k++) {
+			auto one = [&]() {
+				if (k == 0) launch<C>(c, B, B->gT, B->gridT, B->mapsT, o1, s);
+				else if (k == 1) launch<C>(c, B, B->gT, B->gridT, B->mapsT, o2, s);
+				else launch<C>(c, B, B->gT, B->gridT, B->mapsT, o3, s);
+			};
+			one();
+			BTRY(cudaEventRecord(e0, s));
+			for (int i = 0; i < reps; i++) one();
+			BTRY(cudaEventRecord(e1, s));
+			BTRY(cudaEventSynchronize(e1));
+			float t = 0.f;
+			BTRY(cudaEventElapsedTime(&t, e0, e1));
+			ms[k] = (double)t / reps;
+			bytes[k] = words[k] * ts;
+			snprintf(names + 32 * k, 32, "%s_%s", nm[k], B->mixed ? "fp32" : "fp64");
+		}
+		cudaEventDestroy(e0);
+		cudaEventDestroy(e1);
+		*count = 3;
 		BTRY(cudaGetLastError());
 		return 0;
 	}

@@ -31,7 +31,7 @@ namespace sedi {
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s
 
 struct Maps {
-	CUtensorMap m[8];
+	CUtensorMap m[12];
 };
 
 template <class T>

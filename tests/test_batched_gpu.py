@@ -167,3 +167,97 @@ def test_mixed_pcg_estimator_diagonal_error():
         rm = cm.estimate(samples, 1234, 3000, 1e-9)
     assert np.all(rm["results"] == 0)
     assert O.relmax(rm["D"], r64["D"]) <= 1e-8, O.relmax(rm["D"], r64["D"])
+
+
+# BiCGStab: FP64 lanes follow the single-vector parity bars (1e-10 in x up to
+# 20 iterations with identical result codes and counts; converged runs 1e-6
+# with counts within 15%: the reference's own BiCGStab iterates move by 1.5e-3
+# between two floating-point contractions of the same source).
+@pytest.mark.parametrize("nrhs", [1, 5, 16])
+def test_fp64_batch_bicgstab_fixed_iterations(nrhs):
+    dims = (24, 20, 16)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(700 + k, n) for k in range(nrhs)])
+    X = np.zeros_like(B)
+    with S.Context("bicgstab", dims, batch=nrhs) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=15, tol=0.0)
+    for k in range(nrhs):
+        rc0, fe0, fi0, x0, _ = O.solve(1, dims, B[k], maxiter=15, tol=0.0)
+        assert (res[k], fi[k]) == (rc0, fi0)
+        assert O.relmax(X[k], x0) <= 1e-10
+        assert abs(fe[k] - fe0) <= 1e-8 * fe0 + 1e-15
+
+
+def test_fp64_batch_bicgstab_estimator_vs_reference():
+    g = O.golden("bicgstab_32_m20")
+    m = g["meta"]
+    with S.Context("bicgstab", m["grid"], batch=8) as c:
+        r = c.estimate(m["samples"], m["seed"], m["maxiter"], m["tol"], ignore_errors=True)
+    assert np.array_equal(r["iters"], g["iters"]) and np.array_equal(r["results"], g["results"])
+    assert O.relmax(r["D"], g["D"]) <= 1e-10
+    assert np.all(np.abs(r["errs"] - g["errs"]) <= 1e-8 * np.abs(g["errs"]) + 1e-15)
+
+
+def test_fp64_batch_bicgstab_converged_vs_reference():
+    g = O.golden("conv_bicgstab_24x20x16")
+    m = g["meta"]
+    with S.Context("bicgstab", m["grid"], batch=16) as c:
+        r = c.estimate(m["samples"], m["seed"], m["maxiter"], m["tol"], ignore_errors=True)
+    assert np.array_equal(r["results"], g["results"])
+    assert np.all(np.abs(r["iters"] - g["iters"]) <= np.ceil(0.15 * g["iters"]) + 1)
+    assert O.relmax(r["D"], g["D"]) <= 1e-6
+
+
+def test_fp64_batch_bicgstab_edge_lanes():
+    """Zero right-hand side with tol 0 (rho = 0 at iteration 1: the reference
+    reports success at iteration 1), a maxiter stop, and padding lanes."""
+    dims = (12, 10, 8)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(5, n), np.zeros(n), O.fill_probe(6, n)])
+    X = np.zeros_like(B)
+    with S.Context("bicgstab", dims, batch=7) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=6, tol=0.0)
+    for k in range(3):
+        rc0, fe0, fi0, x0, _ = O.solve(1, dims, B[k], maxiter=6, tol=0.0)
+        assert (res[k], fi[k]) == (rc0, fi0), k
+        assert O.relmax(X[k], x0) <= 1e-10 if k != 1 else np.all(X[k] == 0.0)
+    assert (res[1], fi[1], fe[1]) == (0, 1, 0.0)
+
+
+@pytest.mark.parametrize("nrhs,tol", [(4, 1e-9), (32, 1e-10)])
+def test_mixed_batch_bicgstab_true_residual(nrhs, tol):
+    dims = (24, 22, 20)
+    n = int(np.prod(dims))
+    B = np.stack([O.fill_probe(41 + k, n) for k in range(nrhs)])
+    X = np.zeros_like(B)
+    with S.Context("bicgstab", dims, precision=S.MIXED, batch=nrhs) as c:
+        res, fe, fi = c.solve_batch(X, B, maxiter=3000, tol=tol)
+    assert np.all(res == 0)
+    for k in range(nrhs):
+        e = true_err(dims, X[k], B[k])
+        assert e <= tol * 1.0000001, (k, e)
+        assert abs(fe[k] - e) <= 1e-3 * e + 1e-16
+    fi64 = O.solve(1, dims, B[0], maxiter=3000, tol=tol)[2]
+    assert fi[0] <= fi64 * 1.5 + 10
+
+
+def test_mixed_bicgstab_estimator_diagonal_error():
+    """BiCGStab does not minimise an error norm, so two solves that both meet
+    tol land further apart than CG's: the bar is 1e-7 (the reference's own
+    BiCGStab D moves by 2e-7 between two floating-point contractions of the
+    same source at 128^3)."""
+    dims = (32, 32, 32)
+    samples = 16
+    with S.Context("bicgstab", dims, batch=samples) as c64:
+        r64 = c64.estimate(samples, 1234, 3000, 1e-9)
+    with S.Context("bicgstab", dims, precision=S.MIXED, batch=samples) as cm:
+        rm = cm.estimate(samples, 1234, 3000, 1e-9)
+    assert np.all(rm["results"] == 0)
+    assert O.relmax(rm["D"], r64["D"]) <= 1e-7, O.relmax(rm["D"], r64["D"])
+
+
+@pytest.mark.parametrize("solver,nk", [("cg", 2), ("pcg", 1), ("bicgstab", 3)])
+def test_time_kernels_lists_solver_sweeps(solver, nk):
+    with S.Context(solver, (64, 64, 64), precision=S.MIXED, batch=16) as c:
+        ks = c.time_kernels(reps=2)
+    assert len(ks) == nk and all(ms > 0 and by > 0 for _, ms, by in ks)
