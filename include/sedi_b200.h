@@ -196,6 +196,69 @@ long long sedi_launch_count(const sedi_ctx *ctx);
 /* Library version string. */
 const char *sedi_version(void);
 
+/*
+ * Estimation-job server (no counterpart in the reference, which runs one
+ * estimate per process: stochastic-estimator.cc:57-232).  Jobs of any grid,
+ * sample count, tolerance, solver and precision are admitted as they arrive
+ * while their device bytes fit the budget, each on its own batched context
+ * and CUDA stream with all Krylov state resident on the GPU; running jobs
+ * overlap on the device and advance without blocking one another.  Every job
+ * is an estimator run with seeded device probes (probe k of a job is
+ * std::mt19937(seed + k), as DistrRngStd draws them), x = 0, the 7-point
+ * operator a = 6, b = c = 1, iM = 1/6 and -i semantics (all samples run;
+ * per-probe result codes are reported).  A job's result does not depend on
+ * what else runs: the same job gives the same D alone and in any mix.
+ * Not thread-safe: one thread drives a server.
+ */
+typedef struct sedi_server sedi_server;
+
+/* budget_bytes: device memory for job contexts (0: 85% of the free memory);
+ * max_active: jobs running at once (0: 8); job_cap_bytes: largest context of
+ * one job (0: 32 GiB) -- a job whose samples do not fit runs in batches. */
+sedi_server *sedi_server_create(double budget_bytes, int max_active, double job_cap_bytes, int *err);
+void sedi_server_destroy(sedi_server *srv);
+
+/* Queue a job; returns its id (>= 0) or a negative error (SEDI_ERR_NOMEM
+ * when even one batch of it exceeds the budget). */
+long sedi_server_submit(sedi_server *srv, int solver, int precision, long n1, long n2, long n3, int samples,
+                        uint32_t seed, int maxiter, double tol);
+
+/* Advance every running job and admit queued ones, without waiting on the
+ * GPU.  Returns the number of jobs queued or running; *completed (optional)
+ * = jobs finished since creation. */
+int sedi_server_step(sedi_server *srv, int *completed);
+
+/* Step until job `id` is finished (id < 0: until no job is left). */
+int sedi_server_wait(sedi_server *srv, long id);
+
+/* state: 0 queued, 1 running, 2 done, 3 failed; rc: the estimator's code
+ * (worst per-probe result, or a negative error); times in seconds on the
+ * server's clock; lanes: right-hand sides per batch; bytes: device bytes of
+ * its context.  Any output may be NULL. */
+int sedi_server_job_info(sedi_server *srv, long id, int *state, int *rc, double *t_submit, double *t_start,
+                         double *t_done, int *lanes, double *bytes);
+
+/* Copy out a finished job's D (n1*n2*n3), per-probe iterations, final errors
+ * and result codes (any may be NULL) and forget the job.  Returns its rc. */
+int sedi_server_take(sedi_server *srv, long id, double *D, int *iters, double *errs, int *results);
+
+/* Open-loop replay: job k (cubic grid edge[k]) is submitted when arrival_s[k]
+ * seconds (non-decreasing) have passed since the call; the server runs until
+ * all are done.  latency_s[k] = done - scheduled arrival; rcs[k] (optional)
+ * its code; *makespan_s (optional) = first arrival to last completion.
+ * Results are discarded. */
+int sedi_server_replay(sedi_server *srv, int njobs, const double *arrival_s, const int *solver, const int *precision,
+                       const long *edge, const int *samples, const uint32_t *seed, const double *tol, int maxiter,
+                       double *latency_s, int *rcs, double *makespan_s);
+
+/* Peak device bytes held, the budget, contexts created and reused, most jobs
+ * running at once, kernel launches of finished jobs. */
+int sedi_server_stats(const sedi_server *srv, double *peak_bytes, double *budget_bytes, int *ctx_created,
+                      int *ctx_reused, int *max_running, long long *launches);
+
+/* Device bytes of a batched context (the server's admission size). */
+double sedi_job_bytes(int solver, int precision, int lanes, long n1, long n2, long n3);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,8 +26,8 @@ import os
 import numpy as np
 
 __all__ = [
-    "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "estimate", "fill_probe",
-    "library_path", "load", "SOLVER_IDS", "FP64", "MIXED",
+    "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "Server", "estimate", "fill_probe",
+    "job_bytes", "library_path", "load", "SOLVER_IDS", "FP64", "MIXED",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -86,6 +86,21 @@ def load():
     lib.sedi_time_kernels.argtypes = [vp, c_int, vp, vp, vp, vp]
     lib.sedi_fill_probes_dev.argtypes = [ctypes.c_uint32, c_int, c_long, vp, vp]
     lib.sedi_residual_noalloc.argtypes = [c_long, c_long, c_long, c_double, c_double, c_double, vp, vp, vp, pd, vp]
+    lib.sedi_server_create.restype = vp
+    lib.sedi_server_create.argtypes = [c_double, c_int, c_double, pi]
+    lib.sedi_server_destroy.argtypes = [vp]
+    lib.sedi_server_destroy.restype = None
+    lib.sedi_server_submit.restype = c_long
+    lib.sedi_server_submit.argtypes = [vp, c_int, c_int, c_long, c_long, c_long, c_int, ctypes.c_uint32, c_int,
+                                       c_double]
+    lib.sedi_server_step.argtypes = [vp, pi]
+    lib.sedi_server_wait.argtypes = [vp, c_long]
+    lib.sedi_server_job_info.argtypes = [vp, c_long, pi, pi, pd, pd, pd, pi, pd]
+    lib.sedi_server_take.argtypes = [vp, c_long, vp, vp, vp, vp]
+    lib.sedi_server_replay.argtypes = [vp, c_int, vp, vp, vp, vp, vp, vp, vp, c_int, vp, vp, pd]
+    lib.sedi_server_stats.argtypes = [vp, pd, pd, pi, pi, pi, ctypes.POINTER(ctypes.c_longlong)]
+    lib.sedi_job_bytes.restype = c_double
+    lib.sedi_job_bytes.argtypes = [c_int, c_int, c_int, c_long, c_long, c_long]
     _lib = lib
     return lib
 
@@ -329,3 +344,116 @@ def estimate(solver, dims, samples, seed=1234, maxiter=1000, tol=1e-4, ignore_er
     """The estimator loop of stochastic-estimator.cc:155-216 (one call)."""
     with Context(solver, dims, stencil, 0, precision, batch) as ctx:
         return ctx.estimate(samples, seed, maxiter, tol, ignore_errors, probes)
+
+
+def job_bytes(solver, dims, lanes, precision=FP64):
+    """Device bytes of a batched context: the server's admission size."""
+    sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
+    return float(load().sedi_job_bytes(sid, int(precision), int(lanes), *[int(d) for d in dims]))
+
+
+class Server:
+    """Estimation-job server over one GPU (sedi_server_* in the C ABI).
+
+    ``submit`` queues an estimator job (seeded device probes, x = 0, -i
+    semantics) and returns its id; ``step`` advances all running jobs without
+    waiting on the GPU and admits queued jobs while their device bytes fit
+    ``budget_bytes``; ``wait`` steps until a job (or all) is done; ``take``
+    returns a finished job's results.  ``replay`` runs an open-loop arrival
+    schedule natively and returns per-job latencies."""
+
+    STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
+
+    def __init__(self, budget_bytes=0, max_active=0, job_cap_bytes=0):
+        err = ctypes.c_int(0)
+        self._h = load().sedi_server_create(float(budget_bytes), int(max_active), float(job_cap_bytes),
+                                            ctypes.byref(err))
+        if not self._h:
+            raise SediError(err.value, "sedi_server_create")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().sedi_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, solver, dims, samples, seed, maxiter, tol, precision=FP64):
+        sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
+        jid = load().sedi_server_submit(self._h, sid, int(precision), *[int(d) for d in dims], int(samples),
+                                        int(seed) & 0xFFFFFFFF, int(maxiter), float(tol))
+        if jid < 0:
+            raise SediError(int(jid), "sedi_server_submit")
+        self._dims = getattr(self, "_dims", {})
+        self._dims[jid] = (tuple(int(d) for d in dims), int(samples))
+        return jid
+
+    def step(self):
+        done = ctypes.c_int(0)
+        rc = load().sedi_server_step(self._h, ctypes.byref(done))
+        if rc < 0:
+            raise SediError(rc, "sedi_server_step")
+        return rc, done.value
+
+    def wait(self, jid=-1):
+        rc = load().sedi_server_wait(self._h, int(jid))
+        if rc < 0:
+            raise SediError(rc, "sedi_server_wait")
+
+    def info(self, jid):
+        st, rc, lanes = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ts, t0, t1, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        r = load().sedi_server_job_info(self._h, int(jid), ctypes.byref(st), ctypes.byref(rc), ctypes.byref(ts),
+                                        ctypes.byref(t0), ctypes.byref(t1), ctypes.byref(lanes), ctypes.byref(by))
+        if r < 0:
+            raise SediError(r, "sedi_server_job_info")
+        return {"state": self.STATES[st.value], "rc": rc.value, "t_submit": ts.value, "t_start": t0.value,
+                "t_done": t1.value, "lanes": lanes.value, "bytes": by.value}
+
+    def take(self, jid):
+        dims, samples = self._dims.pop(jid)
+        n = int(np.prod(dims))
+        D = np.zeros(n)
+        iters = np.zeros(samples, np.int32)
+        errs = np.zeros(samples)
+        res = np.zeros(samples, np.int32)
+        rc = load().sedi_server_take(self._h, int(jid), _ptr(D), _ptr(iters), _ptr(errs), _ptr(res))
+        if rc < 0:
+            raise SediError(rc, "job failed")
+        return {"rc": rc, "D": D, "iters": iters, "errs": errs, "results": res}
+
+    def replay(self, arrival_s, solver, precision, edge, samples, seed, tol, maxiter):
+        """Open-loop schedule (arrays of one entry per job); returns
+        (latency_s, result codes, makespan_s)."""
+        k = len(arrival_s)
+        a = np.ascontiguousarray(arrival_s, np.float64)
+        so = np.ascontiguousarray([SOLVER_IDS[x] if isinstance(x, str) else int(x) for x in solver], np.int32)
+        pr = np.ascontiguousarray(precision, np.int32)
+        ed = np.ascontiguousarray(edge, np.int64)
+        sa = np.ascontiguousarray(samples, np.int32)
+        se = np.ascontiguousarray(np.asarray(seed, np.int64) & 0xFFFFFFFF, np.uint32)
+        to = np.ascontiguousarray(tol, np.float64)
+        lat = np.zeros(k)
+        rcs = np.zeros(k, np.int32)
+        mk = ctypes.c_double(0.0)
+        r = load().sedi_server_replay(self._h, k, _ptr(a), _ptr(so), _ptr(pr), _ptr(ed), _ptr(sa), _ptr(se), _ptr(to),
+                                      int(maxiter), _ptr(lat), _ptr(rcs), ctypes.byref(mk))
+        if r < 0:
+            raise SediError(r, "sedi_server_replay")
+        return lat, rcs, mk.value
+
+    def stats(self):
+        pk, bu = ctypes.c_double(), ctypes.c_double()
+        cr, ru, mr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        la = ctypes.c_longlong()
+        load().sedi_server_stats(self._h, ctypes.byref(pk), ctypes.byref(bu), ctypes.byref(cr), ctypes.byref(ru),
+                                 ctypes.byref(mr), ctypes.byref(la))
+        return {"peak_bytes": pk.value, "budget_bytes": bu.value, "ctx_created": cr.value, "ctx_reused": ru.value,
+                "max_running": mr.value, "launches": la.value}

@@ -1060,6 +1060,8 @@ __global__ void kb_next_iter(Global *gl) {
 	if (gl->ru_due == 0) gl->iter += 1;
 }
 
+__global__ void kb_setup_done(Global *gl) { gl->active -= 1; }  // drops the setup sweep's guard
+
 __global__ void kb_ru_done(Global *gl) {
 	if (gl->ru_due) {
 		gl->ru_due = 0;
@@ -1182,6 +1184,27 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 	          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+constexpr int kLaneDoubles = 18, kLaneInts = 5;  // LaneState arrays
+
+struct Batched;
+typedef int (*SetupFn)(Ctx *, Batched *, int nrhs, int maxiter, double tol);
+typedef int (*ChunkFn)(Ctx *, Batched *);
+
+// Non-blocking estimator over the context's batches (stochastic-estimator.cc:158-216).
+enum EstStage { EST_IDLE = 0, EST_SOLVE, EST_LANES, EST_FINAL, EST_DONE };
+struct EstState {
+	int stage = EST_IDLE;
+	int samples = 0, k0 = 0, nb = 0, maxiter = 0, ignore_errors = 0, worst = 0, rc = 0;
+	double tol = 0.0;
+	uint32_t seed = 0;
+	const double *probes_dev = nullptr;
+	double *D_dev = nullptr, *t_dev = nullptr, *q_dev = nullptr, *D_host = nullptr;
+	int *iters = nullptr, *results = nullptr;
+	double *errs = nullptr;
+	bool first = true;
+	long long rounds = 0;
+};
+
 struct Batched {
 	int R = 0;
 	bool mixed = false;
@@ -1195,10 +1218,15 @@ struct Batched {
 	void *r1 = nullptr, *v[2] = {nullptr, nullptr}, *rhat = nullptr;                        // BiCGStab
 	double *partials = nullptr;
 	unsigned *ticket = nullptr;
-	Global *gl = nullptr, *gl_host = nullptr;
+	Global *gl = nullptr, *gl_host = nullptr, *g0_host = nullptr;  // gl_host[0]: read back, g0_host: setup
 	LaneState ls;
-	double *lane_mem = nullptr;
-	int *lane_int = nullptr;
+	double *lane_mem = nullptr, *lane_host = nullptr;
+	int *lane_int = nullptr, *lane_host_int = nullptr;
+	SetupFn setup_fn = nullptr;
+	ChunkFn chunk_fn = nullptr;
+	cudaEvent_t ev = nullptr;
+	EstState est;
+	std::vector<int> lane_res;  // result codes of the batch being processed
 	double *t_acc = nullptr, *q_acc = nullptr;
 	int period = 32;
 	int chunk = 16;
@@ -1293,6 +1321,8 @@ static int launch(Ctx *c, Batched *B, const SGeo &sg, dim3 grid, const Maps &map
 	return 0;
 }
 
+static void bind_impl(Batched *B);
+
 int batched_alloc(Ctx *c) {
 	Batched *B = new (std::nothrow) Batched();
 	if (!B) return SEDI_ERR_NOMEM;
@@ -1322,7 +1352,10 @@ int batched_alloc(Ctx *c) {
 	    (B->mixed && cudaMalloc(&B->xh, B->elems * sizeof(double)) != cudaSuccess) ||
 	    cudaMalloc(&B->partials, sizeof(double) * nblk * kMaxDots * B->R) != cudaSuccess ||
 	    cudaMalloc(&B->ticket, sizeof(unsigned)) != cudaSuccess || cudaMalloc(&B->gl, sizeof(Global)) != cudaSuccess ||
-	    cudaMallocHost(&B->gl_host, sizeof(Global)) != cudaSuccess ||
+	    cudaMallocHost(&B->gl_host, 2 * sizeof(Global)) != cudaSuccess ||
+	    cudaMallocHost(&B->lane_host, sizeof(double) * kLaneDoubles * B->R) != cudaSuccess ||
+	    cudaMallocHost(&B->lane_host_int, sizeof(int) * kLaneInts * B->R) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming) != cudaSuccess ||
 	    cudaMalloc(&B->lane_mem, sizeof(double) * 20 * B->R) != cudaSuccess ||
 	    cudaMalloc(&B->lane_int, sizeof(int) * 5 * B->R) != cudaSuccess ||
 	    cudaMalloc(&B->t_acc, sizeof(double) * c->g.n) != cudaSuccess ||
@@ -1381,7 +1414,35 @@ int batched_alloc(Ctx *c) {
 		c->error = "tensor map encoding failed";
 		return SEDI_ERR_CUDA;
 	}
+	B->g0_host = B->gl_host + 1;
+	B->lane_res.assign(B->R, 0);
+	bind_impl(B);
 	return 0;
+}
+
+// Device bytes batched_alloc takes for a context (each allocation rounded
+// up to the 2 MiB granularity of large device allocations).
+size_t batched_bytes(int solver, int precision, int batch, long long n1, long long n2, long long n3) {
+	const bool mixed = precision == SEDI_PREC_MIXED;
+	Geo g;
+	g.n1 = (int)n1;
+	g.n2 = (int)n2;
+	g.n3 = (int)n3;
+	g.n = n1 * n2 * n3;
+	const int R = pick_R(batch, mixed);
+	const size_t elems = (size_t)g.n * R, ts = mixed ? 4 : 8;
+	SGeo sT, sD;
+	dim3 gT, gD;
+	shape(g, R, slice_for(R, !mixed), (int)ts, &sT, &gT);
+	shape(g, R, slice_for(R, true), 8, &sD, &gD);
+	const size_t nblkT = (size_t)gT.x * gT.z, nblkD = (size_t)gD.x * gD.z;
+	const size_t nblk = nblkT > nblkD ? nblkT : nblkD;
+	auto up = [](size_t b) { return (b + (2u << 20) - 1) / (2u << 20) * (2u << 20); };
+	const int nT = 4 + (solver == 3 ? 6 : 0) + (solver == 1 ? 4 : 0);
+	size_t total = nT * up(elems * ts) + up(elems * 8) * (mixed ? 2 : 1);
+	total += up(sizeof(double) * nblk * kMaxDots * R) + 3 * up(1) + up(sizeof(double) * 20 * R) +
+	         up(sizeof(int) * 5 * R) + 2 * up(sizeof(double) * g.n);
+	return total;
 }
 
 void batched_free(Ctx *c) {
@@ -1393,6 +1454,9 @@ void batched_free(Ctx *c) {
 	for (void *p : ptrs)
 		if (p) cudaFree(p);
 	if (B->gl_host) cudaFreeHost(B->gl_host);
+	if (B->lane_host) cudaFreeHost(B->lane_host);
+	if (B->lane_host_int) cudaFreeHost(B->lane_host_int);
+	if (B->ev) cudaEventDestroy(B->ev);
 	if (B->graph) cudaGraphExecDestroy(B->graph);
 	delete B;
 	c->batched = nullptr;
@@ -1593,88 +1657,111 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	}
 }
 
+// Per-configuration driver pieces, bound to the context at allocation.
+// setup: r = b - A x for a batch already in b (and x / x_hi), per-lane <b,b>,
+// <r,r> and the initial stop test, all on the stream (no host round trip:
+// the setup sweep runs under a +1 guard on `active` that kb_setup_done drops).
+// chunk: one launch of the captured graph of `chunk` iterations; lanes and
+// launches past the stop are no-ops.
 template <class T, int RBT, int RBD>
-static int run_batched(Ctx *c, Batched *B, int maxiter, double tol) {
-	cudaStream_t s = c->stream;
-	Global g0 = {};
-	g0.iter = 1;
-	g0.maxiter = maxiter;
-	g0.tol = tol;
-	g0.period = B->period;
-	g0.nrhs = B->gl_host->nrhs;
-	g0.active = 1;  // lets the setup sweep run; its finisher adds one per live lane
-	*B->gl_host = g0;
-	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
-	enqueue_resid<RBD>(c, B, false);
-	BTRY(cudaGetLastError());
-	BTRY(cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s));
-	BTRY(cudaStreamSynchronize(s));
+struct Impl {
+	static int setup(Ctx *c, Batched *B, int nrhs, int maxiter, double tol) {
+		cudaStream_t s = c->stream;
+		Global g0 = {};
+		g0.iter = 1;
+		g0.maxiter = maxiter;
+		g0.tol = tol;
+		g0.period = B->period;
+		g0.nrhs = nrhs;
+		g0.active = 1;
+		*B->g0_host = g0;  // read by the copy below; rewritten only after this batch is over
+		BTRY(cudaMemcpyAsync(B->gl, B->g0_host, sizeof(Global), cudaMemcpyHostToDevice, s));
+		enqueue_resid<RBD>(c, B, false);
+		kb_setup_done<<<1, 1, 0, s>>>(B->gl);
+		c->launches++;
+		if (c->solver == 3) enqueue_pcg_uw<T, RBT>(c, B, 1, 0);  // :138-149 (skipped when no lane is live)
+		BTRY(cudaGetLastError());
+		return 0;
+	}
+	static int chunk(Ctx *c, Batched *B) {
+		cudaStream_t s = c->stream;
+		if (!B->graph) {
+			// The graph reads tol/maxiter/iteration only from Global (device): reusable.
+			cudaGraph_t graph;
+			const long long before = c->launches;
+			BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+			for (int i = 0; i < B->chunk; i++) {
+				if (c->solver == 3) enqueue_pcg_iteration<T, RBT, RBD>(c, B);
+				else if (c->solver == 1) enqueue_bicg_iteration<T, RBT, RBD>(c, B);
+				else enqueue_cg_iteration<T, RBT, RBD>(c, B);
+			}
+			BTRY(cudaStreamEndCapture(s, &graph));
+			B->graph_kernels = c->launches - before;
+			c->launches = before;
+			cudaError_t e = cudaGraphInstantiate(&B->graph, graph, 0);
+			cudaGraphDestroy(graph);
+			if (e != cudaSuccess) {
+				B->graph = nullptr;
+				return set_cuda_error(c, e, "cudaGraphInstantiate");
+			}
+		}
+		BTRY(cudaGraphLaunch(B->graph, s));
+		c->launches += B->graph_kernels;
+		return 0;
+	}
+};
+
+static void bind_impl(Batched *B) {
+	if (B->mixed) {
+		if (B->rbT == 4) {
+			B->setup_fn = B->rbD == 2 ? Impl<float, 4, 2>::setup : Impl<float, 4, 4>::setup;
+			B->chunk_fn = B->rbD == 2 ? Impl<float, 4, 2>::chunk : Impl<float, 4, 4>::chunk;
+		} else {
+			B->setup_fn = Impl<float, 8, 8>::setup;
+			B->chunk_fn = Impl<float, 8, 8>::chunk;
+		}
+		return;
+	}
+	switch (B->rbT) {
+	case 2:
+		B->setup_fn = Impl<double, 2, 2>::setup;
+		B->chunk_fn = Impl<double, 2, 2>::chunk;
+		break;
+	case 4:
+		B->setup_fn = Impl<double, 4, 4>::setup;
+		B->chunk_fn = Impl<double, 4, 4>::chunk;
+		break;
+	default:
+		B->setup_fn = Impl<double, 8, 8>::setup;
+		B->chunk_fn = Impl<double, 8, 8>::chunk;
+	}
+}
+
+static int check_flags(Ctx *c, Batched *B) {
 	if (B->gl_host->err) {
 		c->error = "batched sweep timed out waiting for its data";
 		return SEDI_ERR_CUDA;
 	}
-	B->gl_host->active -= 1;
-	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
-	if (c->solver == 3 && B->gl_host->active > 0) enqueue_pcg_uw<T, RBT>(c, B, 1, 0);  // :138-149
-	if (!B->graph) {
-		// The graph bakes in tol/maxiter only through Global (device), so it is reusable.
-		cudaGraph_t graph;
-		const long long before = c->launches;
-		BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-		for (int i = 0; i < B->chunk; i++) {
-			if (c->solver == 3) enqueue_pcg_iteration<T, RBT, RBD>(c, B);
-			else if (c->solver == 1) enqueue_bicg_iteration<T, RBT, RBD>(c, B);
-			else enqueue_cg_iteration<T, RBT, RBD>(c, B);
-		}
-		BTRY(cudaStreamEndCapture(s, &graph));
-		B->graph_kernels = c->launches - before;
-		c->launches = before;
-		cudaError_t e = cudaGraphInstantiate(&B->graph, graph, 0);
-		cudaGraphDestroy(graph);
-		if (e != cudaSuccess) {
-			B->graph = nullptr;
-			return set_cuda_error(c, e, "cudaGraphInstantiate");
-		}
-	}
-	long long rounds = 0;
-	const long long max_rounds = (long long)maxiter * 2 / B->chunk + 4;
-	while (B->gl_host->active > 0) {
-		BTRY(cudaGraphLaunch(B->graph, s));
-		c->launches += B->graph_kernels;
-		BTRY(cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s));
-		BTRY(cudaStreamSynchronize(s));
-		if (B->gl_host->err) {
-			c->error = "batched sweep timed out waiting for its data";
-			return SEDI_ERR_CUDA;
-		}
-		if (++rounds > max_rounds) {
-			c->error = "batched solver did not stop";
-			return SEDI_ERR_CUDA;
-		}
-	}
 	return 0;
 }
 
-template <class T, int RBT>
-static int dispatch_d(Ctx *c, Batched *B, int maxiter, double tol) {
-	switch (B->rbD) {
-	case 2: return run_batched<T, RBT, 2>(c, B, maxiter, tol);
-	case 4: return run_batched<T, RBT, 4>(c, B, maxiter, tol);
-	default: return run_batched<T, RBT, 8>(c, B, maxiter, tol);
-	}
-}
+static long long max_rounds(const Batched *B, int maxiter) { return (long long)maxiter * 2 / B->chunk + 4; }
 
-static int dispatch_run(Ctx *c, Batched *B, int maxiter, double tol) {
-	if (B->mixed) {
-		switch (B->rbT) {
-		case 4: return dispatch_d<float, 4>(c, B, maxiter, tol);
-		default: return dispatch_d<float, 8>(c, B, maxiter, tol);
+// Blocking solve of the batch in the context's buffers.
+static int run_batched(Ctx *c, Batched *B, int nrhs, int maxiter, double tol) {
+	cudaStream_t s = c->stream;
+	int rc = B->setup_fn(c, B, nrhs, maxiter, tol);
+	if (rc) return rc;
+	for (long long rounds = 0;; rounds++) {
+		if (rounds > max_rounds(B, maxiter)) {
+			c->error = "batched solver did not stop";
+			return SEDI_ERR_CUDA;
 		}
-	}
-	switch (B->rbT) {
-	case 2: return run_batched<double, 2, 2>(c, B, maxiter, tol);
-	case 4: return run_batched<double, 4, 4>(c, B, maxiter, tol);
-	default: return run_batched<double, 8, 8>(c, B, maxiter, tol);
+		if ((rc = B->chunk_fn(c, B))) return rc;
+		BTRY(cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s));
+		BTRY(cudaStreamSynchronize(s));
+		if ((rc = check_flags(c, B))) return rc;
+		if (B->gl_host->active == 0) return 0;
 	}
 }
 
@@ -1720,17 +1807,23 @@ static int lane_result(const LaneOut &l, bool bicg, double tol, int maxiter, dou
 	return 1;
 }
 
-static int batched_run_resident(Ctx *c, int nrhs, int maxiter, double tol, double *final_err, int *final_iter,
-                                int *results) {
-	Batched *B = (Batched *)c->batched;
-	B->gl_host->nrhs = nrhs;
-	int rc = dispatch_run(c, B, maxiter, tol);
-	if (rc) return rc;
+
+// Copies the per-lane state to the pinned mirror (stream-ordered).
+static int enqueue_lane_copy(Ctx *c, Batched *B) {
 	const int R = B->R;
-	std::vector<double> lm(18 * R);
-	std::vector<int> lint(5 * R);
-	BTRY(cudaMemcpy(lm.data(), B->lane_mem, sizeof(double) * 18 * R, cudaMemcpyDeviceToHost));
-	BTRY(cudaMemcpy(lint.data(), B->lane_int, sizeof(int) * 5 * R, cudaMemcpyDeviceToHost));
+	BTRY(cudaMemcpyAsync(B->lane_host, B->lane_mem, sizeof(double) * kLaneDoubles * R, cudaMemcpyDeviceToHost,
+	                     c->stream));
+	BTRY(cudaMemcpyAsync(B->lane_host_int, B->lane_int, sizeof(int) * kLaneInts * R, cudaMemcpyDeviceToHost,
+	                     c->stream));
+	return 0;
+}
+
+// Per-lane results from the pinned mirror (after enqueue_lane_copy completed).
+static int process_lanes(Ctx *c, Batched *B, int nrhs, int maxiter, double tol, double *final_err, int *final_iter,
+                         int *results) {
+	const int R = B->R;
+	const double *lm = B->lane_host;
+	const int *lint = B->lane_host_int;
 	auto at = [&](const double *dev, int j) { return lm[(size_t)(dev - B->lane_mem) + j]; };
 	const bool bicg = c->solver == 1 && !B->mixed;
 	int worst = 0;
@@ -1743,11 +1836,25 @@ static int batched_run_resident(Ctx *c, int nrhs, int maxiter, double tol, doubl
 		l.s_norm2 = at(B->ls.s_norm2, j);
 		l.omega = at(B->ls.omega, j);
 		l.rho = at(B->ls.rho, j);
-		const int res = lane_result(l, bicg, tol, maxiter, &final_err[j], &final_iter[j]);
+		double fe;
+		int fi;
+		const int res = lane_result(l, bicg, tol, maxiter, &fe, &fi);
+		if (final_err) final_err[j] = fe;
+		if (final_iter) final_iter[j] = fi;
 		if (results) results[j] = res;
 		if (res > worst) worst = res;
 	}
 	return worst;
+}
+
+static int batched_run_resident(Ctx *c, int nrhs, int maxiter, double tol, double *final_err, int *final_iter,
+                                int *results) {
+	Batched *B = (Batched *)c->batched;
+	int rc = run_batched(c, B, nrhs, maxiter, tol);
+	if (rc) return rc;
+	if ((rc = enqueue_lane_copy(c, B))) return rc;
+	BTRY(cudaStreamSynchronize(c->stream));
+	return process_lanes(c, B, nrhs, maxiter, tol, final_err, final_iter, results);
 }
 
 static int blocks1d(long long n) {
@@ -1950,56 +2057,179 @@ int batched_estimate_dev(Ctx *c, int samples, const double *probes_dev, int maxi
 	                            errs, results);
 }
 
-// Probes come from device memory (probes_dev) or, when probes_dev is NULL,
-// from the device generator (probe k = std::mt19937(seed + k)), written
-// straight into the lane-sliced right-hand-side buffer.
+// Starts the next batch of probes: fill (device generator or caller probes),
+// x = 0 (:175), setup, first chunk, status copy, event.
+static int est_start_batch(Ctx *c, Batched *B) {
+	EstState &E = B->est;
+	cudaStream_t s = c->stream;
+	const long long n = c->g.n;
+	E.nb = E.samples - E.k0 < c->batch ? E.samples - E.k0 : c->batch;
+	if (E.probes_dev) {
+		kb_interleave<<<blocks1d(n * B->R), 256, 0, s>>>(n, B->R, B->rbD, E.nb, E.probes_dev + (size_t)E.k0 * n, B->b);
+	} else {
+		if (E.nb < B->R) BTRY(cudaMemsetAsync(B->b, 0, B->elems * sizeof(double), s));  // padding lanes
+		if (device_fill_probes(E.seed + (uint32_t)E.k0, E.nb, n, B->rbD, B->b, s))
+			return set_cuda_error(c, cudaGetLastError(), "device probes");
+	}
+	c->launches++;
+	BTRY(cudaMemsetAsync(B->mixed ? (void *)B->xh : B->x, 0, B->elems * sizeof(double), s));  // x = 0 (:175)
+	int rc = B->setup_fn(c, B, E.nb, E.maxiter, E.tol);
+	if (!rc) rc = B->chunk_fn(c, B);
+	if (rc) return rc;
+	BTRY(cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s));
+	BTRY(cudaEventRecord(B->ev, s));
+	E.rounds = 0;
+	E.stage = EST_SOLVE;
+	return 0;
+}
+
+// D = t / q and the result copies.
+static int est_final(Ctx *c, Batched *B) {
+	EstState &E = B->est;
+	cudaStream_t s = c->stream;
+	const long long n = c->g.n;
+	if (E.samples == 0) {
+		BTRY(cudaMemsetAsync(B->t_acc, 0, sizeof(double) * n, s));
+		BTRY(cudaMemsetAsync(B->q_acc, 0, sizeof(double) * n, s));
+	}
+	if (E.t_dev) BTRY(cudaMemcpyAsync(E.t_dev, B->t_acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+	if (E.q_dev) BTRY(cudaMemcpyAsync(E.q_dev, B->q_acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+	kb_divide<<<blocks1d(n), 256, 0, s>>>(n, B->t_acc, B->q_acc, E.D_dev);  // :216 (D_dev may alias t_acc)
+	c->launches++;
+	if (E.D_host) BTRY(cudaMemcpyAsync(E.D_host, E.D_dev, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+	BTRY(cudaEventRecord(B->ev, s));
+	E.stage = EST_FINAL;
+	return 0;
+}
+
+int batched_est_begin(Ctx *c, int samples, const double *probes_dev, uint32_t seed, int maxiter, double tol,
+                      int ignore_errors, double *D_dev, double *t_dev, double *q_dev, double *D_host, int *iters,
+                      double *errs, int *results) {
+	Batched *B = (Batched *)c->batched;
+	if (B->est.stage != EST_IDLE && B->est.stage != EST_DONE) {
+		c->error = "an estimate is already running on this context";
+		return SEDI_ERR_ARG;
+	}
+	EstState &E = B->est;
+	E = EstState();
+	E.samples = samples;
+	E.probes_dev = probes_dev;
+	E.seed = seed;
+	E.maxiter = maxiter;
+	E.tol = tol;
+	E.ignore_errors = ignore_errors;
+	E.D_dev = D_dev ? D_dev : B->t_acc;
+	E.t_dev = t_dev;
+	E.q_dev = q_dev;
+	E.D_host = D_host;
+	E.iters = iters;
+	E.errs = errs;
+	E.results = results;
+	int rc = samples > 0 ? est_start_batch(c, B) : est_final(c, B);
+	if (rc) E.stage = EST_DONE, E.rc = rc;
+	return rc;
+}
+
+// Advances the estimate without blocking: *done = 1 once D (and D_host) are
+// ready, with the result code in the return value's place of the blocking
+// call available through batched_est_result.
+int batched_est_advance(Ctx *c, int *done) {
+	Batched *B = (Batched *)c->batched;
+	EstState &E = B->est;
+	*done = 0;
+	if (E.stage == EST_DONE || E.stage == EST_IDLE) {
+		*done = 1;
+		return E.rc < 0 ? E.rc : 0;
+	}
+	const cudaError_t q = cudaEventQuery(B->ev);
+	if (q == cudaErrorNotReady) return 0;
+	int rc = 0;
+	if (q != cudaSuccess) rc = set_cuda_error(c, q, "estimate");
+	cudaStream_t s = c->stream;
+	const long long n = c->g.n;
+	if (!rc) switch (E.stage) {
+	case EST_SOLVE:
+		if ((rc = check_flags(c, B))) break;
+		if (B->gl_host->active > 0) {
+			if (++E.rounds > max_rounds(B, E.maxiter)) {
+				c->error = "batched solver did not stop";
+				rc = SEDI_ERR_CUDA;
+				break;
+			}
+			if ((rc = B->chunk_fn(c, B))) break;
+			if (cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+			    cudaEventRecord(B->ev, s) != cudaSuccess)
+				rc = set_cuda_error(c, cudaGetLastError(), "estimate");
+			break;
+		}
+		// Batch solved: lane results and t += x.*v, q += v.*v (:195, :198).
+		if ((rc = enqueue_lane_copy(c, B))) break;
+		kb_accumulate<<<blocks1d(n), 256, 0, s>>>(n, B->rbD, E.nb, B->mixed ? B->xh : (const double *)B->x, B->b,
+		                                          B->t_acc, B->q_acc, E.first);
+		c->launches++;
+		E.first = false;
+		if (cudaEventRecord(B->ev, s) != cudaSuccess) rc = set_cuda_error(c, cudaGetLastError(), "estimate");
+		E.stage = EST_LANES;
+		break;
+	case EST_LANES: {
+		const int k0 = E.k0;
+		const int w = process_lanes(c, B, E.nb, E.maxiter, E.tol, E.errs ? E.errs + k0 : nullptr,
+		                            E.iters ? E.iters + k0 : nullptr, B->lane_res.data());
+		if (E.results) std::memcpy(E.results + k0, B->lane_res.data(), sizeof(int) * E.nb);
+		if (w > E.worst) E.worst = w;
+		if (w != 0 && !E.ignore_errors) {  // :181-184: the first failing probe's code, no D
+			for (int j = 0; j < E.nb; j++)
+				if (B->lane_res[j] != 0) {
+					E.rc = B->lane_res[j];
+					break;
+				}
+			E.stage = EST_DONE;
+			*done = 1;
+			return 0;
+		}
+		E.k0 += E.nb;
+		rc = E.k0 < E.samples ? est_start_batch(c, B) : est_final(c, B);
+		break;
+	}
+	case EST_FINAL:
+		E.rc = E.worst;
+		E.stage = EST_DONE;
+		*done = 1;
+		return 0;
+	default:
+		break;
+	}
+	if (rc) {
+		E.rc = rc;
+		E.stage = EST_DONE;
+		*done = 1;
+	}
+	return rc;
+}
+
+int batched_est_result(const Ctx *c) {
+	const Batched *B = (const Batched *)c->batched;
+	return B ? B->est.rc : SEDI_ERR_ARG;
+}
+
+// Blocking estimator: probes from device memory (probes_dev) or, when
+// probes_dev is NULL, from the device generator (probe k = std::mt19937(seed
+// + k)), written straight into the lane-sliced right-hand-side buffer.
 int batched_estimate_src(Ctx *c, int samples, const double *probes_dev, uint32_t seed, int maxiter, double tol,
                          int ignore_errors, double *D_dev, double *t_dev, double *q_dev, int *iters, double *errs,
                          int *results) {
 	Batched *B = (Batched *)c->batched;
-	cudaStream_t s = c->stream;
-	const long long n = c->g.n;
-	std::vector<double> fe(B->R);
-	std::vector<int> fi(B->R), res(B->R);
-	int worst = 0;
-	bool first = true;
-	for (int k0 = 0; k0 < samples; k0 += c->batch) {
-		const int nb = samples - k0 < c->batch ? samples - k0 : c->batch;
-		if (probes_dev) {
-			kb_interleave<<<blocks1d(n * B->R), 256, 0, s>>>(n, B->R, B->rbD, nb, probes_dev + (size_t)k0 * n, B->b);
-		} else {
-			if (nb < B->R) BTRY(cudaMemsetAsync(B->b, 0, B->elems * sizeof(double), s));  // padding lanes
-			if (device_fill_probes(seed + (uint32_t)k0, nb, n, B->rbD, B->b, s)) return set_cuda_error(c, cudaGetLastError(), "device probes");
-		}
-		BTRY(cudaMemsetAsync(B->mixed ? (void *)B->xh : B->x, 0, B->elems * sizeof(double), s));  // x = 0 (:175)
-		c->launches++;
-		int rc = batched_run_resident(c, nb, maxiter, tol, fe.data(), fi.data(), res.data());
-		if (rc < 0) return rc;
-		for (int j = 0; j < nb; j++) {
-			if (iters) iters[k0 + j] = fi[j];
-			if (errs) errs[k0 + j] = fe[j];
-			if (results) results[k0 + j] = res[j];
-		}
-		kb_accumulate<<<blocks1d(n), 256, 0, s>>>(n, B->rbD, nb, B->mixed ? B->xh : (const double *)B->x, B->b,
-		                                          B->t_acc, B->q_acc, first);
-		c->launches++;
-		first = false;
-		if (rc > worst) worst = rc;
-		if (rc != 0 && !ignore_errors) {
-			for (int j = 0; j < nb; j++)
-				if (res[j] != 0) return res[j];
-		}
+	int rc = batched_est_begin(c, samples, probes_dev, seed, maxiter, tol, ignore_errors, D_dev, t_dev, q_dev,
+	                           nullptr, iters, errs, results);
+	if (rc) return rc;
+	for (;;) {
+		BTRY(cudaEventSynchronize(B->ev));
+		int done = 0;
+		if ((rc = batched_est_advance(c, &done))) return rc;
+		if (done) break;
 	}
-	if (samples == 0) {
-		BTRY(cudaMemsetAsync(B->t_acc, 0, sizeof(double) * n, s));
-		BTRY(cudaMemsetAsync(B->q_acc, 0, sizeof(double) * n, s));
-	}
-	kb_divide<<<blocks1d(n), 256, 0, s>>>(n, B->t_acc, B->q_acc, D_dev);
-	c->launches++;
-	if (t_dev) BTRY(cudaMemcpyAsync(t_dev, B->t_acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-	if (q_dev) BTRY(cudaMemcpyAsync(q_dev, B->q_acc, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-	BTRY(cudaStreamSynchronize(s));
-	return worst;
+	BTRY(cudaStreamSynchronize(c->stream));
+	return B->est.rc;
 }
 
 }  // namespace sedi

@@ -7,10 +7,6 @@
 
 #include "sedi_internal.h"
 
-struct sedi_ctx {
-	sedi::Ctx c;
-};
-
 namespace sedi {
 
 int set_cuda_error(Ctx *c, cudaError_t e, const char *where) {

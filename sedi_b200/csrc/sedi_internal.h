@@ -109,9 +109,26 @@ int batched_estimate_src(Ctx *c, int samples, const double *probes_dev, uint32_t
                          int ignore_errors, double *D_dev, double *t_dev, double *q_dev, int *iters, double *errs,
                          int *results);
 
+// Non-blocking estimator on a batched context: begin enqueues the first
+// batch; advance checks the context's event and enqueues the next step
+// (never waits), *done = 1 when D (and the D_host copy) are complete;
+// est_result gives the estimator's return code (worst result, the first
+// failing probe's code without -i, or a negative error).
+int batched_est_begin(Ctx *c, int samples, const double *probes_dev, uint32_t seed, int maxiter, double tol,
+                      int ignore_errors, double *D_dev, double *t_dev, double *q_dev, double *D_host, int *iters,
+                      double *errs, int *results);
+int batched_est_advance(Ctx *c, int *done);
+int batched_est_result(const Ctx *c);
+// Device bytes a batched context allocates (0 for the single-vector form).
+size_t batched_bytes(int solver, int precision, int batch, long long n1, long long n2, long long n3);
+
 // rng.cu
 void host_fill_probe(uint32_t seed, long n, double *out);
 // Probes seed..seed+nprobes-1 on the device: lane-sliced (W > 0) or dense (W == 0).
 int device_fill_probes(uint32_t seed, int nprobes, long long npts, int W, double *out, cudaStream_t s);
 
 }  // namespace sedi
+
+struct sedi_ctx {
+	sedi::Ctx c;
+};
