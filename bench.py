@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--maxiter", type=int, default=None, help="override maxiter (with --tol 0: fixed iterations)")
     ap.add_argument("--tol", type=float, default=None)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, kernel timing, accuracy and other forms")
+    ap.add_argument("--serve-jobs", type=int, default=32, help="jobs in the serving run (0: skip it)")
+    ap.add_argument("--serve-only", action="store_true", help="run only the serving measurement")
     a = ap.parse_args()
     global GRID, MAXITER, TOL
     if a.grid:
@@ -198,6 +200,58 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# Serving: Poisson-arriving estimation jobs on one GPU.
+# ---------------------------------------------------------------------------
+SERVE_EDGES = (32, 48, 64, 96, 128, 192)
+
+
+def serve_jobs(njobs, seed=SEED):
+    """Seeded job mix: cubic grid edge uniform over SERVE_EDGES, samples uniform
+    8..64, tol log-uniform 1e-10..1e-6, solver uniform over CG / pipelined CG /
+    BiCGStab, precision FP64 or FP32 + FP64 reliable update; probe seeds
+    derived from the job id."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return {
+        "edge": rng.choice(SERVE_EDGES, njobs),
+        "samples": rng.integers(8, 65, njobs),
+        "tol": 10.0 ** rng.uniform(-10.0, -6.0, njobs),
+        "solver": rng.choice(["cg", "pcg", "bicgstab"], njobs),
+        "precision": rng.integers(0, 2, njobs),
+        "seed": SEED + 100003 * np.arange(njobs),
+    }
+
+
+def run_serving(S, njobs, maxiter=5000):
+    """Capacity from a closed-loop run (every job queued at t = 0), then an
+    open-loop run with Poisson arrivals (seeded) at 80% of that capacity.
+    Latency = scheduled arrival to D on the host."""
+    import numpy as np
+    jobs = serve_jobs(njobs)
+    args = (jobs["solver"], jobs["precision"], jobs["edge"], jobs["samples"], jobs["seed"], jobs["tol"], maxiter)
+    with S.Server() as srv:
+        lat0, rc0, mk0 = srv.replay(np.zeros(njobs), *args)
+        cap = njobs / mk0
+        rate = 0.8 * cap
+        arrival = np.cumsum(np.random.default_rng(SEED + 1).exponential(1.0 / rate, njobs))
+        arrival -= arrival[0]
+        lat, rcs, mk = srv.replay(arrival, *args)
+        st = srv.stats()
+    probes = int(np.sum(jobs["samples"]))
+    return {
+        "jobs": njobs, "capacity_jobs_per_s": cap, "arrival_rate_jobs_per_s": rate,
+        "jobs_per_s": njobs / mk, "probe_solves_per_s": probes / mk,
+        "p50_latency_ms": 1e3 * float(np.percentile(lat, 50)), "p99_latency_ms": 1e3 * float(np.percentile(lat, 99)),
+        "mean_latency_ms": 1e3 * float(lat.mean()), "closed_loop_p50_ms": 1e3 * float(np.percentile(lat0, 50)),
+        "result_codes_nonzero": int(np.count_nonzero(rcs)) + int(np.count_nonzero(rc0)),
+        "peak_device_gb": st["peak_bytes"] / 1e9, "budget_gb": st["budget_bytes"] / 1e9,
+        "contexts_created": st["ctx_created"], "contexts_reused": st["ctx_reused"], "max_running": st["max_running"],
+        "mix": "edge U{32,48,64,96,128,192}^3, samples U{8..64}, tol logU[1e-10,1e-6], solver U{CG,PCG,BiCGStab}, "
+               "precision U{FP64, FP32+RU}, seed 1234; Poisson arrivals at 0.8 x closed-loop capacity",
+    }
+
+
+# ---------------------------------------------------------------------------
 # The sedi_b200 arm.
 # ---------------------------------------------------------------------------
 def traffic_per_launch(kernel):
@@ -223,6 +277,10 @@ def run_sedi(args):
     import sedi_b200 as S
 
     rank, world, local = dist_env()
+    if args.serve_only:
+        if rank == 0:
+            print(json.dumps({"serving": run_serving(S, args.serve_jobs)}), flush=True)
+        return
     if world > 1:
         from datetime import timedelta
         torch.cuda.set_device(local)
@@ -372,6 +430,7 @@ def run_sedi(args):
             v, wall, kind, it = reference_sample(procs, SEED)
             cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": kind,
                    "sample": f"{procs} concurrent single-rank processes x 1 probe (128^3 CG tol 1e-9), {wall:.1f} s"}
+        serving = run_serving(S, args.serve_jobs) if world == 1 and args.serve_jobs > 0 else None
         gpoint = float(np.sum(it_all)) * n / args.steps / (ms / 1e3 / args.steps) / 1e9 if world == 1 else None
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -392,6 +451,7 @@ def run_sedi(args):
             "gpoint_iterations_per_s": gpoint,
             "accuracy": acc,
             "forms": forms,
+            "serving": serving,
         }
         print(json.dumps(out), flush=True)
     ctx.close()

@@ -173,7 +173,9 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 			mbar_arrive(b);  // ghost plane: completes the phase without data
 			return;
 		}
-		fence_async_smem();
+		// Stages are only read by the generic proxy during the sweep (the
+		// reduction scratch that aliases them is written after the last wait),
+		// so no proxy fence is needed before the copy.
 		mbar_arrive_tx(b, Lay::TX);
 #pragma unroll
 		for (int s = 0; s < NS; s++)
@@ -197,14 +199,11 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 	int sj = 0;      // stage slot of plane j (j mod NST)
 	unsigned par = 0;  // barrier parity of plane j ((j / NST) & 1)
 	for (int j = 0; j <= np; j++, sj = (sj + 1 == NST) ? 0 : sj + 1, par ^= (sj == 0)) {
-		if (j < np) {
-			const bool ok = mbar_wait(&bar[sj], par);
-			if (__syncthreads_or(!ok)) {
-				failed = true;
-				break;
-			}
-			waited = j + 1;
-		}
+		// Each thread waits for plane j's stage itself (the mbarrier's acquire
+		// makes the TMA data visible); a timeout is combined into the one
+		// block barrier at the end of the step.
+		bool ok = true;
+		if (j < np) ok = mbar_wait(&bar[sj], par);
 		// Phase 1: stencil input of plane j (transforming ops only).
 		if (!IDENT && j < np) {
 			const int p = z0 - 1 + j;
@@ -277,7 +276,11 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 				op.out(o, pidx, lane0 + lo, xc, y, qv, rc, part);
 			}
 		}
-		__syncthreads();
+		if (__syncthreads_or(!ok)) {
+			failed = true;  // outputs of this step may be wrong; the host sees gl->err
+			break;
+		}
+		if (j < np) waited = j + 1;
 		// The stage of plane j-KEEP has been read for the last time.
 		if (t == 0 && j >= KEEP && issued < np) {
 			issue(issued);
@@ -1258,8 +1261,33 @@ constexpr int kThr = SEDI_STREAM_THREADS, kSliceLanes = SEDI_SLICE_LANES;
 
 // Point tiles: at least THREADS (point, lane group) slots per block, and a
 // merged TMA row W*(P1+2) within the 256-element box limit.
-__host__ __device__ constexpr int tile_p1(int lg) { return lg == 1 ? 32 : 16; }
-__host__ __device__ constexpr int tile_p2(int lg) { return lg >= 4 ? 8 : 16; }
+#ifndef SEDI_TILE_P1_LG1
+#define SEDI_TILE_P1_LG1 32
+#endif
+#ifndef SEDI_TILE_P2_LG1
+#define SEDI_TILE_P2_LG1 16
+#endif
+#ifndef SEDI_TILE_P1_LG2
+#define SEDI_TILE_P1_LG2 16
+#endif
+#ifndef SEDI_TILE_P2_LG2
+#define SEDI_TILE_P2_LG2 16
+#endif
+#ifndef SEDI_TILE_P1_LG4
+#define SEDI_TILE_P1_LG4 16
+#endif
+#ifndef SEDI_TILE_P2_LG4
+#define SEDI_TILE_P2_LG4 8
+#endif
+#ifndef SEDI_BLOCKS_PER_SM
+#define SEDI_BLOCKS_PER_SM 1  // resident sweep blocks per SM (shared memory bound)
+#endif
+__host__ __device__ constexpr int tile_p1(int lg) {
+	return lg == 1 ? SEDI_TILE_P1_LG1 : (lg == 2 ? SEDI_TILE_P1_LG2 : SEDI_TILE_P1_LG4);
+}
+__host__ __device__ constexpr int tile_p2(int lg) {
+	return lg == 1 ? SEDI_TILE_P2_LG1 : (lg == 2 ? SEDI_TILE_P2_LG2 : SEDI_TILE_P2_LG4);
+}
 
 template <class T, int RB>
 struct CfgFor {
@@ -1288,15 +1316,27 @@ static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid) {
 	tile_for(rb, eb, &P1, &P2);
 	const int t1 = (g.n1 + P1 - 1) / P1, t2 = (g.n2 + P2 - 1) / P2;
 	const int slices = R / rb;
-	// About two blocks' worth of work per SM: split i3 when the tile count is small.
-	const long long want = 148LL * 2;
+	// Split i3 into nz chunks of zc planes.  Blocks run in waves of
+	// 148 x SEDI_BLOCKS_PER_SM; a block streams zc + 2 planes plus about one
+	// plane of pipeline fill.  Pick the split with the fewest wave-planes
+	// (the last wave counts in full), the smaller split on ties.
 	const long long per = (long long)t1 * t2 * slices;
-	long long nz = (want + per - 1) / per;
-	if (nz < 1) nz = 1;
-	if (nz > g.n3) nz = g.n3;
-	int zc = (int)((g.n3 + nz - 1) / nz);
-	if (zc < 4) zc = g.n3 < 4 ? g.n3 : 4;
-	nz = (g.n3 + zc - 1) / zc;
+	const long long wave = 148LL * SEDI_BLOCKS_PER_SM;
+	long long best = -1;
+	int zc = g.n3, nz = 1;
+	const int maxz = g.n3 < 64 ? g.n3 : 64;
+	for (int k = 1; k <= maxz; k++) {
+		const int z = (g.n3 + k - 1) / k;
+		if (z < 2 && g.n3 >= 2) break;
+		const int kk = (g.n3 + z - 1) / z;
+		const long long waves = (per * kk + wave - 1) / wave;
+		const long long cost = waves * (z + 3);
+		if (best < 0 || cost < best) {
+			best = cost;
+			zc = z;
+			nz = kk;
+		}
+	}
 	sg->n1 = g.n1;
 	sg->n2 = g.n2;
 	sg->n3 = g.n3;
