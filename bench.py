@@ -57,9 +57,16 @@ def parse():
     ap.add_argument("--maxiter", type=int, default=None, help="override maxiter (with --tol 0: fixed iterations)")
     ap.add_argument("--tol", type=float, default=None)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, kernel timing, accuracy and other forms")
-    ap.add_argument("--serve-jobs", type=int, default=32, help="jobs in the serving run (0: skip it)")
+    ap.add_argument("--solver", choices=["cg", "pcg", "bicgstab"], default="cg",
+                    help="solver of the timed form (profiling cases; the benchmark configuration is CG)")
+    ap.add_argument("--serve-jobs", type=int, default=12, help="jobs in the serving run (0: skip it)")
     ap.add_argument("--serve-only", action="store_true", help="run only the serving measurement")
+    ap.add_argument("--workload", choices=["dropin", "batched256", "large512"], default="dropin",
+                    help="dropin: the benchmark line; batched256 / large512: the 256^3 x 128-probe and the "
+                         "512^3 x 16-probe configurations, one line each")
     a = ap.parse_args()
+    if a.solver != "cg" and not a.no_extras:
+        ap.error("--solver pcg/bicgstab is for profiling cases (with --no-extras)")
     global GRID, MAXITER, TOL
     if a.grid:
         GRID = tuple(int(v) for v in a.grid.split("x"))
@@ -244,11 +251,121 @@ def run_serving(S, njobs, maxiter=5000):
         "p50_latency_ms": 1e3 * float(np.percentile(lat, 50)), "p99_latency_ms": 1e3 * float(np.percentile(lat, 99)),
         "mean_latency_ms": 1e3 * float(lat.mean()), "closed_loop_p50_ms": 1e3 * float(np.percentile(lat0, 50)),
         "result_codes_nonzero": int(np.count_nonzero(rcs)) + int(np.count_nonzero(rc0)),
+        "nonzero_jobs": [{"solver": str(jobs["solver"][k]), "edge": int(jobs["edge"][k]),
+                          "precision": "fp64" if int(jobs["precision"][k]) == 0 else "mixed",
+                          "tol": float(jobs["tol"][k]), "samples": int(jobs["samples"][k]), "rc": int(rcs[k])}
+                         for k in range(njobs) if rcs[k] != 0],
         "peak_device_gb": st["peak_bytes"] / 1e9, "budget_gb": st["budget_bytes"] / 1e9,
         "contexts_created": st["ctx_created"], "contexts_reused": st["ctx_reused"], "max_running": st["max_running"],
         "mix": "edge U{32,48,64,96,128,192}^3, samples U{8..64}, tol logU[1e-10,1e-6], solver U{CG,PCG,BiCGStab}, "
                "precision U{FP64, FP32+RU}, seed 1234; Poisson arrivals at 0.8 x closed-loop capacity",
     }
+
+
+# ---------------------------------------------------------------------------
+# Large single-GPU configurations (one JSON line each, not the benchmark line).
+# ---------------------------------------------------------------------------
+def _peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    return (json.load(open(path))["hbm_gbs"], "measured") if os.path.exists(path) else (6650.0, "fallback")
+
+
+def _kernel_table(ctx, peak):
+    return [{"kernel": k, "ms": ms, "bytes": by, "GB/s": by / ms / 1e6, "frac": by / ms / 1e6 / peak}
+            for k, ms, by in ctx.time_kernels(reps=10)]
+
+
+def run_batched256(S, args):
+    """256^3 grid, 128 probes interleaved (mixed precision, FP32 vectors with FP64
+    reliable update at the autotuned period), CG and pipelined CG to 1e-9.  D
+    error against the batched FP64 form on the same probes (which follows the
+    single-vector FP64 method lane by lane), rate of the single-vector FP64 form
+    on 4 of the probes."""
+    import numpy as np
+    import torch
+    grid, samples, tol, maxiter = (256, 256, 256), 128, 1e-9, 20000
+    peak, psrc = _peak()
+    out = {"workload": "256^3 x 128 probes, FP32 + FP64 reliable update, tol 1e-9", "peak_gbs": peak,
+           "peak_source": psrc, "solvers": {}}
+    for solver in ("cg", "pcg"):
+        tune = S.autotune(solver, grid, samples, precision=S.MIXED, maxiter=maxiter, tol=tol, seed=SEED)
+        with S.Context(solver, grid, precision=S.MIXED, batch=samples) as c:
+            cfg = c.config()
+            for _ in range(max(args.warmup - 2, 1)):
+                c.estimate(samples, SEED, maxiter, tol)
+            torch.cuda.synchronize()
+            clocks = Clocks(0)
+            clocks.start()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                r = c.estimate(samples, SEED, maxiter, tol)
+            dt = (time.perf_counter() - t0) / args.steps
+            clk = clocks.stop()
+            kern = _kernel_table(c, peak)
+        Dm = r["D"]
+        # FP64 form on the same probes, in two halves of 64 (pipelined CG in
+        # FP64 for 128 probes would need 189 GB); t and q add up exactly.
+        half = samples // 2
+        with S.Context(solver, grid, precision=S.FP64, batch=half) as c64:
+            t0 = time.perf_counter()
+            ra = c64.estimate(half, SEED, maxiter, tol)
+            rb = c64.estimate(half, SEED + half, maxiter, tol)
+            dt64 = time.perf_counter() - t0
+        r64 = {"D": (ra["t"] + rb["t"]) / (ra["q"] + rb["q"])}
+        with S.Context(solver, grid) as cp:
+            cp.estimate(1, SEED, maxiter, tol)
+            t0 = time.perf_counter()
+            cp.estimate(4, SEED, maxiter, tol)
+            plain = 4 / (time.perf_counter() - t0)
+        n = grid[0] * grid[1] * grid[2]
+        out["solvers"][solver] = {
+            "probe_solves_per_s": samples / dt, "ms_per_estimate": 1e3 * dt,
+            "gpoint_iterations_per_s": float(np.sum(r["iters"])) * n / dt / 1e9,
+            "iterations": [int(r["iters"].min()), int(r["iters"].max())],
+            "results_nonzero": int(np.count_nonzero(r["results"])),
+            "D_rel_err_vs_fp64": float(np.abs(Dm - r64["D"]).max() / np.abs(r64["D"]).max()),
+            "batched_fp64_probe_solves_per_s": samples / dt64,
+            "plain_fp64_probe_solves_per_s": plain, "speedup_vs_plain_fp64": samples / dt / plain,
+            "autotuned": tune, "config": cfg, "kernels": kern, "clocks": clk,
+        }
+    print(json.dumps(out), flush=True)
+
+
+def run_large512(S, args):
+    """512^3 grid (134M points), pipelined CG, 16 probes in FP32 with FP64
+    true-residual recompute and FP64 accumulators, tol 1e-8, maxiter 500 (the
+    limit is reached: result 1 per probe); D error against the single-vector
+    FP64 pipelined CG on the same probes."""
+    import numpy as np
+    import torch
+    grid, samples, tol, maxiter = (512, 512, 512), 16, 1e-8, 500
+    peak, psrc = _peak()
+    with S.Context("pcg", grid, precision=S.MIXED, batch=samples) as c:
+        c.estimate(samples, SEED, 20, tol, ignore_errors=True)  # warm-up (graph capture)
+        torch.cuda.synchronize()
+        clocks = Clocks(0)
+        clocks.start()
+        t0 = time.perf_counter()
+        r = c.estimate(samples, SEED, maxiter, tol, ignore_errors=True)
+        dt = time.perf_counter() - t0
+        clk = clocks.stop()
+        kern = _kernel_table(c, peak)
+        cfg = c.config()
+    with S.Context("pcg", grid) as cp:
+        t0 = time.perf_counter()
+        rp = cp.estimate(samples, SEED, maxiter, tol, ignore_errors=True)
+        dtp = time.perf_counter() - t0
+    n = grid[0] * grid[1] * grid[2]
+    out = {"workload": "512^3 x 16 probes, pipelined CG, FP32 + FP64 reliable update, tol 1e-8, maxiter 500",
+           "probe_solves_per_s": samples / dt, "ms_per_estimate": 1e3 * dt,
+           "gpoint_iterations_per_s": float(np.sum(r["iters"])) * n / dt / 1e9,
+           "iterations": [int(r["iters"].min()), int(r["iters"].max())], "results": sorted(set(map(int, r["results"]))),
+           "D_rel_err_vs_plain_fp64": float(np.abs(r["D"] - rp["D"]).max() / np.abs(rp["D"]).max()),
+           "final_err_mixed": [float(r["errs"].min()), float(r["errs"].max())],
+           "final_err_fp64": [float(rp["errs"].min()), float(rp["errs"].max())],
+           "plain_fp64_probe_solves_per_s": samples / dtp, "speedup_vs_plain_fp64": dtp / dt,
+           "kernels": kern, "config": cfg, "clocks": clk, "peak_gbs": peak, "peak_source": psrc}
+    print(json.dumps(out), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -277,6 +394,10 @@ def run_sedi(args):
     import sedi_b200 as S
 
     rank, world, local = dist_env()
+    if args.workload != "dropin":
+        if rank == 0:
+            (run_batched256 if args.workload == "batched256" else run_large512)(S, args)
+        return
     if args.serve_only:
         if rank == 0:
             print(json.dumps({"serving": run_serving(S, args.serve_jobs)}), flush=True)
@@ -299,7 +420,7 @@ def run_sedi(args):
     t = torch.empty(n, dtype=torch.float64, device=dev)
     q = torch.empty(n, dtype=torch.float64, device=dev)
     prec = S.MIXED if args.form == "mixed" else S.FP64
-    ctx = S.Context("cg", GRID, precision=prec, batch=SAMPLES)
+    ctx = S.Context(args.solver, GRID, precision=prec, batch=SAMPLES)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream)
 
@@ -347,6 +468,7 @@ def run_sedi(args):
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                               "ms_per_step": ms / args.steps, "grid": list(GRID), "maxiter": MAXITER, "tol": TOL,
+                              "solver": args.solver,
                               "gpu_launches": launches, "note": "profiling case, not the benchmark configuration"}),
                   flush=True)
         ctx.close()

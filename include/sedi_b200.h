@@ -256,6 +256,39 @@ int sedi_server_replay(sedi_server *srv, int njobs, const double *arrival_s, con
 int sedi_server_stats(const sedi_server *srv, double *peak_bytes, double *budget_bytes, int *ctx_created,
                       int *ctx_reused, int *max_running, long long *launches);
 
+/*
+ * Autotuner of the batched form (no counterpart in the reference).  For
+ * contexts of this solver, precision, batch size and grid it picks, by
+ * measurement on scratch contexts: the lane-slice width of the interleaved
+ * Krylov fields (FP32 8 or 4 lanes, FP64 8, 4 or 2), the i3 split of the
+ * sweeps, and with flags & 1 the iterations per captured graph and (mixed
+ * precision) the reliable-update period in 20..50, the last two by timing a
+ * real estimate of `batch` probes seeded `seed` to `tol`.  The choice is kept
+ * for the process and used by every context created afterwards with the
+ * same parameters (and by the server's admission sizes).
+ * choice[0..3] = slice width, i3 chunks (0: the built-in model), period,
+ * iterations per graph; *score_ms (optional) = the winning estimate time
+ * (flags & 1) or summed per-iteration sweep time.  Needs device memory for
+ * one such context at a time.
+ */
+int sedi_autotune(int solver, int precision, int batch, long n1, long n2, long n3, int maxiter, double tol,
+                  uint32_t seed, int flags, int *choice, double *score_ms);
+
+/* Launch choices of a batched context: config[0..4] = lane-slice width, i3
+ * chunks of a sweep, reliable-update period, iterations per captured graph,
+ * lanes (padded right-hand sides).  SEDI_ERR_UNSUPPORTED for the
+ * single-vector form. */
+int sedi_ctx_config(const sedi_ctx *ctx, int *config);
+
+/*
+ * Self-test of the bounded device wait that every batched sweep uses on its
+ * copy barriers (no counterpart in the reference): one kernel waits on a
+ * barrier that nothing completes, with a limit of limit_ms (0 < limit_ms <=
+ * 5000).  *timed_out = 1 when the wait gave up as it must; *waited_ms
+ * (optional) = how long it waited.  The GPU and any context stay usable.
+ */
+int sedi_selftest_bounded_wait(double limit_ms, int *timed_out, double *waited_ms);
+
 /* Device bytes of a batched context (the server's admission size). */
 double sedi_job_bytes(int solver, int precision, int lanes, long n1, long n2, long n3);
 

@@ -26,7 +26,7 @@ import os
 import numpy as np
 
 __all__ = [
-    "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "Server", "estimate", "fill_probe",
+    "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "Server", "autotune", "estimate", "fill_probe",
     "job_bytes", "library_path", "load", "SOLVER_IDS", "FP64", "MIXED",
 ]
 
@@ -99,6 +99,10 @@ def load():
     lib.sedi_server_take.argtypes = [vp, c_long, vp, vp, vp, vp]
     lib.sedi_server_replay.argtypes = [vp, c_int, vp, vp, vp, vp, vp, vp, vp, c_int, vp, vp, pd]
     lib.sedi_server_stats.argtypes = [vp, pd, pd, pi, pi, pi, ctypes.POINTER(ctypes.c_longlong)]
+    lib.sedi_autotune.argtypes = [c_int, c_int, c_int, c_long, c_long, c_long, c_int, c_double, ctypes.c_uint32,
+                                  c_int, vp, pd]
+    lib.sedi_ctx_config.argtypes = [vp, vp]
+    lib.sedi_selftest_bounded_wait.argtypes = [c_double, pi, pd]
     lib.sedi_job_bytes.restype = c_double
     lib.sedi_job_bytes.argtypes = [c_int, c_int, c_int, c_long, c_long, c_long]
     _lib = lib
@@ -196,6 +200,13 @@ class Context:
     @property
     def launches(self):
         return int(load().sedi_launch_count(self._h))
+
+    def config(self):
+        """Launch choices of a batched context (see autotune)."""
+        cf = np.zeros(5, np.int32)
+        self._check(load().sedi_ctx_config(self._h, _ptr(cf)), "config")
+        return {"slice_width": int(cf[0]), "z_chunks": int(cf[1]), "period": int(cf[2]), "chunk": int(cf[3]),
+                "lanes": int(cf[4])}
 
     def solve(self, x, b, iM=None, maxiter=1000, tol=1e-4):
         """Returns (result_t, final_err, final_iter); x is overwritten with the solution."""
@@ -346,6 +357,21 @@ def estimate(solver, dims, samples, seed=1234, maxiter=1000, tol=1e-4, ignore_er
         return ctx.estimate(samples, seed, maxiter, tol, ignore_errors, probes)
 
 
+def autotune(solver, dims, batch, precision=MIXED, maxiter=5000, tol=1e-9, seed=1234, solve=True):
+    """Pick the batched form's launch choices for this shape by measurement
+    (sedi_autotune); contexts created afterwards use them.  Returns
+    {"slice_width", "z_chunks", "period", "chunk", "score_ms"}."""
+    sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
+    ch = np.zeros(4, np.int32)
+    ms = ctypes.c_double(0.0)
+    rc = load().sedi_autotune(sid, int(precision), int(batch), *[int(d) for d in dims], int(maxiter), float(tol),
+                              int(seed) & 0xFFFFFFFF, 1 if solve else 0, _ptr(ch), ctypes.byref(ms))
+    if rc < 0:
+        raise SediError(rc, "sedi_autotune")
+    return {"slice_width": int(ch[0]), "z_chunks": int(ch[1]), "period": int(ch[2]), "chunk": int(ch[3]),
+            "score_ms": ms.value}
+
+
 def job_bytes(solver, dims, lanes, precision=FP64):
     """Device bytes of a batched context: the server's admission size."""
     sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
@@ -457,3 +483,13 @@ class Server:
                                  ctypes.byref(mr), ctypes.byref(la))
         return {"peak_bytes": pk.value, "budget_bytes": bu.value, "ctx_created": cr.value, "ctx_reused": ru.value,
                 "max_running": mr.value, "launches": la.value}
+
+
+def selftest_bounded_wait(limit_ms=50.0):
+    """Run the device wait on a barrier nothing completes; returns
+    (timed_out, waited_ms).  See sedi_selftest_bounded_wait."""
+    to, ms = ctypes.c_int(0), ctypes.c_double(0.0)
+    rc = load().sedi_selftest_bounded_wait(float(limit_ms), ctypes.byref(to), ctypes.byref(ms))
+    if rc < 0:
+        raise SediError(rc, "sedi_selftest_bounded_wait")
+    return bool(to.value), ms.value

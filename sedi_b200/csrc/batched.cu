@@ -29,9 +29,12 @@
 //         iterations and whenever a lane's FP32 residual reaches tol; a lane
 //         stops only when its FP64 true residual satisfies the reference's
 //         test err = sqrt(<r,r>/<b,b>) <= tol (Cg.hpp:191-193).
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1187,6 +1190,39 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 	          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Launch choices of the batched form for one (solver, precision, lanes,
+// grid): lane-slice width of the Krylov fields, i3 split of the sweeps,
+// reliable-update period and iterations per captured graph.  Zero fields
+// mean "default".  Filled by sedi_autotune, read when a context is created.
+struct Tuning {
+	int W = 0, nz = 0, period = 0, chunk = 0;
+};
+struct TuneKey {
+	int solver, precision, R;
+	long long n1, n2, n3;
+	bool operator<(const TuneKey &o) const {
+		if (solver != o.solver) return solver < o.solver;
+		if (precision != o.precision) return precision < o.precision;
+		if (R != o.R) return R < o.R;
+		if (n1 != o.n1) return n1 < o.n1;
+		if (n2 != o.n2) return n2 < o.n2;
+		return n3 < o.n3;
+	}
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, Tuning> g_tune;
+
+static Tuning tuning_for(const TuneKey &k) {
+	std::lock_guard<std::mutex> lk(g_tune_mu);
+	auto it = g_tune.find(k);
+	return it == g_tune.end() ? Tuning() : it->second;
+}
+
+static void set_tuning(const TuneKey &k, const Tuning &t) {
+	std::lock_guard<std::mutex> lk(g_tune_mu);
+	g_tune[k] = t;
+}
+
 constexpr int kLaneDoubles = 18, kLaneInts = 5;  // LaneState arrays
 
 struct Batched;
@@ -1228,6 +1264,7 @@ struct Batched {
 	SetupFn setup_fn = nullptr;
 	ChunkFn chunk_fn = nullptr;
 	cudaEvent_t ev = nullptr;
+	Tuning tuned;
 	EstState est;
 	std::vector<int> lane_res;  // result codes of the batch being processed
 	double *t_acc = nullptr, *q_acc = nullptr;
@@ -1311,7 +1348,7 @@ static void tile_for(int rb, int eb, int *P1, int *P2) {
 	*P2 = tile_p2(lg);
 }
 
-static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid) {
+static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int nz_force = 0) {
 	int P1, P2;
 	tile_for(rb, eb, &P1, &P2);
 	const int t1 = (g.n1 + P1 - 1) / P1, t2 = (g.n2 + P2 - 1) / P2;
@@ -1336,6 +1373,11 @@ static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid) {
 			zc = z;
 			nz = kk;
 		}
+	}
+	if (nz_force > 0) {  // autotuned split
+		const int k = nz_force < g.n3 ? nz_force : g.n3;
+		zc = (g.n3 + k - 1) / k;
+		nz = (g.n3 + zc - 1) / zc;
 	}
 	sg->n1 = g.n1;
 	sg->n2 = g.n2;
@@ -1379,10 +1421,15 @@ int batched_alloc(Ctx *c) {
 	B->R = pick_R(c->batch, B->mixed);
 	B->elems = (size_t)c->g.n * B->R;
 	const int ebT = B->mixed ? 4 : 8;
+	const Tuning tu = tuning_for(TuneKey{c->solver, c->precision, B->R, c->g.n1, c->g.n2, c->g.n3});
 	B->rbT = slice_for(B->R, !B->mixed);
-	B->rbD = slice_for(B->R, true);
-	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT);
-	shape(c->g, B->R, B->rbD, 8, &B->gD, &B->gridD);
+	if (tu.W > 0 && tu.W <= B->R && B->R % tu.W == 0) B->rbT = tu.W;
+	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
+	B->tuned = tu;
+	if (tu.period > 0) B->period = tu.period;
+	if (tu.chunk > 0) B->chunk = tu.chunk;
+	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz);
+	shape(c->g, B->R, B->rbD, 8, &B->gD, &B->gridD, tu.nz);
 	const size_t ts = B->mixed ? sizeof(float) : sizeof(double);
 	const size_t nblkT = (size_t)B->gridT.x * B->gridT.z, nblkD = (size_t)B->gridD.x * B->gridD.z;
 	const size_t nblk = nblkT > nblkD ? nblkT : nblkD;
@@ -1471,10 +1518,13 @@ size_t batched_bytes(int solver, int precision, int batch, long long n1, long lo
 	g.n = n1 * n2 * n3;
 	const int R = pick_R(batch, mixed);
 	const size_t elems = (size_t)g.n * R, ts = mixed ? 4 : 8;
+	const Tuning tu = tuning_for(TuneKey{solver, precision, R, n1, n2, n3});
+	int wT = slice_for(R, !mixed);
+	if (tu.W > 0 && tu.W <= R && R % tu.W == 0) wT = tu.W;
 	SGeo sT, sD;
 	dim3 gT, gD;
-	shape(g, R, slice_for(R, !mixed), (int)ts, &sT, &gT);
-	shape(g, R, slice_for(R, true), 8, &sD, &gD);
+	shape(g, R, wT, (int)ts, &sT, &gT, tu.nz);
+	shape(g, R, mixed ? slice_for(R, true) : wT, 8, &sD, &gD, tu.nz);
 	const size_t nblkT = (size_t)gT.x * gT.z, nblkD = (size_t)gD.x * gD.z;
 	const size_t nblk = nblkT > nblkD ? nblkT : nblkD;
 	auto up = [](size_t b) { return (b + (2u << 20) - 1) / (2u << 20) * (2u << 20); };
@@ -1753,9 +1803,12 @@ struct Impl {
 
 static void bind_impl(Batched *B) {
 	if (B->mixed) {
-		if (B->rbT == 4) {
-			B->setup_fn = B->rbD == 2 ? Impl<float, 4, 2>::setup : Impl<float, 4, 4>::setup;
-			B->chunk_fn = B->rbD == 2 ? Impl<float, 4, 2>::chunk : Impl<float, 4, 4>::chunk;
+		if (B->rbT == 4 && B->rbD == 4) {
+			B->setup_fn = Impl<float, 4, 4>::setup;
+			B->chunk_fn = Impl<float, 4, 4>::chunk;
+		} else if (B->rbT == 4) {
+			B->setup_fn = Impl<float, 4, 8>::setup;
+			B->chunk_fn = Impl<float, 4, 8>::chunk;
 		} else {
 			B->setup_fn = Impl<float, 8, 8>::setup;
 			B->chunk_fn = Impl<float, 8, 8>::chunk;
@@ -2270,6 +2323,151 @@ int batched_estimate_src(Ctx *c, int samples, const double *probes_dev, uint32_t
 	}
 	BTRY(cudaStreamSynchronize(c->stream));
 	return B->est.rc;
+}
+
+}  // namespace sedi
+
+namespace sedi {
+
+// ---------------------------------------------------------------------------
+// Autotuner.  For one (solver, precision, lanes, grid):
+//   1. lane-slice width W of the Krylov fields (FP32: 8 or 4 lanes; FP64: 8,
+//      4 or 2), each on a scratch context with the model's i3 split, scored
+//      by the summed per-iteration sweep time (CUDA events, kernels alone);
+//   2. the i3 split of the sweeps (the model's choice and 1, 2, 3, 4, 6, 8
+//      chunks) with the best W, same score;
+//   3. with flags & 1: iterations per captured graph (8, 16, 32) and, for the
+//      mixed form, the reliable-update period (20, 32, 50), each scored by the
+//      wall time of a real estimate of `batch` seeded probes to tol.
+// The winner is recorded in the process-wide table that context creation
+// reads, so contexts created afterwards (and the server's admission sizes)
+// use it.  out[0..3] = W, nz (0: model), period, chunk; *score_ms = the best
+// step-3 estimate time (or the step-2 sweep time without flags & 1).
+// ---------------------------------------------------------------------------
+static int tune_sweep_ms(sedi_ctx *h, double *ms_sum) {
+	double ms[8], by[8];
+	char names[8 * 32];
+	int cnt = 0;
+	const int rc = batched_time_kernels(&h->c, 5, ms, by, names, &cnt);
+	if (rc) return rc;
+	*ms_sum = 0.0;
+	for (int k = 0; k < cnt; k++) *ms_sum += ms[k];
+	return 0;
+}
+
+int batched_autotune(int solver, int precision, int batch, long long n1, long long n2, long long n3, int maxiter,
+                     double tol, uint32_t seed, int flags, int *out, double *score_ms) {
+	const bool mixed = precision == SEDI_PREC_MIXED;
+	if (batch < 2 && !mixed) return SEDI_ERR_ARG;  // one FP64 lane is the single-vector form
+	const int R = pick_R(batch, mixed);
+	const TuneKey key{solver, precision, R, n1, n2, n3};
+	std::vector<int> Ws;
+	if (R >= 8) {
+		Ws.push_back(8);
+		Ws.push_back(4);
+		if (!mixed) Ws.push_back(2);
+	} else {
+		Ws.push_back(slice_for(R, !mixed));
+	}
+	Tuning best;
+	double best_ms = -1.0;
+	auto score = [&](const Tuning &t, double *ms) -> int {
+		set_tuning(key, t);
+		int err = 0;
+		sedi_ctx *h = sedi_create(solver, (long)n1, (long)n2, (long)n3, 6.0, 1.0, 1.0, 0, precision, batch, &err);
+		if (!h) return err ? err : SEDI_ERR_CUDA;
+		const int rc = tune_sweep_ms(h, ms);
+		sedi_destroy(h);
+		return rc;
+	};
+	for (int W : Ws) {
+		Tuning t;
+		t.W = W;
+		double ms = 0.0;
+		const int rc = score(t, &ms);
+		if (rc == SEDI_ERR_NOMEM) continue;
+		if (rc) return rc;
+		if (best_ms < 0 || ms < best_ms) best_ms = ms, best = t;
+	}
+	if (best_ms < 0) return SEDI_ERR_NOMEM;
+	const int nzs[] = {1, 2, 3, 4, 6, 8};
+	for (int nz : nzs) {
+		if (nz > n3) break;
+		Tuning t = best;
+		t.nz = nz;
+		double ms = 0.0;
+		const int rc = score(t, &ms);
+		if (rc) return rc;
+		if (ms < 0.97 * best_ms) best_ms = ms, best = t;  // a clear win over the model's split
+	}
+	double best_est = -1.0;
+	if (flags & 1) {
+		set_tuning(key, best);
+		int err = 0;
+		sedi_ctx *h = sedi_create(solver, (long)n1, (long)n2, (long)n3, 6.0, 1.0, 1.0, 0, precision, batch, &err);
+		if (!h) return err ? err : SEDI_ERR_CUDA;
+		Ctx *c = &h->c;
+		Batched *B = (Batched *)c->batched;
+		const long long n = n1 * n2 * n3;
+		double *D = nullptr;
+		if (cudaMalloc(&D, sizeof(double) * n) != cudaSuccess) {
+			cudaGetLastError();
+			sedi_destroy(h);
+			return SEDI_ERR_NOMEM;
+		}
+		auto timed = [&](double *ms) -> int {
+			const auto t0 = std::chrono::steady_clock::now();
+			const int rc = batched_estimate_src(c, batch, nullptr, seed, maxiter, tol, 1, D, nullptr, nullptr,
+			                                    nullptr, nullptr, nullptr);
+			*ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+			return rc < 0 ? rc : 0;
+		};
+		const int periods_mixed[] = {20, 32, 50}, period_fp64[] = {B->period};
+		const int *periods = mixed ? periods_mixed : period_fp64;
+		const int np = mixed ? 3 : 1;
+		const int chunks[] = {16, 8, 32};
+		int rc = 0;
+		for (int ci = 0; ci < 3 && !rc; ci++) {
+			if (B->graph) {
+				cudaGraphExecDestroy(B->graph);
+				B->graph = nullptr;
+			}
+			B->chunk = chunks[ci];
+			for (int pi = 0; pi < np && !rc; pi++) {
+				if (ci > 0 && periods[pi] != (best.period ? best.period : B->period)) continue;  // chunks at the best period
+				B->period = periods[pi];
+				double ms = 0.0;
+				if (!B->graph && (rc = timed(&ms))) break;  // warm-up: graph capture for this chunk size
+				if ((rc = timed(&ms))) break;
+				if (best_est < 0 || ms < best_est) {
+					best_est = ms;
+					best.period = periods[pi];
+					best.chunk = chunks[ci];
+				}
+			}
+		}
+		cudaFree(D);
+		sedi_destroy(h);
+		if (rc) return rc;
+	}
+	set_tuning(key, best);
+	out[0] = best.W;
+	out[1] = best.nz;
+	out[2] = best.period;
+	out[3] = best.chunk;
+	if (score_ms) *score_ms = best_est >= 0 ? best_est : best_ms;
+	return 0;
+}
+
+int batched_config(const Ctx *c, int *out) {
+	const Batched *B = (const Batched *)c->batched;
+	if (!B) return SEDI_ERR_UNSUPPORTED;
+	out[0] = B->rbT;
+	out[1] = (int)B->gridT.z;
+	out[2] = B->period;
+	out[3] = B->chunk;
+	out[4] = B->R;
+	return 0;
 }
 
 }  // namespace sedi

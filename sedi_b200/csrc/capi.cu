@@ -100,6 +100,19 @@ const char *sedi_ctx_error(const sedi_ctx *h) { return h ? h->c.error.c_str() : 
 
 long long sedi_launch_count(const sedi_ctx *h) { return h ? h->c.launches : 0; }
 
+int sedi_autotune(int solver, int precision, int batch, long n1, long n2, long n3, int maxiter, double tol,
+                  uint32_t seed, int flags, int *choice, double *score_ms) {
+	if (solver < 1 || solver > 3 || (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED) || batch < 1 ||
+	    n1 < 1 || n2 < 1 || n3 < 1 || maxiter < 0 || !choice)
+		return SEDI_ERR_ARG;
+	return batched_autotune(solver, precision, batch, n1, n2, n3, maxiter, tol, seed, flags, choice, score_ms);
+}
+
+int sedi_ctx_config(const sedi_ctx *h, int *config) {
+	if (!h || !config) return SEDI_ERR_ARG;
+	return batched_config(&h->c, config);
+}
+
 int sedi_device_memory(double *used_mb, double *total_mb) {
 	if (!used_mb || !total_mb) return SEDI_ERR_ARG;
 	size_t fr = 0, tot = 0;

@@ -119,6 +119,10 @@ int batched_est_begin(Ctx *c, int samples, const double *probes_dev, uint32_t se
                       double *errs, int *results);
 int batched_est_advance(Ctx *c, int *done);
 int batched_est_result(const Ctx *c);
+// Autotuner and the launch choices of a batched context (see batched.cu).
+int batched_autotune(int solver, int precision, int batch, long long n1, long long n2, long long n3, int maxiter,
+                     double tol, uint32_t seed, int flags, int *out, double *score_ms);
+int batched_config(const Ctx *c, int *out);
 // Device bytes a batched context allocates (0 for the single-vector form).
 size_t batched_bytes(int solver, int precision, int batch, long long n1, long long n2, long long n3);
 

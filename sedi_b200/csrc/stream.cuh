@@ -125,13 +125,16 @@ __device__ __forceinline__ unsigned long long gtimer() {
 	return t;
 }
 // Bounded wait; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t *bar, unsigned parity, unsigned long long limit_ns) {
 	if (mbar_try(bar, parity)) return true;
 	const unsigned long long t0 = gtimer();
 	for (;;) {
 		if (mbar_try(bar, parity)) return true;
-		if (gtimer() - t0 > kWaitNs) return false;
+		if (gtimer() - t0 > limit_ns) return false;
 	}
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+	return mbar_wait_limit(bar, parity, kWaitNs);
 }
 __device__ __forceinline__ void fence_async_smem() {
 	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -261,3 +261,34 @@ def test_time_kernels_lists_solver_sweeps(solver, nk):
     with S.Context(solver, (64, 64, 64), precision=S.MIXED, batch=16) as c:
         ks = c.time_kernels(reps=2)
     assert len(ks) == nk and all(ms > 0 and by > 0 for _, ms, by in ks)
+
+
+@pytest.mark.parametrize("solver,prec", [("cg", S.FP64), ("cg", S.MIXED), ("pcg", S.MIXED), ("bicgstab", S.FP64)])
+def test_autotuned_context_keeps_results(solver, prec):
+    """The autotuner's choices (slice width, i3 split, graph chunk, reliable-update
+    period) change only launch shapes and summation order: FP64 CG/PCG stay
+    within 1e-10 of the untuned run with the same iteration counts, BiCGStab
+    FP64 within its 20-iteration bar, mixed within 1e-8 of FP64."""
+    dims, samples = (40, 36, 48), 16
+    maxiter, tol = (20, 0.0) if solver == "bicgstab" else (3000, 1e-9)
+    with S.Context(solver, dims, precision=prec, batch=samples) as c:
+        ref = c.estimate(samples, 321, maxiter, tol, ignore_errors=True)
+        before = c.config()
+    choice = S.autotune(solver, dims, samples, precision=prec, maxiter=maxiter, tol=tol, seed=321)
+    with S.Context(solver, dims, precision=prec, batch=samples) as c:
+        after = c.config()
+        got = c.estimate(samples, 321, maxiter, tol, ignore_errors=True)
+    assert after["slice_width"] == choice["slice_width"] and after["lanes"] == before["lanes"]
+    if choice["chunk"]:
+        assert after["chunk"] == choice["chunk"]
+    if prec == S.MIXED:
+        # Two mixed runs that both meet tol land at different x; each must be
+        # within the mixed bar of the FP64 answer on the same probes.
+        assert 20 <= after["period"] <= 50
+        with S.Context(solver, dims, precision=S.FP64, batch=samples) as c64:
+            r64 = c64.estimate(samples, 321, maxiter, tol, ignore_errors=True)
+        assert O.relmax(got["D"], r64["D"]) <= 1e-8
+        assert O.relmax(ref["D"], r64["D"]) <= 1e-8
+    else:
+        assert np.array_equal(got["iters"], ref["iters"]) and np.array_equal(got["results"], ref["results"])
+        assert O.relmax(got["D"], ref["D"]) <= 1e-10
