@@ -218,9 +218,10 @@ struct Layout {
 	static constexpr size_t OFF_RING = NST * STAGE_PAD;
 	static constexpr size_t OFF_BAR = OFF_RING + RING * HALO_PAD;
 	static constexpr size_t BYTES = OFF_BAR + NST * sizeof(uint64_t);
-	// The per-lane reduction scratch reuses the stage memory after the sweep.
+	// The per-lane reduction scratch reuses the stage and ring memory after
+	// the sweep (both are dead once the last plane is done).
 	static constexpr size_t RED_BYTES = (size_t)(ND > 0 ? ND : 1) * C::NPS * C::RB * sizeof(double);
-	static_assert(RED_BYTES <= OFF_RING, "reduction scratch must fit in the stages");
+	static_assert(RED_BYTES <= OFF_BAR, "reduction scratch must fit in the stages and the ring");
 	static constexpr unsigned TX = (unsigned)STAGE_BYTES;
 };
 

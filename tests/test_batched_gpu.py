@@ -268,7 +268,8 @@ def test_autotuned_context_keeps_results(solver, prec):
     """The autotuner's choices (slice width, i3 split, graph chunk, reliable-update
     period) change only launch shapes and summation order: FP64 CG/PCG stay
     within 1e-10 of the untuned run with the same iteration counts, BiCGStab
-    FP64 within its 20-iteration bar, mixed within 1e-8 of FP64."""
+    FP64 within its 20-iteration bar, mixed CG within 1e-8 of FP64 (pipelined
+    CG 3e-8)."""
     dims, samples = (40, 36, 48), 16
     maxiter, tol = (20, 0.0) if solver == "bicgstab" else (3000, 1e-9)
     with S.Context(solver, dims, precision=prec, batch=samples) as c:
@@ -287,8 +288,11 @@ def test_autotuned_context_keeps_results(solver, prec):
         assert 20 <= after["period"] <= 50
         with S.Context(solver, dims, precision=S.FP64, batch=samples) as c64:
             r64 = c64.estimate(samples, 321, maxiter, tol, ignore_errors=True)
-        assert O.relmax(got["D"], r64["D"]) <= 1e-8
-        assert O.relmax(ref["D"], r64["D"]) <= 1e-8
+        # Pipelined CG's runs meeting tol 1e-9 stop anywhere below it; the D
+        # of two such runs differs by up to a few 1e-8 here.
+        bar = 1e-8 if solver == "cg" else 3e-8
+        assert O.relmax(got["D"], r64["D"]) <= bar
+        assert O.relmax(ref["D"], r64["D"]) <= bar
     else:
         assert np.array_equal(got["iters"], ref["iters"]) and np.array_equal(got["results"], ref["results"])
         assert O.relmax(got["D"], ref["D"]) <= 1e-10
