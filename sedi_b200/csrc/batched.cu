@@ -1340,7 +1340,17 @@ static int pick_R(int nrhs, bool mixed) {
 	return (nrhs + full - 1) / full * full;
 }
 
-static int slice_for(int R, bool) { return R >= kSliceLanes ? kSliceLanes : R; }
+// Lanes per slice: FP64 fields 8 (64 B per point), FP32 Krylov fields 4
+// (16 B per point, 32x16 tiles).  Measured at 128^3 x 64 lanes on B200: the
+// FP32 sweeps are 2-19% faster with 4 lanes than with 8 (pipelined CG 1418 vs
+// 1685 us), the FP64 ones are not.  The autotuner may override it per shape.
+#ifndef SEDI_SLICE_LANES_FP32
+#define SEDI_SLICE_LANES_FP32 4
+#endif
+static int slice_for(int R, bool fp64) {
+	const int w = fp64 ? kSliceLanes : SEDI_SLICE_LANES_FP32;
+	return R >= w ? w : R;
+}
 
 static void tile_for(int rb, int eb, int *P1, int *P2) {
 	const int lg = rb * eb / 16;
