@@ -61,6 +61,7 @@ def parse():
                     help="solver of the timed form (profiling cases; the benchmark configuration is CG)")
     ap.add_argument("--serve-jobs", type=int, default=12, help="jobs in the serving run (0: skip it)")
     ap.add_argument("--serve-only", action="store_true", help="run only the serving measurement")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the autotuner (built-in launch choices)")
     ap.add_argument("--workload", choices=["dropin", "batched256", "large512"], default="dropin",
                     help="dropin: the benchmark line; batched256 / large512: the 256^3 x 128-probe and the "
                          "512^3 x 16-probe configurations, one line each")
@@ -253,8 +254,9 @@ def run_serving(S, njobs, maxiter=5000):
         "result_codes_nonzero": int(np.count_nonzero(rcs)) + int(np.count_nonzero(rc0)),
         "nonzero_jobs": [{"solver": str(jobs["solver"][k]), "edge": int(jobs["edge"][k]),
                           "precision": "fp64" if int(jobs["precision"][k]) == 0 else "mixed",
-                          "tol": float(jobs["tol"][k]), "samples": int(jobs["samples"][k]), "rc": int(rcs[k])}
-                         for k in range(njobs) if rcs[k] != 0],
+                          "tol": float(jobs["tol"][k]), "samples": int(jobs["samples"][k]),
+                          "rc_open_loop": int(rcs[k]), "rc_closed_loop": int(rc0[k])}
+                         for k in range(njobs) if rcs[k] != 0 or rc0[k] != 0],
         "peak_device_gb": st["peak_bytes"] / 1e9, "budget_gb": st["budget_bytes"] / 1e9,
         "contexts_created": st["ctx_created"], "contexts_reused": st["ctx_reused"], "max_running": st["max_running"],
         "mix": "edge U{32,48,64,96,128,192}^3, samples U{8..64}, tol logU[1e-10,1e-6], solver U{CG,PCG,BiCGStab}, "
@@ -420,6 +422,11 @@ def run_sedi(args):
     t = torch.empty(n, dtype=torch.float64, device=dev)
     q = torch.empty(n, dtype=torch.float64, device=dev)
     prec = S.MIXED if args.form == "mixed" else S.FP64
+    # Launch choices for this shape, measured before the timed region
+    # (slice width, i3 split, graph chunk, reliable-update period).
+    tuned = None
+    if not args.no_autotune and not args.no_extras:
+        tuned = S.autotune(args.solver, GRID, SAMPLES, precision=prec, maxiter=MAXITER, tol=TOL, seed=seed0)
     ctx = S.Context(args.solver, GRID, precision=prec, batch=SAMPLES)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream)
@@ -553,6 +560,7 @@ def run_sedi(args):
             cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": kind,
                    "sample": f"{procs} concurrent single-rank processes x 1 probe (128^3 CG tol 1e-9), {wall:.1f} s"}
         serving = run_serving(S, args.serve_jobs) if world == 1 and args.serve_jobs > 0 else None
+        ctx_config = ctx.config()
         gpoint = float(np.sum(it_all)) * n / args.steps / (ms / 1e3 / args.steps) / 1e9 if world == 1 else None
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -562,6 +570,7 @@ def run_sedi(args):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": list(GRID), "probes_per_gpu": SAMPLES, "solver": "cg",
                        "tol": TOL, "form": args.form, "parallelism": f"probe-sharded x{world}",
+                       "autotuned": tuned, "launch": ctx_config,
                        "l2": "inputs larger than L2 (1.07 GB probes + >=1.6 GB Krylov state per GPU)"},
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -64,7 +64,7 @@ struct Global {
 	int period;     // reliable-update period (mixed)
 	int nrhs;
 	int err;        // a bounded wait timed out
-	int pad;
+	int ru_all;     // the pending reliable update covers every lane (periodic)
 };
 
 // Arithmetic: FP64 keeps the reference's operator-by-operator rounding (no
@@ -131,7 +131,9 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 	const int slice = blockIdx.y, lane0 = slice * RB;
 	const int zoff = slice * g.n3;  // plane offset of this slice in the 4-D map
 	const int z0 = blockIdx.z * g.zc, z1 = min(z0 + g.zc, g.n3);
-	const int np = z1 - z0 + 2;  // planes z0-1 .. z1 (relative index j = p - z0 + 1)
+	// Planes z0-1 .. z1 (relative index j = p - z0 + 1); none when the op has
+	// no work for this lane slice (the block still joins the reduction).
+	const int np = op.slice_live(gl, ls, lane0, RB) ? z1 - z0 + 2 : 0;
 	const int lo = lg * V;
 	op.begin(gl, ls, lane0 + lo);
 
@@ -355,6 +357,7 @@ template <class T>
 struct OpBase {
 	T ka, kb, kc;
 	__device__ bool enabled(const Global *) const { return true; }
+	__device__ bool slice_live(const Global *, const LaneState &, int, int) const { return true; }
 };
 
 // ---------------------------------------------------------------------------
@@ -378,11 +381,20 @@ struct OpResid : OpBase<double> {
 	int it;
 	int keep[2], restart[2];
 	__device__ bool enabled(const Global *gl) const { return !ru || gl->ru_due; }
+	// A reliable update triggered by single lanes sweeps only their slices.
+	__device__ bool slice_live(const Global *gl, const LaneState &ls, int lane0, int nl) const {
+		if (!ru || pcg || gl->ru_all) return true;
+		for (int l = lane0; l < lane0 + nl; l++)
+			if (ls.pending[l]) return true;
+		return false;
+	}
 	__device__ bool raw_center() const { return false; }
 	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
 		it = gl->iter;
 		for (int e = 0; e < 2; e++) {
-			keep[e] = ru ? ls.done[lane + e] : 0;
+			// Lanes outside a lane-triggered update keep their recurrence r
+			// (their x_lo was not folded, so b - A x_hi is not their residual).
+			keep[e] = ru ? (ls.done[lane + e] || (!pcg && !gl->ru_all && !ls.pending[lane + e])) : 0;
 			restart[e] = ru && solver == 1 && !keep[e] && ls.s_exit[lane + e] == 2;
 		}
 		// BiCGStab: iteration it+1 reads r from R[(it+1)&1 ? 0 : 1].
@@ -417,6 +429,7 @@ struct OpResid : OpBase<double> {
 		const int maxiter = gl->maxiter;
 		if (ru) {
 			if (ls.done[lane]) return;
+			if (!pcg && !gl->ru_all && !ls.pending[lane]) return;  // not part of this update
 			const double err = sqrt(tot[1] / ls.bb[lane]);
 			ls.err[lane] = err;
 			ls.rr[lane] = tot[1];
@@ -592,7 +605,7 @@ struct OpCgB : OpBase<T> {
 				ls.pending[lane] = 1;
 				gl->ru_due = 1;
 			}
-			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = 1;
+			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = gl->ru_all = 1;
 		} else if (err <= tol) {  // :193
 			ls.done[lane] = 1;
 			ls.exit_iter[lane] = it;
@@ -707,7 +720,7 @@ struct OpPcg : OpBase<T> {
 				ls.pending[lane] = 1;
 				gl->ru_due = 1;
 			}
-			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = 1;
+			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = gl->ru_all = 1;
 		} else if (err <= tol) {
 			ls.done[lane] = 1;
 			ls.exit_iter[lane] = it;
@@ -1028,7 +1041,7 @@ struct OpBicg3 : OpBicgS<T> {
 				ls.pending[lane] = 1;
 				gl->ru_due = 1;
 			}
-			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = 1;
+			if (gl->period > 0 && it % gl->period == 0) gl->ru_due = gl->ru_all = 1;
 			return;
 		}
 		int stop = STOP_NONE, ex = 0;
@@ -1071,15 +1084,20 @@ __global__ void kb_setup_done(Global *gl) { gl->active -= 1; }  // drops the set
 __global__ void kb_ru_done(Global *gl) {
 	if (gl->ru_due) {
 		gl->ru_due = 0;
+		gl->ru_all = 0;
 		gl->iter += 1;
 	}
 }
 
 // Reliable update (MIXED): x_hi += x_lo, x_lo = 0.  x_hi uses FP64 slices
-// of width WD, x_lo FP32 slices of width WT.
+// of width WD, x_lo FP32 slices of width WT.  An update triggered by single
+// lanes (convergence claims, maxiter, breakdowns) folds only those lanes;
+// a periodic one (or any pipelined-CG one) folds every lane.
 __global__ void __launch_bounds__(256) kb_ru_fold(long long npts, int R, int WD, int WT, double *__restrict__ xh,
-                                                  float *__restrict__ xl, Global *gl) {
+                                                  float *__restrict__ xl, const int *__restrict__ pending, int all,
+                                                  Global *gl) {
 	if (gl->active == 0 || gl->ru_due == 0) return;
+	all = all || gl->ru_all;
 	const long long pairs = npts * R / 2;
 	for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < pairs;
 	     u += (long long)gridDim.x * blockDim.x) {
@@ -1088,6 +1106,7 @@ __global__ void __launch_bounds__(256) kb_ru_fold(long long npts, int R, int WD,
 		const long long rem = od - sd * WD * npts;
 		const long long i = rem / WD;
 		const int j = (int)(sd * WD + rem % WD);
+		if (!all && !pending[j] && !pending[j + 1]) continue;  // lanes j, j+1 share the pair
 		const long long ot = sliced(i, j, WT, npts);
 		const float2 lo = *reinterpret_cast<const float2 *>(xl + ot);
 		double2 hi = *reinterpret_cast<double2 *>(xh + od);
@@ -1628,7 +1647,8 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	if (B->mixed) {
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
-		                                                                 (float *)B->x, B->gl);
+		                                                                 (float *)B->x, B->ls.pending,
+		                                                                 c->solver == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD>(c, B, true);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
@@ -1684,7 +1704,8 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 		// w = A u and the next iteration's dots.
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
-		                                                                 (float *)B->x, B->gl);
+		                                                                 (float *)B->x, B->ls.pending,
+		                                                                 c->solver == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD>(c, B, true);
 		OpApply<T> a1;
@@ -1749,7 +1770,8 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 		// the next iteration reads; rho = <r, r_hat> (restarted lanes: r_hat = r).
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
-		                                                                 (float *)B->x, B->gl);
+		                                                                 (float *)B->x, B->ls.pending,
+		                                                                 c->solver == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD>(c, B, true);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
