@@ -1491,14 +1491,18 @@ int batched_alloc(Ctx *c) {
 				c->error = "device allocation failed (batched solver vectors)";
 				return SEDI_ERR_NOMEM;
 			}
-			cudaMemset(*pv[i], 0, B->elems * ts);
+			cudaMemsetAsync(*pv[i], 0, B->elems * ts, c->stream);
 		}
 	}
-	cudaMemset(B->ticket, 0, sizeof(unsigned));
-	cudaMemset(B->x, 0, B->elems * ts);
-	cudaMemset(B->r, 0, B->elems * ts);
-	cudaMemset(B->p0, 0, B->elems * ts);
-	cudaMemset(B->p1, 0, B->elems * ts);
+	// Zero-fills on the context's stream (its own, non-blocking one at this
+	// point): legacy-stream memsets would not be ordered before its kernels.
+	cudaMemsetAsync(B->ticket, 0, sizeof(unsigned), c->stream);
+	cudaMemsetAsync(B->x, 0, B->elems * ts, c->stream);
+	cudaMemsetAsync(B->r, 0, B->elems * ts, c->stream);
+	cudaMemsetAsync(B->p0, 0, B->elems * ts, c->stream);
+	cudaMemsetAsync(B->p1, 0, B->elems * ts, c->stream);
+	cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * 20 * B->R, c->stream);
+	cudaMemsetAsync(B->lane_int, 0, sizeof(int) * kLaneInts * B->R, c->stream);
 	const int R = B->R;
 	LaneState &ls = B->ls;
 	double **dp[] = {&ls.bb, &ls.rr, &ls.err, &ls.ru, &ls.ru_new, &ls.sp, &ls.alpha, &ls.beta, &ls.gamma,
@@ -1533,6 +1537,8 @@ int batched_alloc(Ctx *c) {
 	B->g0_host = B->gl_host + 1;
 	B->lane_res.assign(B->R, 0);
 	bind_impl(B);
+	// The zero-fills must be complete before a caller stream (sedi_set_stream) uses the buffers.
+	if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_cuda_error(c, cudaGetLastError(), "batched_alloc");
 	return 0;
 }
 
@@ -2152,8 +2158,8 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	BTRY(cudaGetLastError());
-	if (B->gl_host && cudaMemcpy(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost) == cudaSuccess &&
-	    B->gl_host->err) {
+	if (B->gl_host && cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+	    cudaStreamSynchronize(s) == cudaSuccess && B->gl_host->err) {
 		c->error = "batched sweep timed out waiting for its data";
 		return SEDI_ERR_CUDA;
 	}

@@ -158,11 +158,12 @@ int sedi_solve(sedi_ctx *h, const double *b, double *x, const double *iM, int ma
 			return set_cuda_error(c, cudaErrorMemoryAllocation, "cudaMalloc");
 		}
 		int res = 0, rc = 0;
-		if (cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
-		    cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+		if (cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+		    cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
 			rc = set_cuda_error(c, cudaGetLastError(), "cudaMemcpy");
 		if (!rc) rc = batched_solve_dev(c, 1, db, dx, maxiter, tol, final_err, final_iter, &res);
-		if (!rc && cudaMemcpy(x, dx, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
+		if (!rc && (cudaMemcpyAsync(x, dx, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+		            cudaStreamSynchronize(c->stream) != cudaSuccess))
 			rc = set_cuda_error(c, cudaGetLastError(), "cudaMemcpy");
 		cudaFree(db);
 		cudaFree(dx);
@@ -198,10 +199,12 @@ int sedi_stencil_apply(sedi_ctx *h, const double *x, double *y) {
 		return set_cuda_error(c, cudaErrorMemoryAllocation, "cudaMalloc");
 	}
 	int rc = 0;
-	if (cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice) != cudaSuccess) rc = set_cuda_error(c, cudaGetLastError(), "H2D");
+	if (cudaMemcpyAsync(dx, x, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) rc = set_cuda_error(c, cudaGetLastError(), "H2D");
 	if (!rc) rc = plain_stencil(c, dx, dy);
 	if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = set_cuda_error(c, cudaGetLastError(), "stencil");
-	if (!rc && cudaMemcpy(y, dy, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) rc = set_cuda_error(c, cudaGetLastError(), "D2H");
+	if (!rc && (cudaMemcpyAsync(y, dy, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+	            cudaStreamSynchronize(c->stream) != cudaSuccess))
+		rc = set_cuda_error(c, cudaGetLastError(), "D2H");
 	cudaFree(dx);
 	cudaFree(dy);
 	return rc;
@@ -394,11 +397,12 @@ int sedi_solve_batch(sedi_ctx *h, int nrhs, const double *b, double *x, int maxi
 		return set_cuda_error(c, cudaErrorMemoryAllocation, "cudaMalloc");
 	}
 	int rc = 0;
-	if (cudaMemcpy(db, b, bytes * nrhs, cudaMemcpyHostToDevice) != cudaSuccess ||
-	    cudaMemcpy(dx, x, bytes * nrhs, cudaMemcpyHostToDevice) != cudaSuccess)
+	if (cudaMemcpyAsync(db, b, bytes * nrhs, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+	    cudaMemcpyAsync(dx, x, bytes * nrhs, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
 		rc = set_cuda_error(c, cudaGetLastError(), "upload");
 	if (!rc) rc = batched_solve_dev(c, nrhs, db, dx, maxiter, tol, final_err, final_iter, results);
-	if (rc >= 0 && cudaMemcpy(x, dx, bytes * nrhs, cudaMemcpyDeviceToHost) != cudaSuccess)
+	if (rc >= 0 && (cudaMemcpyAsync(x, dx, bytes * nrhs, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+	                cudaStreamSynchronize(c->stream) != cudaSuccess))
 		rc = set_cuda_error(c, cudaGetLastError(), "download");
 	cudaFree(db);
 	cudaFree(dx);

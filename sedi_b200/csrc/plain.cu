@@ -506,7 +506,8 @@ int plain_alloc(Ctx *c) {
 	const size_t sweep_blocks = (size_t)l.grid.x * l.grid.y * l.grid.z;
 	SEDI_TRY(cudaMalloc(&c->partials, sizeof(double) * kMaxDots * (sweep_blocks > (size_t)c->nblocks ? sweep_blocks : (size_t)c->nblocks)));
 	SEDI_TRY(cudaMalloc(&c->ticket, sizeof(unsigned)));
-	SEDI_TRY(cudaMemset(c->ticket, 0, sizeof(unsigned)));
+	SEDI_TRY(cudaMemsetAsync(c->ticket, 0, sizeof(unsigned), c->stream));  // ordered before the context's kernels
+	SEDI_TRY(cudaStreamSynchronize(c->stream));
 	SEDI_TRY(cudaMalloc(&c->st, sizeof(SolveState)));
 	SEDI_TRY(cudaMallocHost(&c->st_host, sizeof(SolveState)));
 	c->hist_cap = 0;
@@ -720,7 +721,8 @@ int plain_divide(Ctx *c, double *D_dev) {
 int plain_history(Ctx *c, double *out, int len) {
 	int n = c->hist_len < len ? c->hist_len : len;
 	if (n <= 0 || !c->hist) return 0;
-	SEDI_TRY(cudaMemcpy(out, c->hist, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost));
+	SEDI_TRY(cudaMemcpyAsync(out, c->hist, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+	SEDI_TRY(cudaStreamSynchronize(c->stream));
 	return n;
 }
 

@@ -120,3 +120,24 @@ def test_submit_rejects_what_cannot_fit():
     with S.Server(budget_bytes=64 << 20) as srv:
         with pytest.raises(S.SediError):
             srv.submit("cg", (256, 256, 256), 64, 1, 10, 1e-8)
+
+
+def test_burst_of_fresh_contexts_matches_direct():
+    """Many jobs submitted at once: every context is created while others
+    already run on the GPU.  Each result must still equal the direct
+    estimator's bit for bit (the contexts' zero-fills are ordered before
+    their first kernels on their own streams)."""
+    rng = np.random.default_rng(11)
+    jobs = []
+    for k in range(10):
+        solver = ["cg", "pcg", "bicgstab"][k % 3]
+        edge = int(rng.choice([24, 32, 40, 48]))
+        jobs.append((solver, (edge, edge, edge), int(rng.integers(6, 40)), 500 + 37 * k, 3000,
+                     float(10.0 ** rng.uniform(-10, -7)), S.MIXED if k % 2 else S.FP64))
+    with S.Server(max_active=8) as srv:
+        ids = [_submit(srv, j) for j in jobs]
+        srv.wait()
+        lanes = [srv.info(i)["lanes"] for i in ids]
+        got = [srv.take(i) for i in ids]
+    for j, l, g in zip(jobs, lanes, got):
+        _same(g, _direct(j, l))
