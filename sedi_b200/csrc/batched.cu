@@ -355,6 +355,7 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 
 template <class T>
 struct OpBase {
+	static constexpr int KIND = 0;  // tile configuration (see CfgFor)
 	T ka, kb, kc;
 	__device__ bool enabled(const Global *) const { return true; }
 	__device__ bool slice_live(const Global *, const LaneState &, int, int) const { return true; }
@@ -499,6 +500,7 @@ struct OpResid : OpBase<double> {
 // ---------------------------------------------------------------------------
 template <class T>
 struct OpCgA : OpBase<T> {
+	static constexpr int KIND = 1;
 	static constexpr int NS = 2, NQ = 0, ND = 2;
 	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
 	static constexpr int V = Vec<T>::V;
@@ -929,6 +931,7 @@ struct OpBicgS : OpBase<T> {  // sweeps 2 and 3 share s, s_hat, t
 
 template <class T>
 struct OpBicg2 : OpBicgS<T> {
+	static constexpr int KIND = 1;
 	static constexpr int NS = 2, NQ = 0, ND = 3;
 	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
 	static constexpr int V = Vec<T>::V;
@@ -962,6 +965,7 @@ struct OpBicg2 : OpBicgS<T> {
 
 template <class T>
 struct OpBicg3 : OpBicgS<T> {
+	static constexpr int KIND = 1;
 	static constexpr int NS = 2, NQ = 0, ND = 2;
 	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
 	static constexpr int V = Vec<T>::V;
@@ -1293,9 +1297,9 @@ struct Batched {
 	long long graph_kernels = 0;
 	// launch shapes
 	int rbT = 0, rbD = 0;  // lanes per block slice for T and FP64 streams
-	SGeo gT, gD;
-	dim3 gridT, gridD;
-	Maps mapsT, mapsD;
+	SGeo gT, gD, gT1;
+	dim3 gridT, gridD, gridT1;
+	Maps mapsT, mapsD, mapsT1;  // mapsT1, gT1: the wide-tile (KIND 1) sweeps
 };
 
 #define BTRY(expr)                                                            \
@@ -1345,10 +1349,17 @@ __host__ __device__ constexpr int tile_p2(int lg) {
 	return lg == 1 ? SEDI_TILE_P2_LG1 : (lg == 2 ? SEDI_TILE_P2_LG2 : SEDI_TILE_P2_LG4);
 }
 
-template <class T, int RB>
+// KIND 1 ("wide") for sweeps with at most two stencil sources and no TMA
+// pointwise fields: with one lane group per point (FP32 4-lane slices) a
+// 32x32 tile, two output points per thread and a 4-stage ring (the per-plane
+// barrier and latency are paid once per two points; 222 KB of shared
+// memory).  Measured on B200 at 128^3 x 64 lanes: CG A 449 -> 372 us,
+// BiCGStab 2 463 -> 353 us, BiCGStab 3 877 -> 787 us.
+template <class T, int RB, int KIND = 0>
 struct CfgFor {
 	static constexpr int LG = RB * (int)sizeof(T) / 16;
-	typedef Cfg<T, RB, tile_p1(LG), tile_p2(LG), kThr> type;
+	static constexpr bool WIDE = KIND == 1 && LG == 1;
+	typedef Cfg<T, RB, tile_p1(LG), WIDE ? 32 : tile_p2(LG), kThr, WIDE ? 4 : 0> type;
 };
 
 static int pick_R(int nrhs, bool mixed) {
@@ -1371,15 +1382,15 @@ static int slice_for(int R, bool fp64) {
 	return R >= w ? w : R;
 }
 
-static void tile_for(int rb, int eb, int *P1, int *P2) {
+static void tile_for(int rb, int eb, int *P1, int *P2, int kind = 0) {
 	const int lg = rb * eb / 16;
 	*P1 = tile_p1(lg);
-	*P2 = tile_p2(lg);
+	*P2 = (kind == 1 && lg == 1) ? 32 : tile_p2(lg);
 }
 
-static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int nz_force = 0) {
+static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int nz_force = 0, int kind = 0) {
 	int P1, P2;
-	tile_for(rb, eb, &P1, &P2);
+	tile_for(rb, eb, &P1, &P2, kind);
 	const int t1 = (g.n1 + P1 - 1) / P1, t2 = (g.n2 + P2 - 1) / P2;
 	const int slices = R / rb;
 	// Split i3 into nz chunks of zc planes.  Blocks run in waves of
@@ -1432,6 +1443,14 @@ static int launch(Ctx *c, Batched *B, const SGeo &sg, dim3 grid, const Maps &map
 	return 0;
 }
 
+// Launch of a sweep over the T (Krylov) fields with the op's tile kind.
+template <class T, int RBT, class Op>
+static int launchT(Ctx *c, Batched *B, const Op &op, cudaStream_t s) {
+	typedef typename CfgFor<T, RBT, Op::KIND>::type C;
+	if (Op::KIND == 1) return launch<C>(c, B, B->gT1, B->gridT1, B->mapsT1, op, s);
+	return launch<C>(c, B, B->gT, B->gridT, B->mapsT, op, s);
+}
+
 static void bind_impl(Batched *B);
 
 int batched_alloc(Ctx *c) {
@@ -1458,10 +1477,13 @@ int batched_alloc(Ctx *c) {
 	if (tu.period > 0) B->period = tu.period;
 	if (tu.chunk > 0) B->chunk = tu.chunk;
 	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz);
+	shape(c->g, B->R, B->rbT, ebT, &B->gT1, &B->gridT1, tu.nz, 1);
 	shape(c->g, B->R, B->rbD, 8, &B->gD, &B->gridD, tu.nz);
 	const size_t ts = B->mixed ? sizeof(float) : sizeof(double);
 	const size_t nblkT = (size_t)B->gridT.x * B->gridT.z, nblkD = (size_t)B->gridD.x * B->gridD.z;
-	const size_t nblk = nblkT > nblkD ? nblkT : nblkD;
+	const size_t nblkT1 = (size_t)B->gridT1.x * B->gridT1.z;
+	size_t nblk = nblkT > nblkD ? nblkT : nblkD;
+	if (nblkT1 > nblk) nblk = nblkT1;
 	if (cudaMalloc(&B->x, B->elems * ts) != cudaSuccess || cudaMalloc(&B->r, B->elems * ts) != cudaSuccess ||
 	    cudaMalloc(&B->p0, B->elems * ts) != cudaSuccess || cudaMalloc(&B->p1, B->elems * ts) != cudaSuccess ||
 	    cudaMalloc(&B->b, B->elems * sizeof(double)) != cudaSuccess ||
@@ -1513,20 +1535,25 @@ int batched_alloc(Ctx *c) {
 	for (size_t i = 0; i < 5; i++) *ip[i] = B->lane_int + i * R;
 	// Tensor maps.
 	int P1, P2;
-	tile_for(B->rbT, ebT, &P1, &P2);
-	bool ok = make_map(&B->mapsT.m[MT_R_HALO], B->r, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
-	          make_map(&B->mapsT.m[MT_P0_HALO], B->p0, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
-	          make_map(&B->mapsT.m[MT_P1_HALO], B->p1, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
-	          make_map(&B->mapsT.m[MT_X_INT], B->x, ebT, c->g, R, B->rbT, P1, P2) &&
-	          make_map(&B->mapsT.m[MT_R_INT], B->r, ebT, c->g, R, B->rbT, P1, P2);
-	if (c->solver == 3)
-		ok = ok && make_map(&B->mapsT.m[MT_W0_HALO], B->w[0], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
-		     make_map(&B->mapsT.m[MT_W1_HALO], B->w[1], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
-		     make_map(&B->mapsT.m[MT_Q_HALO], B->q, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2);
-	if (c->solver == 1)
-		ok = ok && make_map(&B->mapsT.m[MT_R1_HALO], B->r1, ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
-		     make_map(&B->mapsT.m[MT_V0_HALO], B->v[0], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2) &&
-		     make_map(&B->mapsT.m[MT_V1_HALO], B->v[1], ebT, c->g, R, B->rbT, P1 + 2, P2 + 2);
+	auto t_maps = [&](Maps &M, int kind) {
+		int Q1, Q2;
+		tile_for(B->rbT, ebT, &Q1, &Q2, kind);
+		bool k = make_map(&M.m[MT_R_HALO], B->r, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
+		         make_map(&M.m[MT_P0_HALO], B->p0, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
+		         make_map(&M.m[MT_P1_HALO], B->p1, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
+		         make_map(&M.m[MT_X_INT], B->x, ebT, c->g, R, B->rbT, Q1, Q2) &&
+		         make_map(&M.m[MT_R_INT], B->r, ebT, c->g, R, B->rbT, Q1, Q2);
+		if (c->solver == 3)
+			k = k && make_map(&M.m[MT_W0_HALO], B->w[0], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
+			    make_map(&M.m[MT_W1_HALO], B->w[1], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
+			    make_map(&M.m[MT_Q_HALO], B->q, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2);
+		if (c->solver == 1)
+			k = k && make_map(&M.m[MT_R1_HALO], B->r1, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
+			    make_map(&M.m[MT_V0_HALO], B->v[0], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
+			    make_map(&M.m[MT_V1_HALO], B->v[1], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2);
+		return k;
+	};
+	bool ok = t_maps(B->mapsT, 0) && t_maps(B->mapsT1, 1);
 	tile_for(B->rbD, 8, &P1, &P2);
 	ok = ok && make_map(&B->mapsD.m[MD_X_HALO], B->mixed ? (void *)B->xh : B->x, 8, c->g, R, B->rbD, P1 + 2, P2 + 2) &&
 	     make_map(&B->mapsD.m[MD_B_INT], B->b, 8, c->g, R, B->rbD, P1, P2);
@@ -1560,8 +1587,12 @@ size_t batched_bytes(int solver, int precision, int batch, long long n1, long lo
 	dim3 gT, gD;
 	shape(g, R, wT, (int)ts, &sT, &gT, tu.nz);
 	shape(g, R, mixed ? slice_for(R, true) : wT, 8, &sD, &gD, tu.nz);
-	const size_t nblkT = (size_t)gT.x * gT.z, nblkD = (size_t)gD.x * gD.z;
-	const size_t nblk = nblkT > nblkD ? nblkT : nblkD;
+	SGeo sT1;
+	dim3 gT1;
+	shape(g, R, wT, (int)ts, &sT1, &gT1, tu.nz, 1);
+	const size_t nblkT = (size_t)gT.x * gT.z, nblkD = (size_t)gD.x * gD.z, nblkT1 = (size_t)gT1.x * gT1.z;
+	size_t nblk = nblkT > nblkD ? nblkT : nblkD;
+	if (nblkT1 > nblk) nblk = nblkT1;
 	auto up = [](size_t b) { return (b + (2u << 20) - 1) / (2u << 20) * (2u << 20); };
 	const int nT = 4 + (solver == 3 ? 6 : 0) + (solver == 1 ? 4 : 0);
 	size_t total = nT * up(elems * ts) + up(elems * 8) * (mixed ? 2 : 1);
@@ -1629,7 +1660,6 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 
 template <class T, int RBT, int RBD>
 static void enqueue_cg_iteration(Ctx *c, Batched *B) {
-	typedef typename CfgFor<T, RBT>::type C;
 	cudaStream_t s = c->stream;
 	OpCgA<T> a;
 	a.ka = (T)c->k.a;
@@ -1638,7 +1668,7 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	a.iMc = (T)(1.0 / c->k.a);
 	a.p0 = (T *)B->p0;
 	a.p1 = (T *)B->p1;
-	launch<C>(c, B, B->gT, B->gridT, B->mapsT, a, s);
+	launchT<T, RBT>(c, B, a, s);
 	OpCgB<T> bo;
 	bo.ka = (T)c->k.a;
 	bo.kb = (T)c->k.b;
@@ -1647,7 +1677,7 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	bo.x = (T *)B->x;
 	bo.r = (T *)B->r;
 	bo.mixed = B->mixed ? 1 : 0;
-	launch<C>(c, B, B->gT, B->gridT, B->mapsT, bo, s);
+	launchT<T, RBT>(c, B, bo, s);
 	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
 	c->launches++;
 	if (B->mixed) {
@@ -1664,7 +1694,6 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 
 template <class T, int RBT>
 static void enqueue_pcg_uw(Ctx *c, Batched *B, int zero, int ru) {
-	typedef typename CfgFor<T, RBT>::type C;
 	OpPcgUW<T> o;
 	o.ka = (T)c->k.a;
 	o.kb = (T)c->k.b;
@@ -1679,12 +1708,11 @@ static void enqueue_pcg_uw(Ctx *c, Batched *B, int zero, int ru) {
 	o.z = (T *)B->z;
 	o.zero = zero;
 	o.ru = ru;
-	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o, c->stream);
+	launchT<T, RBT>(c, B, o, c->stream);
 }
 
 template <class T, int RBT, int RBD>
 static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
-	typedef typename CfgFor<T, RBT>::type C;
 	cudaStream_t s = c->stream;
 	OpPcg<T> o;
 	o.ka = (T)c->k.a;
@@ -1701,7 +1729,7 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 	o.w0 = (T *)B->w[0];
 	o.w1 = (T *)B->w[1];
 	o.mixed = B->mixed ? 1 : 0;
-	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o, s);
+	launchT<T, RBT>(c, B, o, s);
 	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
 	c->launches++;
 	if (B->mixed) {
@@ -1722,12 +1750,12 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 		a1.y = (T *)B->sv;
 		a1.y2 = (T *)B->q;
 		a1.map = MT_P0_HALO;
-		launch<C>(c, B, B->gT, B->gridT, B->mapsT, a1, s);
+		launchT<T, RBT>(c, B, a1, s);
 		OpApply<T> a2 = a1;
 		a2.y = (T *)B->z;
 		a2.y2 = nullptr;
 		a2.map = MT_Q_HALO;
-		launch<C>(c, B, B->gT, B->gridT, B->mapsT, a2, s);
+		launchT<T, RBT>(c, B, a2, s);
 		enqueue_pcg_uw<T, RBT>(c, B, 0, 1);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
 		c->launches++;
@@ -1736,7 +1764,6 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 
 template <class T, int RBT, int RBD>
 static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
-	typedef typename CfgFor<T, RBT>::type C;
 	cudaStream_t s = c->stream;
 	const T ka = (T)c->k.a, kb = (T)c->k.b, kc = (T)c->k.c, iMc = (T)(1.0 / c->k.a);
 	OpBicg1<T> o1;
@@ -1749,13 +1776,13 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	o1.v0 = (T *)B->v[0];
 	o1.v1 = (T *)B->v[1];
 	o1.rhat = (T *)B->rhat;
-	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o1, s);
+	launchT<T, RBT>(c, B, o1, s);
 	OpBicg2<T> o2;
 	o2.ka = ka;
 	o2.kb = kb;
 	o2.kc = kc;
 	o2.iMc = iMc;
-	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o2, s);
+	launchT<T, RBT>(c, B, o2, s);
 	OpBicg3<T> o3;
 	o3.ka = ka;
 	o3.kb = kb;
@@ -1768,7 +1795,7 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	o3.p1 = (T *)B->p1;
 	o3.rhat = (T *)B->rhat;
 	o3.mixed = B->mixed ? 1 : 0;
-	launch<C>(c, B, B->gT, B->gridT, B->mapsT, o3, s);
+	launchT<T, RBT>(c, B, o3, s);
 	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
 	c->launches++;
 	if (B->mixed) {
@@ -2017,7 +2044,6 @@ int batched_solve_dev(Ctx *c, int nrhs, const double *b, double *x, int maxiter,
 // sedi_time_kernels): every lane active, no lane stops, no reliable update.
 template <class T, int RBT>
 static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *bytes, char *names, int *count) {
-	typedef typename CfgFor<T, RBT>::type C;
 	cudaStream_t s = c->stream;
 	Global g = {};
 	g.iter = 2;
@@ -2065,9 +2091,9 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		o.w0 = (T *)B->w[0];
 		o.w1 = (T *)B->w[1];
 		o.mixed = 0;
-		launch<C>(c, B, B->gT, B->gridT, B->mapsT, o, s);
+		launchT<T, RBT>(c, B, o, s);
 		BTRY(cudaEventRecord(e0, s));
-		for (int i = 0; i < reps; i++) launch<C>(c, B, B->gT, B->gridT, B->mapsT, o, s);
+		for (int i = 0; i < reps; i++) launchT<T, RBT>(c, B, o, s);
 		BTRY(cudaEventRecord(e1, s));
 		BTRY(cudaEventSynchronize(e1));
 		float t = 0.f;
@@ -2117,9 +2143,9 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		                                          // 3: r, v, x, p, r_hat in, x, r out
 		for (int k = 0; k < 3; k++) {
 			auto one = [&]() {
-				if (k == 0) launch<C>(c, B, B->gT, B->gridT, B->mapsT, o1, s);
-				else if (k == 1) launch<C>(c, B, B->gT, B->gridT, B->mapsT, o2, s);
-				else launch<C>(c, B, B->gT, B->gridT, B->mapsT, o3, s);
+				if (k == 0) launchT<T, RBT>(c, B, o1, s);
+				else if (k == 1) launchT<T, RBT>(c, B, o2, s);
+				else launchT<T, RBT>(c, B, o3, s);
 			};
 			one();
 			BTRY(cudaEventRecord(e0, s));
@@ -2139,12 +2165,12 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		return 0;
 	}
 	for (int k = 0; k < 2; k++) {
-		if (k == 0) launch<C>(c, B, B->gT, B->gridT, B->mapsT, a, s);
-		else launch<C>(c, B, B->gT, B->gridT, B->mapsT, bo, s);
+		if (k == 0) launchT<T, RBT>(c, B, a, s);
+		else launchT<T, RBT>(c, B, bo, s);
 		BTRY(cudaEventRecord(e0, s));
 		for (int i = 0; i < reps; i++) {
-			if (k == 0) launch<C>(c, B, B->gT, B->gridT, B->mapsT, a, s);
-			else launch<C>(c, B, B->gT, B->gridT, B->mapsT, bo, s);
+			if (k == 0) launchT<T, RBT>(c, B, a, s);
+			else launchT<T, RBT>(c, B, bo, s);
 		}
 		BTRY(cudaEventRecord(e1, s));
 		BTRY(cudaEventSynchronize(e1));

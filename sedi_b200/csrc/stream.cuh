@@ -167,9 +167,10 @@ __host__ __device__ __forceinline__ long long sliced(long long i, int j, int W, 
 	return ((long long)(j / W) * npts + i) * W + (j % W);
 }
 
-template <class T, int RB_, int P1_, int P2_, int THREADS_ = 512>
+template <class T, int RB_, int P1_, int P2_, int THREADS_ = 512, int NSTR_ = 0>
 struct Cfg {
 	typedef T type;
+	static constexpr int NSTR = NSTR_;  // stages of a transforming sweep's ring (0: SEDI_STREAM_NST_RING)
 	static constexpr int V = Vec<T>::V;
 	static constexpr int RB = RB_;
 	static constexpr int LG = RB / V;  // lane groups per point
@@ -204,7 +205,7 @@ struct Cfg {
 template <class C, int NS, int NQ, int ND, bool IDENT>
 struct Layout {
 	typedef typename C::type T;
-	static constexpr int NST = IDENT ? SEDI_STREAM_NST_IDENT : SEDI_STREAM_NST_RING;
+	static constexpr int NST = IDENT ? SEDI_STREAM_NST_IDENT : (C::NSTR > 0 ? C::NSTR : SEDI_STREAM_NST_RING);
 	static constexpr int KEEP = IDENT ? 3 : 2;  // steps a stage outlives its arrival
 	static_assert(NST > KEEP + 1, "ring too shallow");
 	// Every TMA destination starts on a 128-byte boundary.
@@ -218,6 +219,7 @@ struct Layout {
 	static constexpr size_t OFF_RING = NST * STAGE_PAD;
 	static constexpr size_t OFF_BAR = OFF_RING + RING * HALO_PAD;
 	static constexpr size_t BYTES = OFF_BAR + NST * sizeof(uint64_t);
+	static_assert(BYTES <= 232448, "a sweep's shared memory must fit one block on sm_100 (227 KB)");
 	// The per-lane reduction scratch reuses the stage and ring memory after
 	// the sweep (both are dead once the last plane is done).
 	static constexpr size_t RED_BYTES = (size_t)(ND > 0 ? ND : 1) * C::NPS * C::RB * sizeof(double);
