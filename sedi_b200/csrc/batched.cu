@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 	typedef typename C::type T;
 	constexpr int V = C::V, LG = C::LG, RB = C::RB, P1 = C::P1, H1 = C::H1, HALO = C::HALO, INT = C::INT,
 	              NPS = C::NPS, KC = C::KC, KO = C::KO;
-	constexpr int NS = Op::NS, NQ = Op::NQ, ND = Op::ND;
+	constexpr int NS = Op::NS, NQ = Op::NQ, ND = Op::ND, NGX = Op::NG > 0 ? Op::NG : 1;
 	constexpr bool IDENT = Op::IDENT;
 	typedef Layout<C, NS, NQ, ND, IDENT> Lay;
 	constexpr int NST = Lay::NST, KEEP = Lay::KEEP;
@@ -209,6 +209,16 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 		// block barrier at the end of the step.
 		bool ok = true;
 		if (j < np) ok = mbar_wait(&bar[sj], par);
+		// Pointwise fields an op reads with plain loads (Op::NG of them): issue
+		// the loads for this step's outputs (plane j-2) before the halo
+		// transform, so they are in flight during it.
+		Vec<T> gv[KO][NGX];
+		if (Op::NG > 0 && j >= 3) {
+			const long long zb = (long long)(z0 - 1 + j - 2) * plane;
+#pragma unroll
+			for (int k = 0; k < KO; k++)
+				if (oval >> k & 1u) op.gload(((long long)slice * g.npts + zb + obase[k]) * RB + lo, gv[k]);
+		}
 		// Phase 1: stencil input of plane j (transforming ops only).
 		if (!IDENT && j < np) {
 			const int p = z0 - 1 + j;
@@ -278,7 +288,7 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 				}
 				const long long pidx = (long long)z * plane + obase[k];
 				const long long o = ((long long)slice * g.npts + pidx) * RB + lo;
-				op.out(o, pidx, lane0 + lo, xc, y, qv, rc, part);
+				op.out(o, pidx, lane0 + lo, xc, y, qv, rc, gv[k], part);
 			}
 		}
 		if (__syncthreads_or(!ok)) {
@@ -356,7 +366,9 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 template <class T>
 struct OpBase {
 	static constexpr int KIND = 0;  // tile configuration (see CfgFor)
+	static constexpr int NG = 0;    // pointwise fields read with plain loads, prefetched by gload
 	T ka, kb, kc;
+	__device__ void gload(long long, Vec<T> *) const {}
 	__device__ bool enabled(const Global *) const { return true; }
 	__device__ bool slice_live(const Global *, const LaneState &, int, int) const { return true; }
 };
@@ -405,7 +417,7 @@ struct OpResid : OpBase<double> {
 	__device__ int q_map(int) const { return MD_B_INT; }
 	__device__ Vec<double> src(const Vec<double> *raw) const { return raw[0]; }
 	__device__ void out(long long, long long pidx, int lane, const Vec<double> &, const Vec<double> &ax,
-	                    const Vec<double> *q, const Vec<double> *, double (&part)[ND][2]) const {
+	                    const Vec<double> *q, const Vec<double> *, const Vec<double> *gv, double (&part)[ND][2]) const {
 		const long long ot = sliced(pidx, lane, WT, npts);  // lanes lane, lane+1 share a TR slice
 #pragma unroll
 		for (int e = 0; e < 2; e++) {
@@ -534,7 +546,7 @@ struct OpCgA : OpBase<T> {
 		return o;
 	}
 	__device__ void out(long long o, long long, int, const Vec<T> &pc, const Vec<T> &s, const Vec<T> *,
-	                    const Vec<T> *rc, double (&part)[ND][V]) const {
+	                    const Vec<T> *rc, const Vec<T> *gv, double (&part)[ND][V]) const {
 		stg(pout + o, pc);
 #pragma unroll
 		for (int e = 0; e < V; e++) dacc(part[0][e], s.v[e], pc.v[e]);
@@ -579,7 +591,7 @@ struct OpCgB : OpBase<T> {
 	__device__ bool raw_center() const { return false; }
 	__device__ Vec<T> src(const Vec<T> *raw) const { return raw[0]; }
 	__device__ void out(long long o, long long, int, const Vec<T> &pc, const Vec<T> &s, const Vec<T> *q,
-	                    const Vec<T> *, double (&part)[ND][V]) const {
+	                    const Vec<T> *, const Vec<T> *gv, double (&part)[ND][V]) const {
 		Vec<T> xv = q[0], rv = q[1];
 #pragma unroll
 		for (int e = 0; e < V; e++) {
@@ -670,7 +682,7 @@ struct OpPcg : OpBase<T> {
 		return o;
 	}
 	__device__ void out(long long o, long long, int, const Vec<T> &mc, const Vec<T> &nc, const Vec<T> *,
-	                    const Vec<T> *rc, double (&part)[ND][V]) const {
+	                    const Vec<T> *rc, const Vec<T> *gv, double (&part)[ND][V]) const {
 		const Vec<T> wv = rc[0];
 		Vec<T> qv = ldg_rw(q + o), sv = ldg_rw(s + o), pv = ldg_rw(p + o), zv = ldg_rw(z + o);
 		Vec<T> rv = ldg_rw(r + o), xv = ldg_rw(x + o), uv = ldg_rw(u + o), wnv;
@@ -766,7 +778,7 @@ struct OpPcgUW : OpBase<T> {
 		return o;
 	}
 	__device__ void out(long long o, long long, int, const Vec<T> &uc, const Vec<T> &wv, const Vec<T> *,
-	                    const Vec<T> *rc, double (&part)[ND][V]) const {
+	                    const Vec<T> *rc, const Vec<T> *gv, double (&part)[ND][V]) const {
 		stg(u + o, uc);
 		stg(wdst + o, wv);
 		if (zero) {
@@ -811,7 +823,7 @@ struct OpApply : OpBase<T> {
 	__device__ int q_map(int) const { return 0; }
 	__device__ Vec<T> src(const Vec<T> *raw) const { return raw[0]; }
 	__device__ void out(long long o, long long, int, const Vec<T> &, const Vec<T> &yv, const Vec<T> *, const Vec<T> *,
-	                    double (&)[1][V]) const {
+	                    const Vec<T> *, double (&)[1][V]) const {
 		stg(y + o, yv);
 		if (y2) {
 			Vec<T> t;
@@ -836,7 +848,7 @@ struct OpApply : OpBase<T> {
 // ---------------------------------------------------------------------------
 template <class T>
 struct OpBicg1 : OpBase<T> {
-	static constexpr int NS = 3, NQ = 0, ND = 1;
+	static constexpr int NS = 3, NQ = 0, ND = 1, NG = 1;
 	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
 	static constexpr int V = Vec<T>::V;
 	T iMc;
@@ -863,6 +875,7 @@ struct OpBicg1 : OpBase<T> {
 		}
 	}
 	__device__ bool raw_center() const { return true; }
+	__device__ void gload(long long o, Vec<T> *gv) const { gv[0] = ldg_rw(rhat + o); }
 	__device__ int src_map(int s) const {
 		if (s == 0) return (it & 1) ? MT_R_HALO : MT_R1_HALO;
 		if (s == 1) return (it & 1) ? MT_P0_HALO : MT_P1_HALO;
@@ -884,10 +897,10 @@ struct OpBicg1 : OpBase<T> {
 		return o;
 	}
 	__device__ void out(long long o, long long, int, const Vec<T> &, const Vec<T> &vv, const Vec<T> *, const Vec<T> *rc,
-	                    double (&part)[ND][V]) const {
+	                    const Vec<T> *gv, double (&part)[ND][V]) const {
 		stg(pn + o, pval(rc));
 		stg(vn + o, vv);
-		const Vec<T> rh = ldg_rw(rhat + o);
+		const Vec<T> &rh = gv[0];  // r_hat
 #pragma unroll
 		for (int e = 0; e < V; e++) dacc(part[0][e], vv.v[e], rh.v[e]);
 	}
@@ -940,7 +953,7 @@ struct OpBicg2 : OpBicgS<T> {
 	__device__ bool raw_center() const { return true; }
 	__device__ int q_map(int) const { return 0; }
 	__device__ void out(long long, long long, int, const Vec<T> &, const Vec<T> &tv, const Vec<T> *, const Vec<T> *rc,
-	                    double (&part)[ND][V]) const {
+	                    const Vec<T> *gv, double (&part)[ND][V]) const {
 		const Vec<T> sv = this->sval(rc);
 #pragma unroll
 		for (int e = 0; e < V; e++) {
@@ -966,7 +979,7 @@ struct OpBicg2 : OpBicgS<T> {
 template <class T>
 struct OpBicg3 : OpBicgS<T> {
 	static constexpr int KIND = 1;
-	static constexpr int NS = 2, NQ = 0, ND = 2;
+	static constexpr int NS = 2, NQ = 0, ND = 2, NG = 3;
 	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
 	static constexpr int V = Vec<T>::V;
 	T *x, *r0, *r1, *p0, *p1, *rhat;
@@ -988,12 +1001,17 @@ struct OpBicg3 : OpBicgS<T> {
 		}
 	}
 	__device__ bool raw_center() const { return true; }
+	__device__ void gload(long long o, Vec<T> *gv) const {
+		gv[0] = ldg_rw(x + o);
+		gv[1] = ldg_rw(pc + o);
+		gv[2] = ldg_rw(rhat + o);
+	}
 	__device__ int q_map(int) const { return 0; }
 	__device__ void out(long long o, long long, int, const Vec<T> &shv, const Vec<T> &tv, const Vec<T> *, const Vec<T> *rc,
-	                    double (&part)[ND][V]) const {
+	                    const Vec<T> *gv, double (&part)[ND][V]) const {
 		const Vec<T> sv = this->sval(rc);
-		Vec<T> xv = ldg_rw(x + o);
-		const Vec<T> pv = ldg_rw(pc + o), rh = ldg_rw(rhat + o);
+		Vec<T> xv = gv[0];
+		const Vec<T> &pv = gv[1], &rh = gv[2];
 		Vec<T> rv;
 #pragma unroll
 		for (int e = 0; e < V; e++) {
