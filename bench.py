@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["sedi", "reference"], default="sedi")
-    ap.add_argument("--form", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--form", choices=["mixed", "fp64", "plain"], default="mixed",
+                    help="mixed / fp64: batched forms; plain: the single-vector FP64 form (profiling cases)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # Small cases for profiler captures (not the benchmark configuration):
     ap.add_argument("--grid", default=None, help="override the grid, e.g. 128x128x64")
@@ -66,8 +67,8 @@ def parse():
                     help="dropin: the benchmark line; batched256 / large512: the 256^3 x 128-probe and the "
                          "512^3 x 16-probe configurations, one line each")
     a = ap.parse_args()
-    if a.solver != "cg" and not a.no_extras:
-        ap.error("--solver pcg/bicgstab is for profiling cases (with --no-extras)")
+    if (a.solver != "cg" or a.form == "plain") and not a.no_extras:
+        ap.error("--solver pcg/bicgstab and --form plain are for profiling cases (with --no-extras)")
     global GRID, MAXITER, TOL
     if a.grid:
         GRID = tuple(int(v) for v in a.grid.split("x"))
@@ -427,7 +428,7 @@ def run_sedi(args):
     tuned = None
     if not args.no_autotune and not args.no_extras:
         tuned = S.autotune(args.solver, GRID, SAMPLES, precision=prec, maxiter=MAXITER, tol=TOL, seed=seed0)
-    ctx = S.Context(args.solver, GRID, precision=prec, batch=SAMPLES)
+    ctx = S.Context(args.solver, GRID, precision=prec, batch=1 if args.form == "plain" else SAMPLES)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream)
 
