@@ -443,6 +443,13 @@ struct OpResid : OpBase<double> {
 		if (ru) {
 			if (ls.done[lane]) return;
 			if (!pcg && !gl->ru_all && !ls.pending[lane]) return;  // not part of this update
+			// The FP32 recurrence's <r,r> before the replacement: when it sits
+			// far below the true one (squared norms 1e-6 apart: the recurrence
+			// converged in FP32 arithmetic, as small systems do exactly), its
+			// search directions no longer describe the residual and the lane
+			// restarts from the replaced residual.
+			const double rr_rec = pcg ? ls.rr_top[lane] : ls.rr[lane];
+			const bool lost = !(rr_rec >= 1e-6 * tot[1]);
 			const double err = sqrt(tot[1] / ls.bb[lane]);
 			ls.err[lane] = err;
 			ls.rr[lane] = tot[1];
@@ -462,7 +469,12 @@ struct OpResid : OpBase<double> {
 				if (ls.s_exit[lane] != 2) ls.s_exit[lane] = 0;
 			} else if (!pcg) {
 				ls.ru_new[lane] = tot[0];  // continue from the replaced residual
-				ls.beta[lane] = tot[0] / ls.ru[lane];
+				double be = tot[0] / ls.ru[lane];
+				if (lost || ls.s_exit[lane] == 2 || !(be >= 0.0 && isfinite(be))) be = 0.0;  // restart: p = u
+				ls.beta[lane] = be;
+				ls.s_exit[lane] = 0;
+			} else {
+				ls.s_exit[lane] = (lost || ls.s_exit[lane] == 2) ? 2 : 0;  // pipelined CG restarts in its next sweep
 			}
 			return;
 		}
@@ -519,7 +531,7 @@ struct OpCgA : OpBase<T> {
 	T iMc;
 	T *p0, *p1;
 	T *pout;  // p buffer written this iteration
-	int it;
+	int it, mixed;
 	bool first;
 	T beta[V];
 	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
@@ -555,7 +567,7 @@ struct OpCgA : OpBase<T> {
 			for (int e = 0; e < V; e++) dacc(part[1][e], rc[0].v[e], amul(rc[0].v[e], iMc));
 		}
 	}
-	__device__ void fin(int lane, const double *tot, Global *, const LaneState &ls) const {
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
 		if (ls.done[lane]) {
 			ls.alpha[lane] = 0.0;
 			return;
@@ -563,7 +575,18 @@ struct OpCgA : OpBase<T> {
 		ls.sp[lane] = tot[0];
 		const double ru = first ? tot[1] : ls.ru_new[lane];
 		ls.ru[lane] = ru;
-		ls.alpha[lane] = __ddiv_rn(ru, tot[0]);
+		const double al = __ddiv_rn(ru, tot[0]);
+		if (mixed && !(tot[0] > 0.0 && isfinite(al))) {
+			// FP32 breakdown (p = 0 once the recurrence residual is exactly
+			// zero, or overflow): no step now; a reliable update replaces r
+			// and the lane restarts from p = u (s_exit = 2 marks the restart).
+			ls.alpha[lane] = 0.0;
+			ls.pending[lane] = 1;
+			ls.s_exit[lane] = 2;
+			gl->ru_due = 1;
+			return;
+		}
+		ls.alpha[lane] = al;
 	}
 };
 
@@ -615,7 +638,8 @@ struct OpCgB : OpBase<T> {
 		const int maxiter = gl->maxiter;
 		if (mixed) {
 			// The FP32 recurrence only proposes; the FP64 true residual decides.
-			if (err <= tol || it >= maxiter) {
+			if (!(err == err)) ls.s_exit[lane] = 2;  // NaN recurrence: restart after the update
+			if (err <= tol || it >= maxiter || !(err == err)) {
 				ls.pending[lane] = 1;
 				gl->ru_due = 1;
 			}
@@ -652,6 +676,8 @@ struct OpPcg : OpBase<T> {
 	T *wn;
 	int it, mixed;
 	T alpha[V], beta[V];
+	bool fresh[V];  // iteration 1, or a lane restarted after an FP32 breakdown (mixed)
+	bool hold[V];   // non-finite step (FP32 breakdown): the lane's fields stay as they are
 	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
 		it = gl->iter;
 		wn = (it & 1) ? w1 : w0;
@@ -660,7 +686,8 @@ struct OpPcg : OpBase<T> {
 			const int l = lane + e;
 			const double g = ls.gamma[l], d = ls.delta[l];
 			double al, be;
-			if (it > 1) {  // :175-178
+			fresh[e] = it == 1 || ls.s_exit[l] == 2;
+			if (!fresh[e]) {  // :175-178
 				be = __ddiv_rn(g, ls.gamma_old[l]);
 				al = __ddiv_rn(1.0, __dsub_rn(__ddiv_rn(d, g), __ddiv_rn(be, ls.alpha[l])));
 			} else {       // :179-181
@@ -668,6 +695,8 @@ struct OpPcg : OpBase<T> {
 				al = __ddiv_rn(g, d);
 			}
 			if (ls.done[l]) al = be = 0.0;  // finished lanes stay frozen
+			hold[e] = mixed && !(isfinite(al) && isfinite(be));
+			if (hold[e]) al = be = 0.0;
 			alpha[e] = (T)al;
 			beta[e] = (T)be;
 		}
@@ -688,10 +717,21 @@ struct OpPcg : OpBase<T> {
 		Vec<T> rv = ldg_rw(r + o), xv = ldg_rw(x + o), uv = ldg_rw(u + o), wnv;
 #pragma unroll
 		for (int e = 0; e < V; e++) {
-			qv.v[e] = aadd(mc.v[e], amul(beta[e], qv.v[e]));       // :200
-			sv.v[e] = aadd(wv.v[e], amul(beta[e], sv.v[e]));       // :203
-			pv.v[e] = aadd(uv.v[e], amul(beta[e], pv.v[e]));       // :206
-			zv.v[e] = aadd(nc.v[e], amul(beta[e], zv.v[e]));       // :209
+			if (hold[e]) {
+				wnv.v[e] = wv.v[e];
+				continue;
+			}
+			if (fresh[e]) {  // beta = 0, without multiplying stale values
+				qv.v[e] = mc.v[e];
+				sv.v[e] = wv.v[e];
+				pv.v[e] = uv.v[e];
+				zv.v[e] = nc.v[e];
+			} else {
+				qv.v[e] = aadd(mc.v[e], amul(beta[e], qv.v[e]));       // :200
+				sv.v[e] = aadd(wv.v[e], amul(beta[e], sv.v[e]));       // :203
+				pv.v[e] = aadd(uv.v[e], amul(beta[e], pv.v[e]));       // :206
+				zv.v[e] = aadd(nc.v[e], amul(beta[e], zv.v[e]));       // :209
+			}
 			rv.v[e] = aadd(rv.v[e], amul(-alpha[e], sv.v[e]));     // :212
 			xv.v[e] = aadd(xv.v[e], amul(alpha[e], pv.v[e]));      // :215
 			uv.v[e] = aadd(uv.v[e], amul(-alpha[e], qv.v[e]));     // :218
@@ -716,7 +756,9 @@ struct OpPcg : OpBase<T> {
 		ls.err[lane] = err;
 		const double g = ls.gamma[lane], d = ls.delta[lane];
 		double al;
-		if (it > 1) {
+		const bool restarted = ls.s_exit[lane] == 2;
+		ls.s_exit[lane] = 0;
+		if (it > 1 && !restarted) {
 			const double be = __ddiv_rn(g, ls.gamma_old[lane]);
 			al = __ddiv_rn(1.0, __dsub_rn(__ddiv_rn(d, g), __ddiv_rn(be, ls.alpha[lane])));
 		} else {
@@ -730,7 +772,8 @@ struct OpPcg : OpBase<T> {
 		const double tol = gl->tol;
 		const int maxiter = gl->maxiter;
 		if (mixed) {
-			if (err <= tol || it >= maxiter) {
+			if (!isfinite(al) || !(err == err)) ls.s_exit[lane] = 2;  // FP32 breakdown: restart after the update
+			if (err <= tol || it >= maxiter || ls.s_exit[lane] == 2) {
 				ls.pending[lane] = 1;
 				gl->ru_due = 1;
 			}
@@ -1686,6 +1729,7 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	a.iMc = (T)(1.0 / c->k.a);
 	a.p0 = (T *)B->p0;
 	a.p1 = (T *)B->p1;
+	a.mixed = B->mixed ? 1 : 0;
 	launchT<T, RBT>(c, B, a, s);
 	OpCgB<T> bo;
 	bo.ka = (T)c->k.a;
@@ -2081,6 +2125,7 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 	a.iMc = (T)(1.0 / c->k.a);
 	a.p0 = (T *)B->p0;
 	a.p1 = (T *)B->p1;
+	a.mixed = 0;
 	OpCgB<T> bo;
 	bo.ka = (T)c->k.a;
 	bo.kb = (T)c->k.b;
