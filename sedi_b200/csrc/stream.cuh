@@ -5,7 +5,7 @@
 // contiguous, so the TMA view of a field is 3-D: (W*n1, n2, n3*slices).  A
 // block owns a P1 x P2 point tile, one lane slice and a chunk of i3 planes.
 // Plane by plane, thread 0 issues TMA tile loads (cp.async.bulk.tensor.3d,
-// no multicast) of
+// each copy lands in this block's own shared memory only) of
 //   - NS "source" fields with a one-point halo in i1 and i2 (box
 //     W*(P1+2) x (P2+2) x 1), from which the stencil input is computed, and
 //   - NQ "pointwise" fields on the tile interior (box W*P1 x P2 x 1),
