@@ -79,3 +79,41 @@ def test_solver_classes_mirror_reference_enums():
     assert sedi_b200.BiCgStab.BICGSTAB_BREAKDOWN_OMEGA == 3
     with pytest.raises(ValueError):
         sedi_b200.Cg((4, 4, 4), nghost=2)
+
+
+def test_job_bytes_is_host_arithmetic():
+    """The server's admission size needs no device: the lane-sliced fields of
+    a batched context plus its small per-lane and reduction buffers."""
+    n = 64 ** 3
+    # CG mixed, 16 lanes: x_lo, r, p0, p1 in FP32 and b, x_hi in FP64 per point and lane.
+    cg = sedi_b200.job_bytes("cg", (64, 64, 64), 16, sedi_b200.MIXED)
+    assert cg >= n * 16 * (4 * 4 + 2 * 8)
+    assert cg <= n * 16 * (4 * 4 + 2 * 8) * 1.05 + 64 * 2 ** 20
+    # Pipelined CG adds six FP32 fields, BiCGStab four; FP64 doubles the Krylov words.
+    pcg = sedi_b200.job_bytes("pcg", (64, 64, 64), 16, sedi_b200.MIXED)
+    bicg = sedi_b200.job_bytes("bicgstab", (64, 64, 64), 16, sedi_b200.MIXED)
+    assert pcg - cg >= 6 * n * 16 * 4 and bicg - cg >= 4 * n * 16 * 4
+    assert sedi_b200.job_bytes("cg", (64, 64, 64), 16, sedi_b200.FP64) > cg
+    # Monotone in lanes and grid; lanes are padded to whole lane vectors.
+    assert sedi_b200.job_bytes("cg", (64, 64, 64), 32, sedi_b200.MIXED) > cg
+    assert sedi_b200.job_bytes("cg", (96, 96, 96), 16, sedi_b200.MIXED) > cg
+    assert sedi_b200.job_bytes("cg", (64, 64, 64), 13, sedi_b200.MIXED) == cg
+    assert load_bad_job_bytes() == 0.0
+
+
+def load_bad_job_bytes():
+    lib = sedi_b200.load()
+    return lib.sedi_job_bytes(9, 0, 4, 8, 8, 8)
+
+
+def test_server_and_autotune_argument_checks_without_device():
+    lib = sedi_b200.load()
+    choice = np.zeros(4, np.int32)
+    assert lib.sedi_autotune(7, 1, 16, 8, 8, 8, 10, 1e-9, 1, 0, choice.ctypes.data_as(ctypes.c_void_p), None) == -1
+    assert lib.sedi_autotune(2, 1, 16, 0, 8, 8, 10, 1e-9, 1, 0, choice.ctypes.data_as(ctypes.c_void_p), None) == -1
+    assert lib.sedi_server_submit(None, 2, 1, 8, 8, 8, 4, 1, 10, 1e-9) == -1
+    assert lib.sedi_server_step(None, None) == -1
+    assert lib.sedi_server_take(None, 0, None, None, None, None) == -1
+    timed_out = ctypes.c_int(0)
+    assert lib.sedi_selftest_bounded_wait(0.0, ctypes.byref(timed_out), None) == -1
+    assert lib.sedi_selftest_bounded_wait(10000.0, ctypes.byref(timed_out), None) == -1
