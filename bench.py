@@ -1,23 +1,33 @@
 #!/usr/bin/env python
-"""Benchmark: CG probe-solves/s of the SEDI estimator on one B200 (or N, probe-sharded).
+"""Benchmark: CG probe-solves/s of the SEDI estimator, batched mixed precision, on one B200 (or N, probe-sharded).
 
-Workload (the drop-in configuration): 128x128x128 grid, the reference 7-point
-operator (a=6, b=c=1), CG with the constant Jacobi preconditioner 1/a, tol
-1e-9 run to convergence, 64 probes per GPU drawn exactly as the reference
-does (std::mt19937(seed) -> uniform_real(0,1) -> +-1, seeds 1234+k on rank 0,
-disjoint seed ranges on the other ranks).  One step = one full estimate of
-the 64 probes (x = 0, solve to tol, t += x.*v, q += v.*v, D = t./q).  The
-probes are synthetic in the reference's own sense; there is no dataset.
+Workload (the batched mixed-precision configuration): 256x256x256 grid, the
+reference 7-point operator (a=6, b=c=1), 128 probe right-hand sides
+interleaved in one streaming kernel per Krylov sweep, FP32 Krylov vectors with
+an FP64 reliable update of x and r, FP64 reductions and estimator
+accumulators, CG with the constant Jacobi preconditioner 1/a run to FP64
+relative residual 1e-9, iterations replayed from captured CUDA graphs.
+Probes are drawn exactly as the reference draws them (std::mt19937(seed) ->
+uniform_real(0,1) -> +-1), seeds 1234+k on rank 0 and disjoint ranges on
+the other ranks.  One step = one full estimate of the 128 probes (x = 0,
+solve to tol, t += x.*v, q += v.*v, D = t./q).  The probes are synthetic in
+the reference's own sense; there is no dataset.
 
 Arms:
-  --impl sedi (default): the batched mixed-precision form (FP32 Krylov
-      vectors, FP64 reductions and FP64 reliable update), device-resident
-      inputs for `value`; `e2e` repeats the step through the C ABI from pinned
-      host probes to the host D.  N > 1 (torchrun): each rank estimates its
-      own 64 probes and t, q are summed with one NCCL all-reduce per step.
+  --impl sedi (default): `value` = the estimate on probes resident in HBM;
+      `e2e` = the same step through the C ABI from pinned host probes to the
+      host D.  N > 1 (torchrun): each rank estimates its own 128 probes and t,
+      q are summed by sedi_b200.dist.estimate_sharded (one NCCL all-reduce per
+      step).  Extra keys: the 128^3 x 64-probe drop-in configuration for each
+      solver (plain FP64 single-vector form against the reference's own
+      output, batched FP64 and mixed forms), the serving mix, the roofline
+      of every sweep.
   --impl reference: the reference CPU build (stochastic-estimator.cg.exe,
       unmodified sources, single-rank MPI stand-in) on the host cores: one
-      step = P concurrent single-rank processes, one 128^3 probe each.
+      step = P concurrent single-rank processes, one 256^3 probe each, run for
+      a fixed number of iterations (-m M -i); the per-probe time to
+      convergence is extrapolated with the reference's own converged
+      iteration count on this grid (tests/golden/big_cg_256.npz).
 """
 import argparse
 import json
@@ -32,16 +42,25 @@ import time
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-GRID = (128, 128, 128)
-SAMPLES = 64
 SEED = 1234
-TOL = 1e-9
-MAXITER = 5000
 METRIC = "CG probe-solves/s at 1e-8 vs FP64 oracle"
 UNIT = "probe-solves/s"
-WORKLOAD = ("SEDI estimator, 128^3 7-point stencil (a=6,b=c=1), CG + Jacobi, tol 1e-9 to convergence, "
-            "64 probes per GPU (std::mt19937(seed+k) +-1), D = sum x.*v / sum v.*v")
 REF_EXE = os.path.join(REPO, "oracle", "_ref", "stochastic-estimator.cg.exe")
+BIG_FIXTURE = os.path.join(REPO, "tests", "golden", "big_cg_256.npz")
+
+# Workloads: the benchmark line (batched256) and the other single-GPU configurations.
+WORKLOADS = {
+    "batched256": dict(grid=(256, 256, 256), samples=128, tol=1e-9, maxiter=20000, solver="cg", form="mixed",
+                       text="SEDI estimator, 256^3 7-point stencil (a=6,b=c=1), CG + Jacobi to FP64 relative "
+                            "residual 1e-9, 128 probe RHS per GPU interleaved (std::mt19937(seed+k) +-1), FP32 "
+                            "Krylov vectors + FP64 reliable update, FP64 reductions and t/q, D = sum x.*v / sum v.*v"),
+    "dropin": dict(grid=(128, 128, 128), samples=64, tol=1e-9, maxiter=5000, solver="cg", form="mixed",
+                   text="SEDI estimator, 128^3 7-point stencil (a=6,b=c=1), CG + Jacobi, tol 1e-9 to convergence, "
+                        "64 probes per GPU (std::mt19937(seed+k) +-1), D = sum x.*v / sum v.*v"),
+}
+# Compulsory bytes per point, lane and iteration (x, r, p read and written once)
+# of CG: FP32 Krylov words for the mixed form, FP64 for the others.
+CG_BYTES = {"mixed": 24, "fp64": 48, "plain": 48}
 
 
 def parse():
@@ -50,32 +69,38 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["sedi", "reference"], default="sedi")
-    ap.add_argument("--form", choices=["mixed", "fp64", "plain"], default="mixed",
+    ap.add_argument("--workload", choices=["batched256", "dropin", "large512"], default="batched256",
+                    help="batched256: the benchmark line (256^3 x 128 probes, mixed CG); dropin: 128^3 x 64 "
+                         "probes; large512: the 512^3 x 16-probe pipelined-CG configuration (one JSON line)")
+    ap.add_argument("--form", choices=["mixed", "fp64", "plain"], default=None,
                     help="mixed / fp64: batched forms; plain: the single-vector FP64 form (profiling cases)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # Small cases for profiler captures (not the benchmark configuration):
     ap.add_argument("--grid", default=None, help="override the grid, e.g. 128x128x64")
+    ap.add_argument("--samples", type=int, default=None, help="override the probes per GPU")
     ap.add_argument("--maxiter", type=int, default=None, help="override maxiter (with --tol 0: fixed iterations)")
     ap.add_argument("--tol", type=float, default=None)
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, kernel timing, accuracy and other forms")
-    ap.add_argument("--solver", choices=["cg", "pcg", "bicgstab"], default="cg",
+    ap.add_argument("--solver", choices=["cg", "pcg", "bicgstab"], default=None,
                     help="solver of the timed form (profiling cases; the benchmark configuration is CG)")
-    ap.add_argument("--serve-jobs", type=int, default=12, help="jobs in the serving run (0: skip it)")
+    ap.add_argument("--serve-jobs", type=int, default=50, help="jobs in the serving run (0: skip it)")
     ap.add_argument("--serve-only", action="store_true", help="run only the serving measurement")
-    ap.add_argument("--no-autotune", action="store_true", help="skip the autotuner (built-in launch choices)")
-    ap.add_argument("--workload", choices=["dropin", "batched256", "large512"], default="dropin",
-                    help="dropin: the benchmark line; batched256 / large512: the 256^3 x 128-probe and the "
-                         "512^3 x 16-probe configurations, one line each")
+    ap.add_argument("--e2e-steps", type=int, default=3, help="steps of the end-to-end measurement")
+    ap.add_argument("--ref-iters", type=int, default=30,
+                    help="iterations each reference process runs per sample (-m M -i), then extrapolated")
     a = ap.parse_args()
-    if (a.solver != "cg" or a.form == "plain") and not a.no_extras:
+    wl = dict(WORKLOADS.get(a.workload, WORKLOADS["batched256"]))
+    profiling = a.grid or a.samples or a.maxiter is not None or a.tol is not None or a.solver or a.form == "plain"
+    if (a.solver not in (None, "cg") or a.form == "plain") and not a.no_extras:
         ap.error("--solver pcg/bicgstab and --form plain are for profiling cases (with --no-extras)")
-    global GRID, MAXITER, TOL
     if a.grid:
-        GRID = tuple(int(v) for v in a.grid.split("x"))
-    if a.maxiter is not None:
-        MAXITER = a.maxiter
-    if a.tol is not None:
-        TOL = a.tol
+        wl["grid"] = tuple(int(v) for v in a.grid.split("x"))
+    for key in ("samples", "maxiter", "tol", "solver", "form"):
+        if getattr(a, key) is not None:
+            wl[key] = getattr(a, key)
+    if profiling:
+        wl["text"] = "profiling case (not the benchmark configuration)"
+    a.wl = wl
     return a
 
 
@@ -84,6 +109,13 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return rank, world, local
+
+
+def _peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
 
 
 # ---------------------------------------------------------------------------
@@ -138,38 +170,137 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # CPU reference (the reference's own binary), P concurrent single-rank processes.
 # ---------------------------------------------------------------------------
-def reference_sample(procs, seed0, grid=GRID):
-    """One bounded sample: `procs` single-rank reference processes, one probe each.
-    Returns (probe-solves/s, wall seconds, kind, iteration counts)."""
+TIMER_KEYS = ("TIMER_GLOBAL", "TIMER_COMPUTE_STENCIL_INNER", "TIMER_COMPUTE_STENCIL_BORDER", "TIMER_COMPUTE_DOTPROD",
+              "TIMER_COMPUTE_RNG", "TIMER_COMPUTE_MISC", "TIMER_HALO_PACK", "TIMER_HALO_ISEND_IRECV",
+              "TIMER_HALO_UNPACK_WAIT", "TIMER_COMM_DOTPROD")
+
+
+def parse_reference_output(text):
+    """The reference's report (stochastic-estimator.cc:218-222, Timers.hpp:57-70):
+    iteration min/max and its ten timer buckets in seconds."""
+    out = {"timers": {}}
+    for line in text.splitlines():
+        if line.startswith("Total solve time"):
+            out["seconds"] = float(line.split(":", 1)[1].split()[0])
+            out["iter_min"] = int(line.split("min=", 1)[1].split()[0])
+            out["iter_max"] = int(line.rsplit("max=", 1)[1])
+        for k in TIMER_KEYS:
+            if line.startswith(k + " "):
+                out["timers"][k] = float(line.split("=", 1)[1].split()[0])
+    return out
+
+
+def reference_fixed_sample(procs, seed0, grid, iters, tol):
+    """One bounded sample: `procs` concurrent single-rank reference processes,
+    one probe each (seeds seed0 ..), `iters` iterations (-m iters -i).
+    Returns (list of parsed reports, wall seconds, kind)."""
     g = "x".join(map(str, grid))
-    jobs = []
     t0 = time.perf_counter()
     if os.path.exists(REF_EXE):
-        kind = "reference"
+        jobs = []
         for j in range(procs):
             env = dict(os.environ, SEDI_SEED=str(seed0 + j), OMP_NUM_THREADS="1")
-            jobs.append(subprocess.Popen([REF_EXE, "-g", g, "-p", "1x1x1", "-s", "1", "-e", repr(TOL), "-m",
-                                          str(MAXITER)], env=env, stdout=subprocess.PIPE,
+            jobs.append(subprocess.Popen([REF_EXE, "-g", g, "-p", "1x1x1", "-s", "1", "-e", repr(tol), "-m",
+                                          str(iters), "-i"], env=env, stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True))
-        iters = []
+        reps = []
         for p in jobs:
             out, _ = p.communicate()
             if p.returncode != 0:
                 raise RuntimeError("reference process failed")
-            for line in out.splitlines():
-                if line.startswith("Total solve time"):
-                    iters.append(int(line.rsplit("max=", 1)[1]))
-    else:
-        kind = "port"
-        code = ("import sys; sys.path.insert(0, %r); import _oracle as O; "
-                "r = O.estimate(2, %r, 1, int(sys.argv[1]), %d, %r); print(int(r['iters'][0]))"
-                % (os.path.join(REPO, "tests"), tuple(grid), MAXITER, TOL))
-        for j in range(procs):
-            jobs.append(subprocess.Popen([sys.executable, "-c", code, str(seed0 + j)], stdout=subprocess.PIPE,
-                                         text=True))
-        iters = [int(p.communicate()[0].strip()) for p in jobs]
-    wall = time.perf_counter() - t0
-    return procs / wall, wall, kind, iters
+            reps.append(parse_reference_output(out))
+        return reps, time.perf_counter() - t0, "reference"
+    # Without the reference binary: the oracle's restatement (one process per core).
+    code = ("import sys, time; sys.path.insert(0, %r); import _oracle as O; t = time.perf_counter(); "
+            "r = O.estimate(2, %r, 1, int(sys.argv[1]), %d, %r); "
+            "print('Total solve time: %%e seconds, iteration count min=%%d max=%%d' %% "
+            "(time.perf_counter() - t, r['iters'][0], r['iters'][0]))"
+            % (os.path.join(REPO, "tests"), tuple(grid), iters, tol))
+    jobs = [subprocess.Popen([sys.executable, "-c", code, str(seed0 + j)], stdout=subprocess.PIPE, text=True)
+            for j in range(procs)]
+    reps = [parse_reference_output(p.communicate()[0]) for p in jobs]
+    return reps, time.perf_counter() - t0, "port"
+
+
+def converged_iterations(grid, tol):
+    """The reference's own mean converged CG iteration count on `grid` at tol
+    (committed fixture made by the reference binary), or None."""
+    import numpy as np
+    if tuple(grid) == (256, 256, 256) and tol == 1e-9 and os.path.exists(BIG_FIXTURE):
+        return float(np.load(BIG_FIXTURE)["iters"].mean()), "reference run of 8 probes (tests/golden/big_cg_256.npz)"
+    if tuple(grid) == (128, 128, 128) and tol == 1e-9:
+        path = os.path.join(REPO, "tests", "golden", "full_cg_128.npz")
+        if os.path.exists(path):
+            return float(np.load(path)["iters"].mean()), "reference run of 64 probes (tests/golden/full_cg_128.npz)"
+    return None, None
+
+
+def extrapolate(reps, iters, n_conv):
+    """Per-probe time to convergence from a fixed-iteration sample: the RNG fill
+    once, the rest (setup residual + iterations + accumulation) scaled by
+    n_conv / iters (the setup share is counted as iterations: conservative)."""
+    per = []
+    for r in reps:
+        rng = r["timers"].get("TIMER_COMPUTE_RNG", 0.0)
+        per.append(rng + (r["seconds"] - rng) * n_conv / iters)
+    return per
+
+
+def reference_baseline(procs, seed0, grid, iters, tol, points):
+    """probe-solves/s of the reference on `procs` host cores (extrapolated to
+    convergence), with its timer breakdown, GPoint-it/s and effective GB/s."""
+    reps, wall, kind = reference_fixed_sample(procs, seed0, grid, iters, tol)
+    n_conv, src = converged_iterations(grid, tol)
+    if n_conv is None:
+        n_conv, src = float(iters), "no converged count known: rate at the fixed iteration count"
+    per = extrapolate(reps, iters, n_conv)
+    value = procs / statistics.mean(per)
+    timers = {k: statistics.mean(r["timers"].get(k, 0.0) for r in reps) for k in TIMER_KEYS} if reps[0]["timers"] \
+        else None
+    it_s = sum(r["iter_max"] for r in reps) / sum(r["seconds"] for r in reps)  # iterations per second per process
+    return {
+        "value": value, "kind": kind, "wall_s": wall, "per_probe_s": statistics.mean(per),
+        "converged_iterations": n_conv, "converged_source": src, "sample_iterations": iters,
+        "timers_s_per_process": timers,
+        "gpoint_iterations_per_s": procs * it_s * points / 1e9,
+        "effective_gbs": procs * it_s * points * CG_BYTES["fp64"] / 1e9,
+    }
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    wl = args.wl
+    grid, tol = wl["grid"], wl["tol"]
+    points = grid[0] * grid[1] * grid[2]
+    procs = host_cores()
+    for w in range(args.warmup):
+        reference_fixed_sample(procs, SEED, grid, 2, tol)  # untimed: page-in, allocation, RNG
+    vals, walls, last = [], [], None
+    for k in range(args.steps):
+        last = reference_baseline(procs, SEED + k * procs, grid, args.ref_iters, tol, points)
+        vals.append(last["value"])
+        walls.append(last["wall_s"])
+    value = statistics.mean(vals)
+    sample = (f"{procs} concurrent single-rank processes (-p 1x1x1) x 1 probe x {args.ref_iters} iterations "
+              f"(-m {args.ref_iters} -i) per step on {'x'.join(map(str, grid))}, extrapolated per probe to "
+              f"{last['converged_iterations']:.1f} iterations ({last['converged_source']}); {args.steps} steps")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl["text"], "grid": list(grid), "probes_per_step": procs, "solver": "cg", "tol": tol,
+                   "parallelism": f"{procs} processes x -p 1x1x1"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": last["kind"], "sample": sample,
+                         "extrapolated": True},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timers_s_per_process": last["timers_s_per_process"],
+        "gpoint_iterations_per_s": last["gpoint_iterations_per_s"],
+        "effective_gbs": last["effective_gbs"],
+        "effective_gbs_basis": "48 B per point per iteration (FP64 CG: x, r, p read and written)",
+    }
+    print(json.dumps(line), flush=True)
 
 
 def host_cores():
@@ -177,35 +308,6 @@ def host_cores():
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
-
-
-def run_reference(args):
-    rank, world, _ = dist_env()
-    if rank != 0:
-        return
-    procs = host_cores()
-    for w in range(args.warmup):
-        reference_sample(procs, SEED, grid=(32, 32, 32))  # untimed warm-up on the small grid
-    vals, walls, kind, iters = [], [], None, []
-    for k in range(args.steps):
-        v, wall, kind, it = reference_sample(procs, SEED + k * procs)
-        vals.append(v)
-        walls.append(wall)
-        iters += it
-    value = sum(procs for _ in vals) / sum(walls)
-    sample = (f"{procs} concurrent single-rank processes x 1 probe each per step (128^3 CG tol 1e-9, "
-              f"-p 1x1x1), {args.steps} steps")
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(walls) / len(walls),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": list(GRID), "probes_per_step": procs, "solver": "cg", "tol": TOL,
-                   "parallelism": f"{procs} processes x -p 1x1x1"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "iterations": [min(iters), max(iters)] if iters else None,
-    }
-    print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -231,10 +333,19 @@ def serve_jobs(njobs, seed=SEED):
     }
 
 
+def _latency_stats(lat):
+    import numpy as np
+    if len(lat) == 0:
+        return None
+    return {"jobs": int(len(lat)), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+            "p99_ms": 1e3 * float(np.percentile(lat, 99)), "max_ms": 1e3 * float(lat.max())}
+
+
 def run_serving(S, njobs, maxiter=5000):
     """Capacity from a closed-loop run (every job queued at t = 0), then an
     open-loop run with Poisson arrivals (seeded) at 80% of that capacity.
-    Latency = scheduled arrival to D on the host."""
+    Latency = scheduled arrival to D on the host; p50/p99 overall, per
+    precision, per solver and per grid edge, and the served GPoint-iterations/s."""
     import numpy as np
     jobs = serve_jobs(njobs)
     args = (jobs["solver"], jobs["precision"], jobs["edge"], jobs["samples"], jobs["seed"], jobs["tol"], maxiter)
@@ -244,19 +355,25 @@ def run_serving(S, njobs, maxiter=5000):
         rate = 0.8 * cap
         arrival = np.cumsum(np.random.default_rng(SEED + 1).exponential(1.0 / rate, njobs))
         arrival -= arrival[0]
-        lat, rcs, mk = srv.replay(arrival, *args)
+        lat, rcs, mk, its = srv.replay(arrival, *args, iterations=True)
         st = srv.stats()
     probes = int(np.sum(jobs["samples"]))
+    pts = jobs["edge"].astype(np.float64) ** 3
+    gpit = float(np.sum(pts * its)) / mk / 1e9
+    prec_name = np.where(jobs["precision"] == 0, "fp64", "mixed")
     return {
         "jobs": njobs, "capacity_jobs_per_s": cap, "arrival_rate_jobs_per_s": rate,
-        "jobs_per_s": njobs / mk, "probe_solves_per_s": probes / mk,
+        "jobs_per_s": njobs / mk, "probe_solves_per_s": probes / mk, "gpoint_iterations_per_s": gpit,
         "p50_latency_ms": 1e3 * float(np.percentile(lat, 50)), "p99_latency_ms": 1e3 * float(np.percentile(lat, 99)),
         "mean_latency_ms": 1e3 * float(lat.mean()), "closed_loop_p50_ms": 1e3 * float(np.percentile(lat0, 50)),
+        "by_precision": {p: _latency_stats(lat[prec_name == p]) for p in ("fp64", "mixed")},
+        "by_solver": {s: _latency_stats(lat[jobs["solver"] == s]) for s in ("cg", "pcg", "bicgstab")},
+        "by_edge": {str(e): _latency_stats(lat[jobs["edge"] == e]) for e in SERVE_EDGES},
         "result_codes_nonzero": int(np.count_nonzero(rcs)) + int(np.count_nonzero(rc0)),
         "nonzero_jobs": [{"solver": str(jobs["solver"][k]), "edge": int(jobs["edge"][k]),
-                          "precision": "fp64" if int(jobs["precision"][k]) == 0 else "mixed",
-                          "tol": float(jobs["tol"][k]), "samples": int(jobs["samples"][k]),
-                          "rc_open_loop": int(rcs[k]), "rc_closed_loop": int(rc0[k])}
+                          "precision": str(prec_name[k]), "tol": float(jobs["tol"][k]),
+                          "samples": int(jobs["samples"][k]), "rc_open_loop": int(rcs[k]),
+                          "rc_closed_loop": int(rc0[k])}
                          for k in range(njobs) if rcs[k] != 0 or rc0[k] != 0],
         "peak_device_gb": st["peak_bytes"] / 1e9, "budget_gb": st["budget_bytes"] / 1e9,
         "contexts_created": st["ctx_created"], "contexts_reused": st["ctx_reused"], "max_running": st["max_running"],
@@ -266,72 +383,64 @@ def run_serving(S, njobs, maxiter=5000):
 
 
 # ---------------------------------------------------------------------------
-# Large single-GPU configurations (one JSON line each, not the benchmark line).
+# Extra single-GPU measurements.
 # ---------------------------------------------------------------------------
-def _peak():
-    path = os.path.join(REPO, "MEASURED_PEAKS.json")
-    return (json.load(open(path))["hbm_gbs"], "measured") if os.path.exists(path) else (6650.0, "fallback")
-
-
 def _kernel_table(ctx, peak):
     return [{"kernel": k, "ms": ms, "bytes": by, "GB/s": by / ms / 1e6, "frac": by / ms / 1e6 / peak}
             for k, ms, by in ctx.time_kernels(reps=10)]
 
 
-def run_batched256(S, args):
-    """256^3 grid, 128 probes interleaved (mixed precision, FP32 vectors with FP64
-    reliable update at the autotuned period), CG and pipelined CG to 1e-9.  D
-    error against the batched FP64 form on the same probes (which follows the
-    single-vector FP64 method lane by lane), rate of the single-vector FP64 form
-    on 4 of the probes."""
+def _relmax(a, b):
+    import numpy as np
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def dropin_forms(S, stream):
+    """The 128^3 x 64-probe drop-in configuration for each solver, tol 1e-9 to
+    convergence: the plain FP64 single-vector form (the reference's method
+    kernel by kernel) with its D against the reference's own 64-probe output
+    (strided sample, tests/golden/full_<solver>_128.npz), the batched FP64
+    form and the mixed form (its D against the batched FP64 form)."""
     import numpy as np
     import torch
-    grid, samples, tol, maxiter = (256, 256, 256), 128, 1e-9, 20000
-    peak, psrc = _peak()
-    out = {"workload": "256^3 x 128 probes, FP32 + FP64 reliable update, tol 1e-9", "peak_gbs": peak,
-           "peak_source": psrc, "solvers": {}}
-    for solver in ("cg", "pcg"):
-        tune = S.autotune(solver, grid, samples, precision=S.MIXED, maxiter=maxiter, tol=tol, seed=SEED)
-        with S.Context(solver, grid, precision=S.MIXED, batch=samples) as c:
-            cfg = c.config()
-            for _ in range(max(args.warmup - 2, 1)):
-                c.estimate(samples, SEED, maxiter, tol)
-            torch.cuda.synchronize()
-            clocks = Clocks(0)
-            clocks.start()
-            t0 = time.perf_counter()
-            for _ in range(args.steps):
-                r = c.estimate(samples, SEED, maxiter, tol)
-            dt = (time.perf_counter() - t0) / args.steps
-            clk = clocks.stop()
-            kern = _kernel_table(c, peak)
-        Dm = r["D"]
-        # FP64 form on the same probes, in two halves of 64 (pipelined CG in
-        # FP64 for 128 probes would need 189 GB); t and q add up exactly.
-        half = samples // 2
-        with S.Context(solver, grid, precision=S.FP64, batch=half) as c64:
-            t0 = time.perf_counter()
-            ra = c64.estimate(half, SEED, maxiter, tol)
-            rb = c64.estimate(half, SEED + half, maxiter, tol)
-            dt64 = time.perf_counter() - t0
-        r64 = {"D": (ra["t"] + rb["t"]) / (ra["q"] + rb["q"])}
-        with S.Context(solver, grid) as cp:
-            cp.estimate(1, SEED, maxiter, tol)
-            t0 = time.perf_counter()
-            cp.estimate(4, SEED, maxiter, tol)
-            plain = 4 / (time.perf_counter() - t0)
-        n = grid[0] * grid[1] * grid[2]
-        out["solvers"][solver] = {
-            "probe_solves_per_s": samples / dt, "ms_per_estimate": 1e3 * dt,
-            "gpoint_iterations_per_s": float(np.sum(r["iters"])) * n / dt / 1e9,
-            "iterations": [int(r["iters"].min()), int(r["iters"].max())],
-            "results_nonzero": int(np.count_nonzero(r["results"])),
-            "D_rel_err_vs_fp64": float(np.abs(Dm - r64["D"]).max() / np.abs(r64["D"]).max()),
-            "batched_fp64_probe_solves_per_s": samples / dt64,
-            "plain_fp64_probe_solves_per_s": plain, "speedup_vs_plain_fp64": samples / dt / plain,
-            "autotuned": tune, "config": cfg, "kernels": kern, "clocks": clk,
-        }
-    print(json.dumps(out), flush=True)
+    grid, samples, tol, maxiter = (128, 128, 128), 64, 1e-9, 5000
+    n = grid[0] * grid[1] * grid[2]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    probes = torch.empty((samples, n), dtype=torch.float64, device=dev)
+    S.fill_probes_dev(SEED, probes, stream)
+    D = torch.empty(n, dtype=torch.float64, device=dev)
+    out = {}
+    for solver in ("cg", "pcg", "bicgstab"):
+        row = {}
+        fix = os.path.join(REPO, "tests", "golden", f"full_{solver}_128.npz")
+        z = np.load(fix) if os.path.exists(fix) else None
+        stride = int(eval(str(z["meta"]))["sample_stride"]) if z is not None else None
+        for form, prec, batch in (("plain_fp64", S.FP64, 1), ("batched_fp64", S.FP64, samples),
+                                  ("mixed", S.MIXED, samples)):
+            with S.Context(solver, grid, precision=prec, batch=batch) as c:
+                c.set_stream(stream)
+                c.estimate_dev(min(4, samples) if batch == 1 else samples, probes, D, maxiter=maxiter, tol=tol)
+                torch.cuda.synchronize()
+                a = time.perf_counter()
+                r = c.estimate_dev(samples, probes, D, maxiter=maxiter, tol=tol)
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - a
+            Dh = D.cpu().numpy()
+            ent = {"probe_solves_per_s": samples / dt, "iterations": [int(r["iters"].min()), int(r["iters"].max())],
+                   "results_nonzero": int(np.count_nonzero(r["results"]))}
+            if z is not None:
+                ent["D_rel_err_vs_reference_sample"] = _relmax(Dh[::stride], z["D_sample"])
+                ent["iters_equal_reference"] = bool(np.array_equal(r["iters"], z["iters"]))
+            row[form] = ent
+            row["_D_" + form] = Dh
+        row["mixed"]["D_rel_err_vs_batched_fp64"] = _relmax(row.pop("_D_mixed"), row["_D_batched_fp64"])
+        row.pop("_D_batched_fp64")
+        row.pop("_D_plain_fp64")
+        row["mixed_vs_plain_fp64"] = row["mixed"]["probe_solves_per_s"] / row["plain_fp64"]["probe_solves_per_s"]
+        out[solver] = row
+    del probes
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_large512(S, args):
@@ -363,7 +472,7 @@ def run_large512(S, args):
            "probe_solves_per_s": samples / dt, "ms_per_estimate": 1e3 * dt,
            "gpoint_iterations_per_s": float(np.sum(r["iters"])) * n / dt / 1e9,
            "iterations": [int(r["iters"].min()), int(r["iters"].max())], "results": sorted(set(map(int, r["results"]))),
-           "D_rel_err_vs_plain_fp64": float(np.abs(r["D"] - rp["D"]).max() / np.abs(rp["D"]).max()),
+           "D_rel_err_vs_plain_fp64": _relmax(r["D"], rp["D"]),
            "final_err_mixed": [float(r["errs"].min()), float(r["errs"].max())],
            "final_err_fp64": [float(rp["errs"].min()), float(rp["errs"].max())],
            "plain_fp64_probe_solves_per_s": samples / dtp, "speedup_vs_plain_fp64": dtp / dt,
@@ -371,35 +480,40 @@ def run_large512(S, args):
     print(json.dumps(out), flush=True)
 
 
-# ---------------------------------------------------------------------------
-# The sedi_b200 arm.
-# ---------------------------------------------------------------------------
-def traffic_per_launch(kernel):
-    """DRAM bytes per launch of `kernel` at the bench size, from the committed
-    ncu summary (profiles/ncu_traffic.txt: '<kernel> <bytes per launch>')."""
+def traffic_per_launch(kernel, grid, lanes):
+    """DRAM bytes per launch of `kernel` at this size, from the committed ncu
+    summary (profiles/ncu_traffic.txt lines '<kernel> <n1>x<n2>x<n3> <lanes>
+    <bytes per launch>'), scaled by point-lanes (traffic is proportional to
+    the grid and the lanes)."""
     path = os.path.join(REPO, "profiles", "ncu_traffic.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
         f = line.split()
-        if len(f) >= 2 and f[0] == kernel:
+        if len(f) >= 4 and f[0] == kernel and not line.startswith("#"):
             try:
-                return float(f[1])
+                g = [int(v) for v in f[1].split("x")]
+                return float(f[3]) * (grid[0] * grid[1] * grid[2] * lanes) / (g[0] * g[1] * g[2] * int(f[2]))
             except ValueError:
                 return None
     return None
 
 
+# ---------------------------------------------------------------------------
+# The sedi_b200 arm.
+# ---------------------------------------------------------------------------
 def run_sedi(args):
     import numpy as np
     import torch
     import torch.distributed as dist
     import sedi_b200 as S
+    from sedi_b200 import dist as sdist
 
     rank, world, local = dist_env()
-    if args.workload != "dropin":
+    wl = args.wl
+    if args.workload == "large512":
         if rank == 0:
-            (run_batched256 if args.workload == "batched256" else run_large512)(S, args)
+            run_large512(S, args)
         return
     if args.serve_only:
         if rank == 0:
@@ -408,37 +522,39 @@ def run_sedi(args):
     if world > 1:
         from datetime import timedelta
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    GRID, SAMPLES, TOL, MAXITER = wl["grid"], wl["samples"], wl["tol"], wl["maxiter"]
+    solver, form = wl["solver"], wl["form"]
     dev = torch.device("cuda", torch.cuda.current_device())
     n = GRID[0] * GRID[1] * GRID[2]
-    seed0 = SEED + rank * SAMPLES
+    stream = torch.cuda.current_stream()
+    prec = S.MIXED if form == "mixed" else S.FP64
+    batch = 1 if form == "plain" else SAMPLES
+    peak, peak_src = _peak()
 
-    # Probes: generated once on the host with the reference's generator, pinned.
-    host = torch.empty((SAMPLES, n), dtype=torch.float64).pin_memory()
-    hv = host.numpy()
-    for k in range(SAMPLES):
-        hv[k] = S.fill_probe(seed0 + k, n)
-    probes = host.to(dev)
+    # This rank's probes (seeds SEED + rank*SAMPLES + k), generated on the
+    # device with the reference's generator: resident for `value`, copied
+    # once to pinned host memory for `e2e`.
+    probes = torch.empty((SAMPLES, n), dtype=torch.float64, device=dev)
+    S.fill_probes_dev(SEED + rank * SAMPLES, probes, stream)
     D = torch.empty(n, dtype=torch.float64, device=dev)
     t = torch.empty(n, dtype=torch.float64, device=dev)
     q = torch.empty(n, dtype=torch.float64, device=dev)
-    prec = S.MIXED if args.form == "mixed" else S.FP64
-    # Launch choices for this shape, measured before the timed region
-    # (slice width, i3 split, graph chunk, reliable-update period).
+    # Launch choices for this shape, measured before the timed region (lane
+    # slice width and i3 split from the sweeps' own timing).
     tuned = None
-    if not args.no_autotune and not args.no_extras:
-        tuned = S.autotune(args.solver, GRID, SAMPLES, precision=prec, maxiter=MAXITER, tol=TOL, seed=seed0)
-    ctx = S.Context(args.solver, GRID, precision=prec, batch=1 if args.form == "plain" else SAMPLES)
-    stream = torch.cuda.current_stream()
+    if form != "plain" and not args.no_extras:
+        tuned = S.autotune(solver, GRID, SAMPLES, precision=prec, maxiter=MAXITER, tol=TOL, solve=False)
+    ctx = S.Context(solver, GRID, precision=prec, batch=batch)
     ctx.set_stream(stream)
 
+    def local_dev(solver_, dims, count, first_seed, maxiter, tol, precision, batch_, stencil):
+        r = ctx.estimate_dev(count, probes, D, t, q, maxiter=maxiter, tol=tol)
+        return dict(r, t=t, q=q)
+
     def step():
-        r = ctx.estimate_dev(SAMPLES, probes, D, t, q, maxiter=MAXITER, tol=TOL)
-        if world > 1:
-            dist.all_reduce(t)
-            dist.all_reduce(q)
-            torch.div(t, q, out=D)
-        return r
+        return sdist.estimate_sharded(solver, GRID, SAMPLES * world, seed=SEED, maxiter=MAXITER, tol=TOL,
+                                      precision=prec, batch=batch, device=dev, local_estimate=local_dev)
 
     def barrier():
         if world > 1:
@@ -472,11 +588,12 @@ def run_sedi(args):
     it_all = np.concatenate(iters)
     if TOL > 0:
         assert np.all(res["results"] == 0), "a probe did not converge"
+    Dcur = res["D"].cpu().numpy() if rank == 0 else None
     if args.no_extras:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                              "ms_per_step": ms / args.steps, "grid": list(GRID), "maxiter": MAXITER, "tol": TOL,
-                              "solver": args.solver,
+                              "ms_per_step": ms / args.steps, "grid": list(GRID), "samples": SAMPLES,
+                              "maxiter": MAXITER, "tol": TOL, "solver": solver, "form": form,
                               "gpu_launches": launches, "note": "profiling case, not the benchmark configuration"}),
                   flush=True)
         ctx.close()
@@ -485,108 +602,137 @@ def run_sedi(args):
         return
 
     # End to end through the C ABI: pinned host probes in, host D out, per step.
-    Dh = np.empty(n)
+    host = torch.empty((SAMPLES, n), dtype=torch.float64).pin_memory()
+    host.copy_(probes)
+    hv = host.numpy()
+
+    def local_host(solver_, dims, count, first_seed, maxiter, tol, precision, batch_, stencil):
+        return ctx.estimate(count, probes=hv, maxiter=maxiter, tol=tol)
+
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
     barrier()
     w0 = time.perf_counter()
-    for _ in range(args.steps):
-        rr = ctx.estimate(SAMPLES, probes=hv, maxiter=MAXITER, tol=TOL)
-        if world > 1:
-            tt = torch.from_numpy(rr["t"]).to(dev)
-            qq = torch.from_numpy(rr["q"]).to(dev)
-            dist.all_reduce(tt)
-            dist.all_reduce(qq)
-            Dh[:] = (tt / qq).cpu().numpy()
-        else:
-            Dh[:] = rr["D"]
+    for _ in range(e2e_steps):
+        rr = sdist.estimate_sharded(solver, GRID, SAMPLES * world, seed=SEED, maxiter=MAXITER, tol=TOL,
+                                    precision=prec, batch=batch, device=dev, local_estimate=local_host)
+        Dh = rr["D"].cpu().numpy()
     barrier()
     e2e_s = torch.tensor([time.perf_counter() - w0], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
-    e2e_val = world * SAMPLES * args.steps / float(e2e_s.item())
+    e2e_val = world * SAMPLES * e2e_steps / float(e2e_s.item())
+    del host, hv
 
     out = None
     if rank == 0:
-        # Roofline of the dominant per-iteration kernel (timed alone, CUDA events on this stream).
-        kern = ctx.time_kernels(reps=20)
-        dom = max(kern, key=lambda k: k[1])
-        peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
-        if os.path.exists(peaks_path):
-            peak = json.load(open(peaks_path))["hbm_gbs"]
-            peak_src = "measured"
-        else:
-            peak, peak_src = 6650.0, "fallback"
-        ach = dom[2] / (dom[1] * 1e-3) / 1e9
-        roofline = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": peak, "unit": "GB/s",
-                    "frac": ach / peak, "peak_source": peak_src, "traffic": traffic_per_launch(dom[0]),
-                    "bytes_per_launch": dom[2], "ms_per_launch": dom[1],
-                    "kernels": [{"kernel": k[0], "ms": k[1], "bytes": k[2], "GB/s": k[2] / k[1] / 1e6,
-                                 "frac": k[2] / k[1] / 1e6 / peak} for k in kern]}
-        # Accuracy of this form's D against the reference's own 64-probe run
-        # (strided sample of D) and against the FP64 GPU form on the same probes.
+        # Roofline of the dominant per-iteration sweep (each sweep timed alone,
+        # CUDA events on the launching stream), and of the whole iteration
+        # against the compulsory bytes of CG (x, r, p read and written).
+        kern = ctx.time_kernels(reps=10) if form != "plain" else []
+        ctx_config = ctx.config() if form != "plain" else None
+        theta = ctx.mixed_target if form == "mixed" else None
+        roofline = None
+        if kern:
+            dom = max(kern, key=lambda k: k[1])
+            ach = dom[2] / (dom[1] * 1e-3) / 1e9
+            it_ms = sum(k[1] for k in kern)
+            it_bytes = CG_BYTES[form] * n * SAMPLES
+            roofline = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": peak, "unit": "GB/s",
+                        "frac": ach / peak, "peak_source": peak_src,
+                        "traffic": traffic_per_launch(dom[0], GRID, SAMPLES),
+                        "bytes_per_launch": dom[2], "ms_per_launch": dom[1],
+                        "kernels": [{"kernel": k[0], "ms": k[1], "bytes": k[2], "GB/s": k[2] / k[1] / 1e6,
+                                     "frac": k[2] / k[1] / 1e6 / peak} for k in kern],
+                        "iteration": {"ms": it_ms, "compulsory_bytes": it_bytes,
+                                      "basis": f"{CG_BYTES[form]} B per point-lane (x, r, p read and written)",
+                                      "GB/s": it_bytes / it_ms / 1e6, "frac": it_bytes / it_ms / 1e6 / peak}}
+        ctx.close()
         acc = {}
-        Dcur = D.cpu().numpy()
-        fix = os.path.join(REPO, "tests", "golden", "full_cg_128.npz")
-        if world == 1 and os.path.exists(fix):
-            z = np.load(fix)
-            samp = z["D_sample"]
-            stride = int(eval(str(z["meta"]))["sample_stride"])
-            acc["D_rel_err_vs_reference_sample"] = float(np.abs(Dcur[::stride] - samp).max() / np.abs(samp).max())
-            acc["iters_equal_reference"] = bool(np.array_equal(iters[-1], z["iters"]))
         forms = {}
-        with S.Context("cg", GRID, precision=S.FP64, batch=SAMPLES) as c64:
-            c64.set_stream(stream)
-            D64 = torch.empty_like(D)
-            c64.estimate_dev(SAMPLES, probes, D64, maxiter=MAXITER, tol=TOL)
-            torch.cuda.synchronize()
-            a = time.perf_counter()
-            c64.estimate_dev(SAMPLES, probes, D64, maxiter=MAXITER, tol=TOL)
-            torch.cuda.synchronize()
-            forms["batched_fp64"] = SAMPLES / (time.perf_counter() - a)
-            d64 = D64.cpu().numpy()
-            acc["D_rel_err_vs_gpu_fp64"] = float(np.abs(Dcur - d64).max() / np.abs(d64).max())
-        with S.Context("cg", GRID) as cp:
-            cp.set_stream(stream)
-            Dp = torch.empty_like(D)
-            k8 = 8
-            cp.estimate_dev(1, probes, Dp, maxiter=MAXITER, tol=TOL)
-            torch.cuda.synchronize()
-            a = time.perf_counter()
-            cp.estimate_dev(k8, probes, Dp, maxiter=MAXITER, tol=TOL)
-            torch.cuda.synchronize()
-            forms["plain_fp64_single_vector"] = k8 / (time.perf_counter() - a)
+        if world == 1 and form == "mixed":
+            # The FP64 batched form on the same probes (two halves of the lanes:
+            # t and q add up exactly), and the plain single-vector FP64 form.
+            half = SAMPLES // 2
+            with S.Context(solver, GRID, precision=S.FP64, batch=half) as c64:
+                c64.set_stream(stream)
+                t64 = torch.zeros(n, dtype=torch.float64, device=dev)
+                q64 = torch.zeros(n, dtype=torch.float64, device=dev)
+                D64 = torch.empty(n, dtype=torch.float64, device=dev)
+                torch.cuda.synchronize()
+                a = time.perf_counter()
+                for h in range(2):
+                    c64.estimate_dev(half, probes[h * half:(h + 1) * half], D64, t, q, maxiter=MAXITER, tol=TOL)
+                    t64 += t
+                    q64 += q
+                torch.cuda.synchronize()
+                forms["batched_fp64"] = SAMPLES / (time.perf_counter() - a)
+            d64 = (t64 / q64).cpu().numpy()
+            acc["D_rel_err_vs_batched_fp64"] = _relmax(Dcur, d64)
+            acc["tolerance"] = 1e-8
+            acc["mixed_target_theta"] = theta
+            del t64, q64, D64
+            with S.Context(solver, GRID) as cp:
+                cp.set_stream(stream)
+                kp = 2
+                cp.estimate_dev(1, probes, D, maxiter=MAXITER, tol=TOL)
+                torch.cuda.synchronize()
+                a = time.perf_counter()
+                rp = cp.estimate_dev(kp, probes, D, maxiter=MAXITER, tol=TOL)
+                torch.cuda.synchronize()
+                forms["plain_fp64_single_vector"] = kp / (time.perf_counter() - a)
+                forms["plain_fp64_iterations"] = [int(v) for v in rp["iters"]]
+            forms["mixed_vs_plain_fp64"] = value / forms["plain_fp64_single_vector"]
+            forms["mixed_vs_batched_fp64"] = value / forms["batched_fp64"]
+            # The reference's own converged run of probes 0..7 on this grid.
+            if tuple(GRID) == (256, 256, 256) and os.path.exists(BIG_FIXTURE):
+                z = np.load(BIG_FIXTURE)
+                kz = len(z["iters"])
+                acc["iters_probes_0_7_mixed"] = [int(v) for v in iters[-1][:kz]]
+                acc["iters_probes_0_7_reference"] = [int(v) for v in z["iters"]]
+                acc["iters_probes_0_7_plain_fp64_first2_equal_reference"] = bool(
+                    np.array_equal(rp["iters"], z["iters"][:kp]))
+        del probes
+        torch.cuda.empty_cache()
+        dropin = dropin_forms(S, stream) if world == 1 and tuple(GRID) == (256, 256, 256) else None
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             procs = host_cores()
-            v, wall, kind, it = reference_sample(procs, SEED)
-            cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": kind,
-                   "sample": f"{procs} concurrent single-rank processes x 1 probe (128^3 CG tol 1e-9), {wall:.1f} s"}
+            rb = reference_baseline(procs, SEED, GRID, args.ref_iters, TOL, n)
+            cpu = {"value": rb["value"], "unit": UNIT, "cores": procs, "kind": rb["kind"], "extrapolated": True,
+                   "sample": f"{procs} concurrent single-rank processes x 1 probe x {args.ref_iters} iterations "
+                             f"({'x'.join(map(str, GRID))} CG, -p 1x1x1, {rb['wall_s']:.1f} s), extrapolated per "
+                             f"probe to {rb['converged_iterations']:.1f} iterations ({rb['converged_source']})",
+                   "gpoint_iterations_per_s": rb["gpoint_iterations_per_s"], "effective_gbs": rb["effective_gbs"],
+                   "timers_s_per_process": rb["timers_s_per_process"]}
         serving = run_serving(S, args.serve_jobs) if world == 1 and args.serve_jobs > 0 else None
-        ctx_config = ctx.config()
-        gpoint = float(np.sum(it_all)) * n / args.steps / (ms / 1e3 / args.steps) / 1e9 if world == 1 else None
+        gpoint = float(np.sum(it_all)) * n / (ms / 1e3) / 1e9 * world
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 vectors / f64 reductions+reliable update" if prec == S.MIXED else "f64",
+            "dtype": "f32 vectors / f64 reductions+reliable update" if form == "mixed" else "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": list(GRID), "probes_per_gpu": SAMPLES, "solver": "cg",
-                       "tol": TOL, "form": args.form, "parallelism": f"probe-sharded x{world}",
+            "config": {"workload": wl["text"], "grid": list(GRID), "probes_per_gpu": SAMPLES, "solver": solver,
+                       "tol": TOL, "form": form, "parallelism": f"probe-sharded x{world}",
                        "autotuned": tuned, "launch": ctx_config,
-                       "l2": "inputs larger than L2 (1.07 GB probes + >=1.6 GB Krylov state per GPU)"},
+                       "l2": f"inputs larger than L2 ({SAMPLES * n * 8 / 1e9:.1f} GB probes + Krylov state per GPU)"},
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": SAMPLES * n * 8,
-                    "d2h_bytes_per_step": n * 8 * (3 if world > 1 else 1) + SAMPLES * 16},
+            "e2e": {"value": e2e_val, "unit": UNIT, "steps": e2e_steps, "h2d_bytes_per_step": SAMPLES * n * 8,
+                    "d2h_bytes_per_step": n * 8 * 3 + SAMPLES * 16},
             "clocks": clk,
             "gpu_launches": launches,
             "iterations": [int(it_all.min()), int(it_all.max())],
             "gpoint_iterations_per_s": gpoint,
             "accuracy": acc,
             "forms": forms,
+            "dropin_128": dropin,
             "serving": serving,
         }
+    else:
+        ctx.close()
+    if rank == 0:
         print(json.dumps(out), flush=True)
-    ctx.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

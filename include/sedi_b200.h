@@ -47,6 +47,9 @@ extern "C" {
 /* Arithmetic forms. */
 #define SEDI_PREC_FP64 0  /* the reference method in FP64, kernel by kernel */
 #define SEDI_PREC_MIXED 1 /* FP32 Krylov vectors, FP64 reductions, FP64 reliable update of x and r */
+/* As SEDI_PREC_MIXED with r and p stored in FP16 (per-lane power-of-two
+ * scales, FP32 arithmetic, FP32 x correction); CG only. */
+#define SEDI_PREC_MIXED16 2
 
 /* Reference result_t values. */
 #define SEDI_SOLUTION_FOUND 0
@@ -75,7 +78,8 @@ typedef struct sedi_ctx sedi_ctx;
  *   n1,n2,n3   grid (every dimension >= 1)
  *   a,b,c      stencil coefficients: y = a*x_c - c*(x_{i-1}+...) - b*(x_{i+1}+...)
  *   mode       SEDI_MODE_* bits (accepted, no effect on one GPU)
- *   precision  SEDI_PREC_FP64 or SEDI_PREC_MIXED
+ *   precision  SEDI_PREC_FP64, SEDI_PREC_MIXED or SEDI_PREC_MIXED16 (CG only;
+ *              SEDI_ERR_UNSUPPORTED for the other solvers)
  *   batch      right-hand sides in flight per launch (1 = single-vector form)
  *   err        out: 0 or a negative SEDI_ERR_* (may be NULL)
  * Returns NULL on error.
@@ -154,8 +158,10 @@ int sedi_time_kernels(sedi_ctx *ctx, int reps, double *ms, double *bytes, char *
  * Computes r = b - A x with zero ghosts (x_dev, b_dev inputs, r_dev output;
  * device pointers, n1*n2*n3 doubles, i1 fastest) and *err_out (host) =
  * sqrt(<r,r>/<b,b>) with <b,b> taken as 1 when it is 0, the solvers' initial
- * residual test.  Runs on `stream` (a cudaStream_t as void*, NULL = default
- * stream) and returns after the result is on the host.
+ * residual test.  r_dev must not overlap x_dev or b_dev (SEDI_ERR_ARG).
+ * Runs on `stream` (a cudaStream_t as void*, NULL = default stream); the
+ * call synchronizes that stream and copies err into host memory before it
+ * returns.
  * Scratch: a fixed device array in the library (about 64 KiB per GPU, held
  * until the process exits) -- nothing is allocated per call.  Limit: the
  * grid's sweep may use at most 4096 thread blocks, which holds whenever
@@ -167,6 +173,43 @@ int sedi_time_kernels(sedi_ctx *ctx, int reps, double *ms, double *bytes, char *
 int sedi_residual_noalloc(long n1, long n2, long n3, double a, double b, double c, const double *x_dev,
                           const double *b_dev, double *r_dev, double *err_out, void *stream);
 
+/*
+ * Slab (i3) domain decomposition of the FP64 CG method: the kernels one rank
+ * runs on its slab (the host loop, halo exchange and collectives are in
+ * sedi_b200/domain.py).  Replaces, for a decomposition -p 1x1xP, the
+ * reference's DomainDecomposition (DomainDecomposition.hpp:51-80), the halo
+ * exchange (CommHalo.hpp:84-181) -- a halo is one contiguous ghost plane --,
+ * the inner/border stencil split (DistrAsyncStencil.hpp:52-100) and the
+ * local part of DistrAsyncDotProds (DistrAsyncDotProds.hpp:85-136).
+ * Every slab vector is [nloc + 2][n2][n1] doubles (device), i1 fastest, with
+ * ghost planes 0 and nloc+1; ghost planes on the global boundary are zero.
+ *
+ * sedi_slab_sweep: for ghosted planes z in [z_lo, z_hi) (1 <= z_lo <= z_hi
+ * <= nloc+1), with the stencil applied to src:
+ *   mode 0  r = b - A src; dots <b,b>, <r,r>                 (Cg.hpp:112-129)
+ *   mode 1  dots <A src, src> and, when first, <r, r*iM>     (Cg.hpp:152-166)
+ *   mode 2  x += alpha src; r -= alpha A src; dots <r, r*iM>, <r,r>
+ *                                                             (Cg.hpp:169-182)
+ *   mode 3  y = A src                                         (Stencil.hpp:38-54)
+ * plane_part[(z-1)*2 + d] receives plane z's dot d, summed in an order fixed
+ * by n1 and n2 only (sedi_slab_chunks() row chunks per plane, scratch
+ * chunk_part of nloc*chunks*2 doubles), so plane sums, and the solve, do not
+ * depend on how the planes are split into slabs.  Elementwise values round
+ * as the reference's.  Runs on `stream` (cudaStream_t as void*).
+ */
+int sedi_slab_sweep(int mode, long n1, long n2, long nloc, double a, double b, double c, long z_lo, long z_hi,
+                    double iM, double alpha, int first, const double *src, double *x, double *r, const double *bvec,
+                    double *y, double *chunk_part, double *plane_part, void *stream);
+/* p = u + beta p, u = r .* iM (p = u when first), over n elements (Cg.hpp:144-147, :188). */
+int sedi_slab_p(long n, const double *r, double *p, double iM, double beta, int first, void *stream);
+/* t += x .* v, q += v .* v (t = x .* v, q = v .* v when reset) over n elements
+ * (stochastic-estimator.cc:195, :198). */
+int sedi_slab_accumulate(long n, const double *x, const double *v, double *t, double *q, int reset, void *stream);
+/* D = t ./ q over n elements (stochastic-estimator.cc:216). */
+int sedi_slab_divide(long n, const double *t, const double *q, double *D, void *stream);
+/* Row chunks per plane of sedi_slab_sweep's dot products. */
+int sedi_slab_chunks(void);
+
 /* Device probe generator: probes seed, seed+1, ..., seed+nprobes-1 (each
  * DistrRngStd's +-1 vector from std::mt19937(seed + k), bit-identical to
  * sedi_fill_probe) into out_dev[k*n + i], on `stream` (cudaStream_t as void*). */
@@ -174,6 +217,11 @@ int sedi_fill_probes_dev(uint32_t seed, int nprobes, long n, double *out_dev, vo
 
 /* Host probe generator, bit-identical to DistrRngStd with std::mt19937(seed). */
 void sedi_fill_probe(uint32_t seed, long n, double *out);
+/* Points [offset, offset + count) of the probe sedi_fill_probe(seed, ...)
+ * writes (the part of the global probe one slab of a decomposed grid holds;
+ * the reference fills each rank's cells from its own generator,
+ * DistrRngStd.hpp:22-42, so its probes depend on -p -- these do not). */
+void sedi_fill_probe_range(uint32_t seed, long offset, long count, double *out);
 
 /* y = A x with zero ghosts (host buffers), the kernel the solvers use. */
 int sedi_stencil_apply(sedi_ctx *ctx, const double *x, double *y);
@@ -245,11 +293,12 @@ int sedi_server_take(sedi_server *srv, long id, double *D, int *iters, double *e
 /* Open-loop replay: job k (cubic grid edge[k]) is submitted when arrival_s[k]
  * seconds (non-decreasing) have passed since the call; the server runs until
  * all are done.  latency_s[k] = done - scheduled arrival; rcs[k] (optional)
- * its code; *makespan_s (optional) = first arrival to last completion.
+ * its code; *makespan_s (optional) = first arrival to last completion;
+ * iterations[k] (optional) = the sum of job k's per-probe iteration counts.
  * Results are discarded. */
 int sedi_server_replay(sedi_server *srv, int njobs, const double *arrival_s, const int *solver, const int *precision,
                        const long *edge, const int *samples, const uint32_t *seed, const double *tol, int maxiter,
-                       double *latency_s, int *rcs, double *makespan_s);
+                       double *latency_s, int *rcs, double *makespan_s, long long *iterations);
 
 /* Peak device bytes held, the budget, contexts created and reused, most jobs
  * running at once, kernel launches of finished jobs. */
@@ -273,6 +322,23 @@ int sedi_server_stats(const sedi_server *srv, double *peak_bytes, double *budget
  */
 int sedi_autotune(int solver, int precision, int batch, long n1, long n2, long n3, int maxiter, double tol,
                   uint32_t seed, int flags, int *choice, double *score_ms);
+
+/*
+ * In-loop stop target of the mixed-precision batched form (no counterpart in
+ * the reference, whose FP64 method needs none).  A mixed lane leaves its loop
+ * when its FP64 true residual sqrt(<b - A x, b - A x>/<b,b>) <= theta * tol,
+ * 0 < theta <= 1; result codes and final_err are still judged against tol
+ * as the reference does (Cg.hpp:191-206), and the initial test stays
+ * err < tol (Cg.hpp:130-134).  Two solutions that both meet tol differ by
+ * the error each leaves behind the residual bound, which for the FP32
+ * recurrences of pipelined CG and BiCGStab is larger than for FP64; a
+ * tighter target brings the mixed solution within the FP64 form's own
+ * truncation error of it, at the cost of the extra iterations.  The default
+ * is chosen per solver by measurement (sedi_mixed_target reads it).
+ * SEDI_ERR_UNSUPPORTED for FP64 contexts, SEDI_ERR_ARG for theta outside (0, 1].
+ */
+int sedi_set_mixed_target(sedi_ctx *ctx, double theta);
+double sedi_mixed_target(const sedi_ctx *ctx);
 
 /* Launch choices of a batched context: config[0..4] = lane-slice width, i3
  * chunks of a sweep, reliable-update period, iterations per captured graph,

@@ -27,7 +27,7 @@ import numpy as np
 
 __all__ = [
     "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "Server", "autotune", "estimate", "fill_probe",
-    "job_bytes", "library_path", "load", "SOLVER_IDS", "FP64", "MIXED",
+    "job_bytes", "library_path", "load", "SOLVER_IDS", "FP64", "MIXED", "MIXED16",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -35,7 +35,7 @@ _LIB_PATH = os.path.join(_HERE, "_lib", "libsedi_b200.so")
 
 BICGSTAB, CG, PIPELINED_CG = 1, 2, 3
 SOLVER_IDS = {"bicgstab": BICGSTAB, "cg": CG, "pcg": PIPELINED_CG, "pipelined_cg": PIPELINED_CG}
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED16 = 0, 1, 2  # MIXED16: r and p stored in FP16 (CG)
 
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "device out of memory", -4: "no CUDA device",
           -5: "unsupported"}
@@ -97,11 +97,14 @@ def load():
     lib.sedi_server_wait.argtypes = [vp, c_long]
     lib.sedi_server_job_info.argtypes = [vp, c_long, pi, pi, pd, pd, pd, pi, pd]
     lib.sedi_server_take.argtypes = [vp, c_long, vp, vp, vp, vp]
-    lib.sedi_server_replay.argtypes = [vp, c_int, vp, vp, vp, vp, vp, vp, vp, c_int, vp, vp, pd]
+    lib.sedi_server_replay.argtypes = [vp, c_int, vp, vp, vp, vp, vp, vp, vp, c_int, vp, vp, pd, vp]
     lib.sedi_server_stats.argtypes = [vp, pd, pd, pi, pi, pi, ctypes.POINTER(ctypes.c_longlong)]
     lib.sedi_autotune.argtypes = [c_int, c_int, c_int, c_long, c_long, c_long, c_int, c_double, ctypes.c_uint32,
                                   c_int, vp, pd]
     lib.sedi_ctx_config.argtypes = [vp, vp]
+    lib.sedi_set_mixed_target.argtypes = [vp, c_double]
+    lib.sedi_mixed_target.argtypes = [vp]
+    lib.sedi_mixed_target.restype = c_double
     lib.sedi_selftest_bounded_wait.argtypes = [c_double, pi, pd]
     lib.sedi_job_bytes.restype = c_double
     lib.sedi_job_bytes.argtypes = [c_int, c_int, c_int, c_long, c_long, c_long]
@@ -207,6 +210,15 @@ class Context:
         self._check(load().sedi_ctx_config(self._h, _ptr(cf)), "config")
         return {"slice_width": int(cf[0]), "z_chunks": int(cf[1]), "period": int(cf[2]), "chunk": int(cf[3]),
                 "lanes": int(cf[4])}
+
+    @property
+    def mixed_target(self):
+        """theta of the mixed form: lanes stop on FP64 true residual <= theta * tol."""
+        return float(load().sedi_mixed_target(self._h))
+
+    @mixed_target.setter
+    def mixed_target(self, theta):
+        self._check(load().sedi_set_mixed_target(self._h, float(theta)), "mixed_target")
 
     def solve(self, x, b, iM=None, maxiter=1000, tol=1e-4):
         """Returns (result_t, final_err, final_iter); x is overwritten with the solution."""
@@ -455,9 +467,10 @@ class Server:
             raise SediError(rc, "job failed")
         return {"rc": rc, "D": D, "iters": iters, "errs": errs, "results": res}
 
-    def replay(self, arrival_s, solver, precision, edge, samples, seed, tol, maxiter):
+    def replay(self, arrival_s, solver, precision, edge, samples, seed, tol, maxiter, iterations=False):
         """Open-loop schedule (arrays of one entry per job); returns
-        (latency_s, result codes, makespan_s)."""
+        (latency_s, result codes, makespan_s), and with iterations=True also
+        each job's summed per-probe iteration counts."""
         k = len(arrival_s)
         a = np.ascontiguousarray(arrival_s, np.float64)
         so = np.ascontiguousarray([SOLVER_IDS[x] if isinstance(x, str) else int(x) for x in solver], np.int32)
@@ -469,11 +482,12 @@ class Server:
         lat = np.zeros(k)
         rcs = np.zeros(k, np.int32)
         mk = ctypes.c_double(0.0)
+        its = np.zeros(k, np.int64)
         r = load().sedi_server_replay(self._h, k, _ptr(a), _ptr(so), _ptr(pr), _ptr(ed), _ptr(sa), _ptr(se), _ptr(to),
-                                      int(maxiter), _ptr(lat), _ptr(rcs), ctypes.byref(mk))
+                                      int(maxiter), _ptr(lat), _ptr(rcs), ctypes.byref(mk), _ptr(its))
         if r < 0:
             raise SediError(r, "sedi_server_replay")
-        return lat, rcs, mk.value
+        return (lat, rcs, mk.value, its) if iterations else (lat, rcs, mk.value)
 
     def stats(self):
         pk, bu = ctypes.c_double(), ctypes.c_double()

@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC",
                   "-I" + os.path.join(REPO, "include")]
 
-CU_SOURCES = ["plain.cu", "batched.cu", "rng.cu", "capi.cu", "noalloc.cu", "serve.cu", "selftest.cu"]
+CU_SOURCES = ["plain.cu", "batched.cu", "rng.cu", "capi.cu", "noalloc.cu", "serve.cu", "selftest.cu", "slab.cu"]
 
 
 def _run(cmd):

@@ -52,6 +52,7 @@ struct LaneState {
 	double *bb, *rr, *err, *ru, *ru_new, *sp, *alpha, *beta;  // CG
 	double *gamma, *gamma_old, *delta, *rr_top;                 // pipelined CG
 	double *rho, *rho_prev, *omega, *s_norm2, *ts, *tt;         // BiCGStab
+	double *r_scale, *p_scale0, *p_scale1, *pp;                 // FP16 storage: field scales, <p,p>
 	int *done, *exit_iter, *reason, *pending, *s_exit;
 };
 
@@ -65,6 +66,7 @@ struct Global {
 	int nrhs;
 	int err;        // a bounded wait timed out
 	int ru_all;     // the pending reliable update covers every lane (periodic)
+	double tol_in;  // in-loop stop target: tol (FP64 form), theta * tol (mixed lanes)
 };
 
 // Arithmetic: FP64 keeps the reference's operator-by-operator rounding (no
@@ -109,9 +111,10 @@ enum { MD_X_HALO = 0, MD_B_INT };                                     // FP64 fi
 template <class C, class Op>
 __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_constant__ Maps maps, Op op,
                                                        double *partials, unsigned *ticket, Global *gl, LaneState ls) {
-	typedef typename C::type T;
+	typedef typename C::type E;   // storage element of the streamed fields
+	typedef typename C::ctype T;  // arithmetic type
 	constexpr int V = C::V, LG = C::LG, RB = C::RB, P1 = C::P1, H1 = C::H1, HALO = C::HALO, INT = C::INT,
-	              NPS = C::NPS, KC = C::KC, KO = C::KO;
+	              NPS = C::NPS, KC = C::KC, KO = C::KO, ME = C::ME;
 	constexpr int NS = Op::NS, NQ = Op::NQ, ND = Op::ND, NGX = Op::NG > 0 ? Op::NG : 1;
 	constexpr bool IDENT = Op::IDENT;
 	typedef Layout<C, NS, NQ, ND, IDENT> Lay;
@@ -119,10 +122,10 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 	extern __shared__ __align__(128) unsigned char smem[];
 	if (gl->active == 0 || !op.enabled(gl)) return;
 
-	T *const stage0 = reinterpret_cast<T *>(smem);
-	T *const ring = reinterpret_cast<T *>(smem + Lay::OFF_RING);
+	E *const stage0 = reinterpret_cast<E *>(smem);
+	E *const ring = reinterpret_cast<E *>(smem + Lay::OFF_RING);
 	uint64_t *const bar = reinterpret_cast<uint64_t *>(smem + Lay::OFF_BAR);
-	constexpr int SE = (int)(Lay::STAGE_PAD / sizeof(T));
+	constexpr int SE = (int)(Lay::STAGE_PAD / sizeof(E));
 	constexpr int HE = (int)Lay::HALO_ELEMS, IE = (int)Lay::INT_ELEMS;
 
 	const int t = threadIdx.x, lg = t % LG, ps = t / LG;
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 	auto issue = [&](int j) {  // thread 0
 		const int p = z0 - 1 + j;
 		uint64_t *b = &bar[j % NST];
-		T *st = stage0 + (j % NST) * SE;
+		E *st = stage0 + (j % NST) * SE;
 		if (p < 0 || p >= g.n3) {
 			mbar_arrive(b);  // ghost plane: completes the phase without data
 			return;
@@ -184,9 +187,9 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 		mbar_arrive_tx(b, Lay::TX);
 #pragma unroll
 		for (int s = 0; s < NS; s++)
-			tma_load3(st + s * HE, &maps.m[op.src_map(s)], b, (i1_0 - 1) * RB, i2_0 - 1, zoff + p);
+			tma_load3(st + s * HE, &maps.m[op.src_map(s)], b, (i1_0 - 1) * ME, i2_0 - 1, zoff + p);
 #pragma unroll
-		for (int q = 0; q < NQ; q++) tma_load3(st + NS * HE + q * IE, &maps.m[op.q_map(q)], b, i1_0 * RB, i2_0, zoff + p);
+		for (int q = 0; q < NQ; q++) tma_load3(st + NS * HE + q * IE, &maps.m[op.q_map(q)], b, i1_0 * ME, i2_0, zoff + p);
 	};
 	int issued = 0;
 	if (t == 0)
@@ -222,8 +225,8 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 		// Phase 1: stencil input of plane j (transforming ops only).
 		if (!IDENT && j < np) {
 			const int p = z0 - 1 + j;
-			T *cr = ring + (j & 3) * HE;
-			const T *st = stage0 + sj * SE;
+			E *cr = ring + (j & 3) * HE;
+			const E *st = stage0 + sj * SE;
 			const bool pin = p >= 0 && p < g.n3;
 #pragma unroll
 			for (int k = 0; k < KC; k++) {
@@ -248,8 +251,8 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 			const int sm1 = sj >= 3 ? sj - 3 : sj - 3 + NST;
 			const int s0 = sj >= 2 ? sj - 2 : sj - 2 + NST;
 			const int sp1 = sj >= 1 ? sj - 1 : sj - 1 + NST;
-			const T *stz = stage0 + s0 * SE;
-			const T *cm, *c0, *cp;
+			const E *stz = stage0 + s0 * SE;
+			const E *cm, *c0, *cp;
 			bool zm = true, zp = true;  // planes m-1, m+1 inside the grid
 			if (IDENT) {
 				cm = stage0 + sm1 * SE;
@@ -438,7 +441,9 @@ struct OpResid : OpBase<double> {
 		}
 	}
 	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
-		const double tol = gl->tol;
+		// The setup keeps the reference's initial test against tol (:130-134);
+		// a reliable update stops a lane on the in-loop target.
+		const double tol = ru ? gl->tol_in : gl->tol;
 		const int maxiter = gl->maxiter;
 		if (ru) {
 			if (ls.done[lane]) return;
@@ -634,7 +639,7 @@ struct OpCgB : OpBase<T> {
 		ls.beta[lane] = __ddiv_rn(tot[0], ls.ru[lane]);           // :185
 		const double err = sqrt(__ddiv_rn(tot[1], ls.bb[lane]));  // :191
 		ls.err[lane] = err;
-		const double tol = gl->tol;
+		const double tol = gl->tol_in;
 		const int maxiter = gl->maxiter;
 		if (mixed) {
 			// The FP32 recurrence only proposes; the FP64 true residual decides.
@@ -769,7 +774,7 @@ struct OpPcg : OpBase<T> {
 		ls.gamma[lane] = tot[0];
 		ls.delta[lane] = tot[1];
 		ls.rr_top[lane] = tot[2];
-		const double tol = gl->tol;
+		const double tol = gl->tol_in;
 		const int maxiter = gl->maxiter;
 		if (mixed) {
 			if (!isfinite(al) || !(err == err)) ls.s_exit[lane] = 2;  // FP32 breakdown: restart after the update
@@ -1010,7 +1015,7 @@ struct OpBicg2 : OpBicgS<T> {
 		ls.s_norm2[lane] = tot[0];  // :192-193
 		ls.ts[lane] = tot[1];
 		ls.tt[lane] = tot[2];
-		if (tot[0] < __dmul_rn(gl->tol, gl->tol)) {
+		if (tot[0] < __dmul_rn(gl->tol_in, gl->tol_in)) {
 			ls.s_exit[lane] = 1;  // :194
 		} else {
 			ls.s_exit[lane] = 0;
@@ -1077,7 +1082,7 @@ struct OpBicg3 : OpBicgS<T> {
 	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
 		if (ls.done[lane]) return;
 		const int it = this->it;
-		const double tol = gl->tol;
+		const double tol = gl->tol_in;
 		const int maxiter = gl->maxiter;
 		if (ls.s_exit[lane]) {
 			if (mixed) {
@@ -1135,6 +1140,291 @@ struct OpBicg3 : OpBicgS<T> {
 			ls.reason[lane] = stop;
 			atomicSub(&gl->active, 1);
 		}
+	}
+};
+
+// ---------------------------------------------------------------------------
+// CG with FP16 storage of the Krylov fields r and p (mixed form, FP32
+// arithmetic, FP32 x_lo, FP64 reductions and reliable update).  A stored
+// value h of lane l means h * scale[l]; every scale is a power of two picked
+// from the lane's RMS (RMS / scale in [0.5, 1)), so scaling is exact and the
+// FP16 range (6e-5 .. 65504 at full precision) is centred on the field.  The
+// FP16 rounding of r and p (2^-11 relative) acts like the FP32 rounding of
+// the FP32 form, at a larger size; the FP64 reliable update bounds its effect
+// on the solution, and a lane still stops only on its FP64 true residual.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float pow2_scale(double rms) {
+	if (!(rms > 0.0) || !isfinite(rms)) return 1.0f;
+	int e;
+	frexp(rms, &e);  // rms = m * 2^e, m in [0.5, 1)
+	e = e < -100 ? -100 : (e > 100 ? 100 : e);
+	return ldexpf(1.0f, e);
+}
+
+// p = u + beta p_old (u = r .* iM; p = u on iteration 1), s = A p, <s,p>,
+// <p,p> (next scale of p) and <r,u> on iteration 1 (Cg.hpp:150-166, :188).
+// The stencil input p is rounded to FP16 once, in the ring: the stored p and
+// the p that s = A p is computed from are the same values.
+struct OpCgAh : OpBase<float> {
+	static constexpr int KIND = 1;
+	static constexpr int NS = 2, NQ = 0, ND = 3;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr int V = 4;
+	float iMc;
+	double iMd;
+	long long npts;
+	__half *p0, *p1;
+	__half *pout;
+	int it;
+	bool first;
+	float beta[V], sr[V], spo[V], spn[V], ispn[V];
+	// Scale of the p written this iteration: an upper bound of its RMS by
+	// the triangle inequality, from <r,r> and the previous <p,p>.
+	__device__ static float p_scale(const LaneState &ls, int l, bool first, double iMd, long long n) {
+		double est = sqrt(ls.rr[l] / (double)n) * fabs(iMd);
+		if (!first) est += fabs(ls.beta[l]) * sqrt(ls.pp[l] / (double)n);
+		return pow2_scale(est);
+	}
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+		first = (it == 1);
+		pout = (it & 1) ? p1 : p0;
+		const double *so = (it & 1) ? ls.p_scale0 : ls.p_scale1;  // p_old is the other buffer
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const int l = lane + e;
+			beta[e] = (float)ls.beta[l];
+			sr[e] = (float)ls.r_scale[l];
+			spo[e] = (float)so[l];
+			spn[e] = p_scale(ls, l, first, iMd, npts);
+			ispn[e] = 1.0f / spn[e];
+		}
+	}
+	__device__ bool raw_center() const { return first; }
+	__device__ int src_map(int s) const { return s == 0 ? MT_R_HALO : ((it & 1) ? MT_P0_HALO : MT_P1_HALO); }
+	__device__ int q_map(int) const { return 0; }
+	__device__ Vec<float> src(const Vec<float> *raw) const {
+		Vec<float> o;
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const float u = (raw[0].v[e] * sr[e]) * iMc;
+			o.v[e] = (first ? u : u + beta[e] * (raw[1].v[e] * spo[e])) * ispn[e];
+		}
+		return o;
+	}
+	__device__ void out(long long o, long long, int, const Vec<float> &pc, const Vec<float> &s, const Vec<float> *,
+	                    const Vec<float> *rc, const Vec<float> *, double (&part)[ND][V]) const {
+		stg(pout + o, pc);  // FP16 values of the ring: stored exactly
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const float pt = pc.v[e] * spn[e], st = s.v[e] * spn[e];
+			dacc(part[0][e], st, pt);
+			dacc(part[2][e], pt, pt);
+		}
+		if (first) {
+#pragma unroll
+			for (int e = 0; e < V; e++) {
+				const float r = rc[0].v[e] * sr[e];
+				dacc(part[1][e], r, r * iMc);
+			}
+		}
+	}
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		double *sn = (it & 1) ? ls.p_scale1 : ls.p_scale0;
+		sn[lane] = p_scale(ls, lane, first, iMd, npts);  // before <p,p> is replaced
+		ls.pp[lane] = tot[2];
+		if (ls.done[lane]) {
+			ls.alpha[lane] = 0.0;
+			return;
+		}
+		ls.sp[lane] = tot[0];
+		const double ru = first ? tot[1] : ls.ru_new[lane];
+		ls.ru[lane] = ru;
+		const double al = __ddiv_rn(ru, tot[0]);
+		if (!(tot[0] > 0.0 && isfinite(al))) {  // breakdown: restart after a reliable update (as OpCgA)
+			ls.alpha[lane] = 0.0;
+			ls.pending[lane] = 1;
+			ls.s_exit[lane] = 2;
+			gl->ru_due = 1;
+			return;
+		}
+		ls.alpha[lane] = al;
+	}
+};
+
+// s = A p, x += alpha p, r -= alpha s, u = r .* iM, <r,u>, <r,r>; beta,
+// err, reliable-update trigger (Cg.hpp:169-193).  p (FP16) is the stencil
+// source, r (FP16) a pointwise TMA field, x_lo (FP32) is read with plain
+// loads.  r is rewritten at the scale of the previous <r,r>.
+struct OpCgBh : OpBase<float> {
+	static constexpr int NS = 1, NQ = 1, ND = 2, NG = 1;
+	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
+	static constexpr int V = 4;
+	float iMc;
+	long long npts;
+	float *x;
+	__half *r;
+	int it;
+	float alpha[V], sp[V], sro[V], isrn[V];
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+		const double *ps = (it & 1) ? ls.p_scale1 : ls.p_scale0;  // p written by this iteration's sweep A
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const int l = lane + e;
+			alpha[e] = (float)ls.alpha[l];
+			sp[e] = (float)ps[l];
+			sro[e] = (float)ls.r_scale[l];
+			isrn[e] = 1.0f / pow2_scale(sqrt(ls.rr[l] / (double)npts));
+		}
+	}
+	__device__ int src_map(int) const { return (it & 1) ? MT_P1_HALO : MT_P0_HALO; }
+	__device__ int q_map(int) const { return MT_R_INT; }
+	__device__ bool raw_center() const { return false; }
+	__device__ Vec<float> src(const Vec<float> *raw) const { return raw[0]; }
+	__device__ void gload(long long o, Vec<float> *gv) const { gv[0] = ldg_rw(x + o); }
+	__device__ void out(long long o, long long, int, const Vec<float> &pc, const Vec<float> &s, const Vec<float> *q,
+	                    const Vec<float> *, const Vec<float> *gv, double (&part)[ND][V]) const {
+		Vec<float> xv = gv[0], rv;
+#pragma unroll
+		for (int e = 0; e < V; e++) {
+			const float pt = pc.v[e] * sp[e], st = s.v[e] * sp[e];
+			xv.v[e] = xv.v[e] + alpha[e] * pt;                      // :169
+			const float r = q[0].v[e] * sro[e] - alpha[e] * st;     // :172
+			const float u = r * iMc;                                // :175
+			dacc(part[0][e], r, u);
+			dacc(part[1][e], r, r);
+			rv.v[e] = r * isrn[e];
+		}
+		stg(x + o, xv);
+		stg(r + o, rv);
+	}
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		ls.r_scale[lane] = pow2_scale(sqrt(ls.rr[lane] / (double)npts));  // the scale r was written at
+		if (ls.done[lane]) return;
+		ls.ru_new[lane] = tot[0];
+		ls.rr[lane] = tot[1];
+		ls.beta[lane] = __ddiv_rn(tot[0], ls.ru[lane]);           // :185
+		const double err = sqrt(__ddiv_rn(tot[1], ls.bb[lane]));  // :191
+		ls.err[lane] = err;
+		if (!(err == err)) ls.s_exit[lane] = 2;
+		if (err <= gl->tol_in || it >= gl->maxiter || !(err == err)) {
+			ls.pending[lane] = 1;
+			gl->ru_due = 1;
+		}
+		if (gl->period > 0 && it % gl->period == 0) gl->ru_due = gl->ru_all = 1;
+	}
+};
+
+// r = b - A x_hi in FP64 for the FP16 CG form (setup and reliable update,
+// Cg.hpp:119-134).  Two passes: `measure` computes each lane's <r,r> and
+// sets the scale r is stored at; the second pass stores r in FP16 at that
+// scale (and x_lo = 0 at setup) and runs the stop logic of OpResid.
+struct OpResidH : OpBase<double> {
+	static constexpr int NS = 1, NQ = 1, ND = 2;
+	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
+	__half *r;
+	float *xlo;
+	double iMd;
+	long long npts;
+	int ru, measure, WT;
+	int it;
+	int keep[2];
+	float isr[2];
+	__device__ bool enabled(const Global *gl) const { return !ru || gl->ru_due; }
+	__device__ bool slice_live(const Global *gl, const LaneState &ls, int lane0, int nl) const {
+		if (!ru || gl->ru_all) return true;
+		for (int l = lane0; l < lane0 + nl; l++)
+			if (ls.pending[l]) return true;
+		return false;
+	}
+	__device__ bool raw_center() const { return false; }
+	__device__ bool in_update(const Global *gl, const LaneState &ls, int l) const {
+		return !ru || (!ls.done[l] && (gl->ru_all || ls.pending[l]));
+	}
+	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
+		it = gl->iter;
+		for (int e = 0; e < 2; e++) {
+			keep[e] = !in_update(gl, ls, lane + e);
+			isr[e] = measure ? 1.0f : 1.0f / (float)ls.r_scale[lane + e];
+		}
+	}
+	__device__ int src_map(int) const { return MD_X_HALO; }
+	__device__ int q_map(int) const { return MD_B_INT; }
+	__device__ Vec<double> src(const Vec<double> *raw) const { return raw[0]; }
+	__device__ void out(long long, long long pidx, int lane, const Vec<double> &, const Vec<double> &ax,
+	                    const Vec<double> *q, const Vec<double> *, const Vec<double> *, double (&part)[ND][2]) const {
+		const long long ot = sliced(pidx, lane, WT, npts);  // lanes lane, lane+1 share a slice of r and x_lo
+#pragma unroll
+		for (int e = 0; e < 2; e++) {
+			const double bi = q[0].v[e];
+			const double ri = aadd(bi, -ax.v[e]);  // combine2(1.0, b, -1.0, r, r)
+			if (!measure) {
+				if (!keep[e]) r[ot + e] = __float2half_rn((float)ri * isr[e]);
+				if (!ru) xlo[ot + e] = 0.0f;
+			}
+			if (ru) part[0][e] = fma(ri, ri * iMd, part[0][e]);
+			else part[0][e] = fma(bi, bi, part[0][e]);
+			part[1][e] = fma(ri, ri, part[1][e]);
+		}
+	}
+	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		if (measure) {
+			if (in_update(gl, ls, lane)) ls.r_scale[lane] = pow2_scale(sqrt(tot[1] / (double)npts));
+			return;
+		}
+		const int maxiter = gl->maxiter;
+		if (ru) {
+			if (!in_update(gl, ls, lane)) return;
+			const bool lost = !(ls.rr[lane] >= 1e-6 * tot[1]);  // see OpResid
+			const double err = sqrt(tot[1] / ls.bb[lane]);
+			ls.err[lane] = err;
+			ls.rr[lane] = tot[1];
+			ls.pending[lane] = 0;
+			if (err <= gl->tol_in) {
+				ls.done[lane] = 1;
+				ls.exit_iter[lane] = it;
+				ls.reason[lane] = STOP_CONVERGED;
+				atomicSub(&gl->active, 1);
+			} else if (it >= maxiter) {
+				ls.done[lane] = 1;
+				ls.exit_iter[lane] = maxiter + 1;
+				ls.reason[lane] = STOP_MAXITER;
+				atomicSub(&gl->active, 1);
+			} else {
+				ls.ru_new[lane] = tot[0];  // continue from the replaced residual
+				double be = tot[0] / ls.ru[lane];
+				if (lost || ls.s_exit[lane] == 2 || !(be >= 0.0 && isfinite(be))) be = 0.0;  // restart: p = u
+				ls.beta[lane] = be;
+				ls.s_exit[lane] = 0;
+			}
+			return;
+		}
+		const double bb = tot[0] == 0.0 ? 1.0 : tot[0];  // Cg.hpp:112-115
+		ls.bb[lane] = bb;
+		ls.rr[lane] = tot[1];
+		const double err = sqrt(__ddiv_rn(tot[1], bb));
+		ls.err[lane] = err;
+		ls.alpha[lane] = 0.0;
+		ls.beta[lane] = 0.0;
+		ls.s_exit[lane] = 0;
+		ls.pending[lane] = 0;
+		ls.pp[lane] = 0.0;
+		int done = 0, reason = STOP_NONE, ex = 0;
+		if (lane >= gl->nrhs) {
+			done = 1;
+		} else if (err < gl->tol) {  // :130-134
+			done = 1;
+			reason = STOP_EARLY;
+		} else if (maxiter < 1) {
+			done = 1;
+			reason = STOP_MAXITER;
+			ex = 1;
+		}
+		ls.done[lane] = done;
+		ls.reason[lane] = reason;
+		ls.exit_iter[lane] = ex;
+		if (!done) atomicAdd(&gl->active, 1);
 	}
 };
 
@@ -1307,7 +1597,17 @@ static void set_tuning(const TuneKey &k, const Tuning &t) {
 	g_tune[k] = t;
 }
 
-constexpr int kLaneDoubles = 18, kLaneInts = 5;  // LaneState arrays
+constexpr int kLaneDoubles = 22, kLaneInts = 5;  // LaneState arrays
+
+#ifndef SEDI_MIXED_THETA_CG
+#define SEDI_MIXED_THETA_CG 1.0
+#endif
+#ifndef SEDI_MIXED_THETA_PCG
+#define SEDI_MIXED_THETA_PCG 0.1
+#endif
+#ifndef SEDI_MIXED_THETA_BICGSTAB
+#define SEDI_MIXED_THETA_BICGSTAB 0.1
+#endif
 
 struct Batched;
 typedef int (*SetupFn)(Ctx *, Batched *, int nrhs, int maxiter, double tol);
@@ -1330,7 +1630,8 @@ struct EstState {
 
 struct Batched {
 	int R = 0;
-	bool mixed = false;
+	bool mixed = false;  // FP32 or FP16 Krylov fields, FP64 x_hi, reductions and reliable update
+	bool half = false;   // FP16 storage of r and p (CG), FP32 x_lo
 	size_t elems = 0;  // npts * R
 	// vectors ([point][R])
 	void *x = nullptr;     // FP64 form: x; MIXED: x_lo (FP32)
@@ -1354,6 +1655,7 @@ struct Batched {
 	double *t_acc = nullptr, *q_acc = nullptr;
 	int period = 32;
 	int chunk = 16;
+	double theta = 1.0;  // mixed lanes stop on the FP64 true residual <= theta * tol
 	cudaGraphExec_t graph = nullptr;
 	long long graph_kernels = 0;
 	// launch shapes
@@ -1423,7 +1725,8 @@ struct CfgFor {
 	typedef Cfg<T, RB, tile_p1(LG), WIDE ? 32 : tile_p2(LG), kThr, WIDE ? 4 : 0> type;
 };
 
-static int pick_R(int nrhs, bool mixed) {
+static int pick_R(int nrhs, bool mixed, bool half = false) {
+	if (half) return (nrhs + 7) / 8 * 8;  // whole 8-lane FP16 slices (16 bytes per point)
 	const int V = mixed ? 4 : 2, full = 8 * V;
 	if (nrhs <= V) return V;
 	if (nrhs <= 2 * V) return 2 * V;
@@ -1514,11 +1817,49 @@ static int launchT(Ctx *c, Batched *B, const Op &op, cudaStream_t s) {
 
 static void bind_impl(Batched *B);
 
+// Default in-loop target of the mixed form, theta * tol on the FP64 true
+// residual.  Two solutions that both meet tol can differ by more than the
+// solver's own rounding: the FP32 recurrence takes a different path and
+// leaves a different error behind the same residual bound.  A tighter
+// target puts the mixed solution nearer the exact one, so its distance to
+// the FP64 form's solution is the FP64 form's own truncation error.
+static double default_theta(int solver) {
+	switch (solver) {
+	case 2: return SEDI_MIXED_THETA_CG;
+	case 3: return SEDI_MIXED_THETA_PCG;
+	default: return SEDI_MIXED_THETA_BICGSTAB;
+	}
+}
+
+int batched_set_theta(Ctx *c, double theta) {
+	Batched *B = (Batched *)c->batched;
+	if (!B || !B->mixed) {
+		c->error = "the in-loop target applies to the mixed-precision batched form";
+		return SEDI_ERR_UNSUPPORTED;
+	}
+	if (!(theta > 0.0 && theta <= 1.0)) {
+		c->error = "theta must be in (0, 1]";
+		return SEDI_ERR_ARG;
+	}
+	B->theta = theta;
+	return 0;
+}
+
+double batched_theta(const Ctx *c) {
+	const Batched *B = (const Batched *)c->batched;
+	return B && B->mixed ? B->theta : 1.0;
+}
+
 int batched_alloc(Ctx *c) {
 	Batched *B = new (std::nothrow) Batched();
 	if (!B) return SEDI_ERR_NOMEM;
 	c->batched = B;
-	B->mixed = c->precision == SEDI_PREC_MIXED;
+	B->half = c->precision == SEDI_PREC_MIXED16;
+	B->mixed = c->precision == SEDI_PREC_MIXED || B->half;
+	if (B->half && c->solver != SEDI_CG) {
+		c->error = "FP16 Krylov storage is implemented for CG";
+		return SEDI_ERR_UNSUPPORTED;
+	}
 	if (c->batch > (B->mixed ? 256 : 128)) {
 		c->error = "batch too large for one context (max 256 FP32 / 128 FP64 right-hand sides)";
 		return SEDI_ERR_ARG;
@@ -1527,25 +1868,27 @@ int batched_alloc(Ctx *c) {
 		c->error = "cuTensorMapEncodeTiled unavailable";
 		return SEDI_ERR_NODEV;
 	}
-	B->R = pick_R(c->batch, B->mixed);
+	B->R = pick_R(c->batch, B->mixed, B->half);
 	B->elems = (size_t)c->g.n * B->R;
-	const int ebT = B->mixed ? 4 : 8;
+	const int ebT = B->half ? 2 : (B->mixed ? 4 : 8);
 	const Tuning tu = tuning_for(TuneKey{c->solver, c->precision, B->R, c->g.n1, c->g.n2, c->g.n3});
-	B->rbT = slice_for(B->R, !B->mixed);
-	if (tu.W > 0 && tu.W <= B->R && B->R % tu.W == 0) B->rbT = tu.W;
+	B->rbT = B->half ? 8 : slice_for(B->R, !B->mixed);
+	if (!B->half && tu.W > 0 && tu.W <= B->R && B->R % tu.W == 0) B->rbT = tu.W;
 	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
 	B->tuned = tu;
 	if (tu.period > 0) B->period = tu.period;
+	B->theta = default_theta(c->solver);
 	if (tu.chunk > 0) B->chunk = tu.chunk;
 	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz);
 	shape(c->g, B->R, B->rbT, ebT, &B->gT1, &B->gridT1, tu.nz, 1);
 	shape(c->g, B->R, B->rbD, 8, &B->gD, &B->gridD, tu.nz);
-	const size_t ts = B->mixed ? sizeof(float) : sizeof(double);
+	const size_t ts = (size_t)ebT;                                  // Krylov field element
+	const size_t xs = B->mixed ? sizeof(float) : sizeof(double);   // x (FP64 form) or x_lo (mixed)
 	const size_t nblkT = (size_t)B->gridT.x * B->gridT.z, nblkD = (size_t)B->gridD.x * B->gridD.z;
 	const size_t nblkT1 = (size_t)B->gridT1.x * B->gridT1.z;
 	size_t nblk = nblkT > nblkD ? nblkT : nblkD;
 	if (nblkT1 > nblk) nblk = nblkT1;
-	if (cudaMalloc(&B->x, B->elems * ts) != cudaSuccess || cudaMalloc(&B->r, B->elems * ts) != cudaSuccess ||
+	if (cudaMalloc(&B->x, B->elems * xs) != cudaSuccess || cudaMalloc(&B->r, B->elems * ts) != cudaSuccess ||
 	    cudaMalloc(&B->p0, B->elems * ts) != cudaSuccess || cudaMalloc(&B->p1, B->elems * ts) != cudaSuccess ||
 	    cudaMalloc(&B->b, B->elems * sizeof(double)) != cudaSuccess ||
 	    (B->mixed && cudaMalloc(&B->xh, B->elems * sizeof(double)) != cudaSuccess) ||
@@ -1555,7 +1898,7 @@ int batched_alloc(Ctx *c) {
 	    cudaMallocHost(&B->lane_host, sizeof(double) * kLaneDoubles * B->R) != cudaSuccess ||
 	    cudaMallocHost(&B->lane_host_int, sizeof(int) * kLaneInts * B->R) != cudaSuccess ||
 	    cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming) != cudaSuccess ||
-	    cudaMalloc(&B->lane_mem, sizeof(double) * 20 * B->R) != cudaSuccess ||
+	    cudaMalloc(&B->lane_mem, sizeof(double) * kLaneDoubles * B->R) != cudaSuccess ||
 	    cudaMalloc(&B->lane_int, sizeof(int) * 5 * B->R) != cudaSuccess ||
 	    cudaMalloc(&B->t_acc, sizeof(double) * c->g.n) != cudaSuccess ||
 	    cudaMalloc(&B->q_acc, sizeof(double) * c->g.n) != cudaSuccess) {
@@ -1580,17 +1923,18 @@ int batched_alloc(Ctx *c) {
 	// Zero-fills on the context's stream (its own, non-blocking one at this
 	// point): legacy-stream memsets would not be ordered before its kernels.
 	cudaMemsetAsync(B->ticket, 0, sizeof(unsigned), c->stream);
-	cudaMemsetAsync(B->x, 0, B->elems * ts, c->stream);
+	cudaMemsetAsync(B->x, 0, B->elems * xs, c->stream);
 	cudaMemsetAsync(B->r, 0, B->elems * ts, c->stream);
 	cudaMemsetAsync(B->p0, 0, B->elems * ts, c->stream);
 	cudaMemsetAsync(B->p1, 0, B->elems * ts, c->stream);
-	cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * 20 * B->R, c->stream);
+	cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * kLaneDoubles * B->R, c->stream);
 	cudaMemsetAsync(B->lane_int, 0, sizeof(int) * kLaneInts * B->R, c->stream);
 	const int R = B->R;
 	LaneState &ls = B->ls;
 	double **dp[] = {&ls.bb, &ls.rr, &ls.err, &ls.ru, &ls.ru_new, &ls.sp, &ls.alpha, &ls.beta, &ls.gamma,
 	                 &ls.gamma_old, &ls.delta, &ls.rr_top, &ls.rho, &ls.rho_prev, &ls.omega, &ls.s_norm2, &ls.ts,
-	                 &ls.tt};
+	                 &ls.tt, &ls.r_scale, &ls.p_scale0, &ls.p_scale1, &ls.pp};
+	static_assert(sizeof(dp) / sizeof(dp[0]) == kLaneDoubles, "lane arrays");
 	for (size_t i = 0; i < sizeof(dp) / sizeof(dp[0]); i++) *dp[i] = B->lane_mem + i * R;
 	int **ip[] = {&ls.done, &ls.exit_iter, &ls.reason, &ls.pending, &ls.s_exit};
 	for (size_t i = 0; i < 5; i++) *ip[i] = B->lane_int + i * R;
@@ -1599,6 +1943,15 @@ int batched_alloc(Ctx *c) {
 	auto t_maps = [&](Maps &M, int kind) {
 		int Q1, Q2;
 		tile_for(B->rbT, ebT, &Q1, &Q2, kind);
+		if (B->half) {
+			// FP16 fields as 32-bit pairs of lanes (the same 16 bytes per point
+			// as the FP32 4-lane slices); x_lo is read with plain loads.
+			const int Rp = R / 2, Wp = B->rbT / 2;
+			return make_map(&M.m[MT_R_HALO], B->r, 4, c->g, Rp, Wp, Q1 + 2, Q2 + 2) &&
+			       make_map(&M.m[MT_P0_HALO], B->p0, 4, c->g, Rp, Wp, Q1 + 2, Q2 + 2) &&
+			       make_map(&M.m[MT_P1_HALO], B->p1, 4, c->g, Rp, Wp, Q1 + 2, Q2 + 2) &&
+			       make_map(&M.m[MT_R_INT], B->r, 4, c->g, Rp, Wp, Q1, Q2);
+		}
 		bool k = make_map(&M.m[MT_R_HALO], B->r, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_P0_HALO], B->p0, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_P1_HALO], B->p1, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
@@ -1633,17 +1986,18 @@ int batched_alloc(Ctx *c) {
 // Device bytes batched_alloc takes for a context (each allocation rounded
 // up to the 2 MiB granularity of large device allocations).
 size_t batched_bytes(int solver, int precision, int batch, long long n1, long long n2, long long n3) {
-	const bool mixed = precision == SEDI_PREC_MIXED;
+	const bool half = precision == SEDI_PREC_MIXED16;
+	const bool mixed = precision == SEDI_PREC_MIXED || half;
 	Geo g;
 	g.n1 = (int)n1;
 	g.n2 = (int)n2;
 	g.n3 = (int)n3;
 	g.n = n1 * n2 * n3;
-	const int R = pick_R(batch, mixed);
-	const size_t elems = (size_t)g.n * R, ts = mixed ? 4 : 8;
+	const int R = pick_R(batch, mixed, half);
+	const size_t elems = (size_t)g.n * R, ts = half ? 2 : (mixed ? 4 : 8), xs = mixed ? 4 : 8;
 	const Tuning tu = tuning_for(TuneKey{solver, precision, R, n1, n2, n3});
-	int wT = slice_for(R, !mixed);
-	if (tu.W > 0 && tu.W <= R && R % tu.W == 0) wT = tu.W;
+	int wT = half ? 8 : slice_for(R, !mixed);
+	if (!half && tu.W > 0 && tu.W <= R && R % tu.W == 0) wT = tu.W;
 	SGeo sT, sD;
 	dim3 gT, gD;
 	shape(g, R, wT, (int)ts, &sT, &gT, tu.nz);
@@ -1655,9 +2009,9 @@ size_t batched_bytes(int solver, int precision, int batch, long long n1, long lo
 	size_t nblk = nblkT > nblkD ? nblkT : nblkD;
 	if (nblkT1 > nblk) nblk = nblkT1;
 	auto up = [](size_t b) { return (b + (2u << 20) - 1) / (2u << 20) * (2u << 20); };
-	const int nT = 4 + (solver == 3 ? 6 : 0) + (solver == 1 ? 4 : 0);
-	size_t total = nT * up(elems * ts) + up(elems * 8) * (mixed ? 2 : 1);
-	total += up(sizeof(double) * nblk * kMaxDots * R) + 3 * up(1) + up(sizeof(double) * 20 * R) +
+	const int nT = 3 + (solver == 3 ? 6 : 0) + (solver == 1 ? 4 : 0);  // r, p0, p1 and the solver's own
+	size_t total = nT * up(elems * ts) + up(elems * xs) + up(elems * 8) * (mixed ? 2 : 1);
+	total += up(sizeof(double) * nblk * kMaxDots * R) + 3 * up(1) + up(sizeof(double) * kLaneDoubles * R) +
 	         up(sizeof(int) * 5 * R) + 2 * up(sizeof(double) * g.n);
 	return total;
 }
@@ -1888,6 +2242,7 @@ struct Impl {
 		g0.iter = 1;
 		g0.maxiter = maxiter;
 		g0.tol = tol;
+		g0.tol_in = B->mixed ? B->theta * tol : tol;
 		g0.period = B->period;
 		g0.nrhs = nrhs;
 		g0.active = 1;
@@ -1928,7 +2283,110 @@ struct Impl {
 	}
 };
 
+// FP16 storage form of CG: the residual sweep runs twice (scale of r, then
+// the stores), so setup and every reliable update know r's scale before r
+// is written.
+template <int RBD>
+static void enqueue_resid_h(Ctx *c, Batched *B, bool ru) {
+	typedef typename CfgFor<double, RBD>::type CD;
+	OpResidH op;
+	op.ka = c->k.a;
+	op.kb = c->k.b;
+	op.kc = c->k.c;
+	op.r = (__half *)B->r;
+	op.xlo = (float *)B->x;
+	op.iMd = 1.0 / c->k.a;
+	op.npts = c->g.n;
+	op.ru = ru ? 1 : 0;
+	op.WT = B->rbT;
+	op.measure = 1;
+	launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, c->stream);
+	op.measure = 0;
+	launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, c->stream);
+}
+
+template <int RBD>
+static void enqueue_cgh_iteration(Ctx *c, Batched *B) {
+	cudaStream_t s = c->stream;
+	OpCgAh a;
+	a.ka = (float)c->k.a;
+	a.kb = (float)c->k.b;
+	a.kc = (float)c->k.c;
+	a.iMc = (float)(1.0 / c->k.a);
+	a.iMd = 1.0 / c->k.a;
+	a.npts = c->g.n;
+	a.p0 = (__half *)B->p0;
+	a.p1 = (__half *)B->p1;
+	launchT<__half, 8>(c, B, a, s);
+	OpCgBh bo;
+	bo.ka = (float)c->k.a;
+	bo.kb = (float)c->k.b;
+	bo.kc = (float)c->k.c;
+	bo.iMc = (float)(1.0 / c->k.a);
+	bo.npts = c->g.n;
+	bo.x = (float *)B->x;
+	bo.r = (__half *)B->r;
+	launchT<__half, 8>(c, B, bo, s);
+	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
+	c->launches++;
+	const long long nb = ((long long)B->elems / 2 + 255) / 256;
+	kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
+	                                                                 (float *)B->x, B->ls.pending, 0, B->gl);
+	c->launches++;
+	enqueue_resid_h<RBD>(c, B, true);
+	kb_ru_done<<<1, 1, 0, s>>>(B->gl);
+	c->launches++;
+}
+
+template <int RBD>
+struct ImplH {
+	static int setup(Ctx *c, Batched *B, int nrhs, int maxiter, double tol) {
+		cudaStream_t s = c->stream;
+		Global g0 = {};
+		g0.iter = 1;
+		g0.maxiter = maxiter;
+		g0.tol = tol;
+		g0.tol_in = B->theta * tol;
+		g0.period = B->period;
+		g0.nrhs = nrhs;
+		g0.active = 1;
+		*B->g0_host = g0;
+		BTRY(cudaMemcpyAsync(B->gl, B->g0_host, sizeof(Global), cudaMemcpyHostToDevice, s));
+		enqueue_resid_h<RBD>(c, B, false);
+		kb_setup_done<<<1, 1, 0, s>>>(B->gl);
+		c->launches++;
+		BTRY(cudaGetLastError());
+		return 0;
+	}
+	static int chunk(Ctx *c, Batched *B) {
+		cudaStream_t s = c->stream;
+		if (!B->graph) {
+			cudaGraph_t graph;
+			const long long before = c->launches;
+			BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+			for (int i = 0; i < B->chunk; i++) enqueue_cgh_iteration<RBD>(c, B);
+			BTRY(cudaStreamEndCapture(s, &graph));
+			B->graph_kernels = c->launches - before;
+			c->launches = before;
+			cudaError_t e = cudaGraphInstantiate(&B->graph, graph, 0);
+			cudaGraphDestroy(graph);
+			if (e != cudaSuccess) {
+				B->graph = nullptr;
+				return set_cuda_error(c, e, "cudaGraphInstantiate");
+			}
+		}
+		BTRY(cudaGraphLaunch(B->graph, s));
+		c->launches += B->graph_kernels;
+		return 0;
+	}
+};
+
 static void bind_impl(Batched *B) {
+	if (B->half) {  // R >= 8: the FP64 fields use 8-lane slices
+		B->setup_fn = ImplH<8>::setup;
+		B->chunk_fn = ImplH<8>::chunk;
+		return;
+	}
 	if (B->mixed) {
 		if (B->rbT == 4 && B->rbD == 4) {
 			B->setup_fn = Impl<float, 4, 4>::setup;
@@ -2001,7 +2459,9 @@ static int lane_result(const LaneOut &l, bool bicg, double tol, int maxiter, dou
 		return 0;
 	}
 	if (l.err <= tol) {
-		*fi = l.exit_iter;
+		// A mixed lane that met tol but not its tighter in-loop target by
+		// maxiter still has a solution in the reference's sense.
+		*fi = l.reason == STOP_MAXITER ? maxiter : l.exit_iter;
 		*fe = l.err;
 		return 0;
 	}
@@ -2112,12 +2572,13 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 	g.active = B->R;
 	g.maxiter = 1 << 30;
 	g.tol = 0.0;
+	g.tol_in = 0.0;
 	g.period = 0;
 	g.nrhs = B->R;
 	*B->gl_host = g;
 	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
 	BTRY(cudaMemsetAsync(B->ls.done, 0, sizeof(int) * B->R, s));
-	BTRY(cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * 20 * B->R, s));
+	BTRY(cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * kLaneDoubles * B->R, s));
 	OpCgA<T> a;
 	a.ka = (T)c->k.a;
 	a.kb = (T)c->k.b;
@@ -2256,8 +2717,72 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 	return 0;
 }
 
+// FP16 storage form: sweeps A and B timed alone (every lane active, unit
+// scales, no lane stops).
+static int time_cgh_kernels(Ctx *c, Batched *B, int reps, double *ms, double *bytes, char *names, int *count) {
+	cudaStream_t s = c->stream;
+	Global g = {};
+	g.iter = 2;
+	g.active = B->R;
+	g.maxiter = 1 << 30;
+	g.nrhs = B->R;
+	*B->gl_host = g;
+	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
+	BTRY(cudaMemsetAsync(B->ls.done, 0, sizeof(int) * B->R, s));
+	BTRY(cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * kLaneDoubles * B->R, s));
+	OpCgAh a;
+	a.ka = (float)c->k.a;
+	a.kb = (float)c->k.b;
+	a.kc = (float)c->k.c;
+	a.iMc = (float)(1.0 / c->k.a);
+	a.iMd = 1.0 / c->k.a;
+	a.npts = c->g.n;
+	a.p0 = (__half *)B->p0;
+	a.p1 = (__half *)B->p1;
+	OpCgBh bo;
+	bo.ka = (float)c->k.a;
+	bo.kb = (float)c->k.b;
+	bo.kc = (float)c->k.c;
+	bo.iMc = (float)(1.0 / c->k.a);
+	bo.npts = c->g.n;
+	bo.x = (float *)B->x;
+	bo.r = (__half *)B->r;
+	cudaEvent_t e0, e1;
+	BTRY(cudaEventCreate(&e0));
+	BTRY(cudaEventCreate(&e1));
+	const double el = (double)B->elems;
+	for (int k = 0; k < 2; k++) {
+		auto one = [&]() {
+			if (k == 0) launchT<__half, 8>(c, B, a, s);
+			else launchT<__half, 8>(c, B, bo, s);
+		};
+		one();
+		BTRY(cudaEventRecord(e0, s));
+		for (int i = 0; i < reps; i++) one();
+		BTRY(cudaEventRecord(e1, s));
+		BTRY(cudaEventSynchronize(e1));
+		float t = 0.f;
+		BTRY(cudaEventElapsedTime(&t, e0, e1));
+		ms[k] = (double)t / reps;
+		// A: r, p_old in, p out (FP16); B: p, r in and r out (FP16), x_lo in and out (FP32).
+		bytes[k] = (k == 0 ? 6.0 : 14.0) * el;
+		snprintf(names + 32 * k, 32, "%s", k == 0 ? "cg_a_fp16" : "cg_b_fp16");
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	BTRY(cudaGetLastError());
+	if (cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+	    cudaStreamSynchronize(s) == cudaSuccess && B->gl_host->err) {
+		c->error = "batched sweep timed out waiting for its data";
+		return SEDI_ERR_CUDA;
+	}
+	*count = 2;
+	return 0;
+}
+
 int batched_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count) {
 	Batched *B = (Batched *)c->batched;
+	if (B->half) return time_cgh_kernels(c, B, reps, ms, bytes, names, count);
 	if (B->mixed) {
 		switch (B->rbT) {
 		case 4: return time_cg_kernels<float, 4>(c, B, reps, ms, bytes, names, count);
@@ -2484,12 +3009,16 @@ static int tune_sweep_ms(sedi_ctx *h, double *ms_sum) {
 
 int batched_autotune(int solver, int precision, int batch, long long n1, long long n2, long long n3, int maxiter,
                      double tol, uint32_t seed, int flags, int *out, double *score_ms) {
-	const bool mixed = precision == SEDI_PREC_MIXED;
+	const bool half = precision == SEDI_PREC_MIXED16;
+	const bool mixed = precision == SEDI_PREC_MIXED || half;
 	if (batch < 2 && !mixed) return SEDI_ERR_ARG;  // one FP64 lane is the single-vector form
-	const int R = pick_R(batch, mixed);
+	if (half && solver != SEDI_CG) return SEDI_ERR_UNSUPPORTED;
+	const int R = pick_R(batch, mixed, half);
 	const TuneKey key{solver, precision, R, n1, n2, n3};
 	std::vector<int> Ws;
-	if (R >= 8) {
+	if (half) {
+		Ws.push_back(8);  // FP16 fields: 8-lane slices only
+	} else if (R >= 8) {
 		Ws.push_back(8);
 		Ws.push_back(4);
 		if (!mixed) Ws.push_back(2);

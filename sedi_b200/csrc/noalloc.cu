@@ -82,6 +82,14 @@ extern "C" int sedi_residual_noalloc(long n1, long n2, long n3, double a, double
 	g.n2 = (int)n2;
 	g.n3 = (int)n3;
 	g.n = (long long)n1 * n2 * n3;
+	// r is written while other blocks still read x (its neighbours) and b
+	// through the read-only path: r may share no element with either.
+	const size_t bytes = (size_t)g.n * sizeof(double);
+	auto overlap = [bytes](const void *p, const void *q) {
+		const char *a = static_cast<const char *>(p), *b2 = static_cast<const char *>(q);
+		return a < b2 + bytes && b2 < a + bytes;
+	};
+	if (overlap(r_dev, x_dev) || overlap(r_dev, b_dev)) return SEDI_ERR_ARG;
 	dim3 grid;
 	int zc;
 	shape(g, &grid, &zc);

@@ -20,6 +20,20 @@ void host_fill_probe(uint32_t seed, long n, double *out) {
 	}
 }
 
+// Points [offset, offset + count) of the same probe: a double of
+// uniform_real_distribution<double> takes two 32-bit draws of mt19937
+// (generate_canonical with 53 bits from a 32-bit engine), so the engine
+// skips 2 * offset draws first.
+void host_fill_probe_range(uint32_t seed, long long offset, long long count, double *out) {
+	std::mt19937 engine(seed);
+	engine.discard((unsigned long long)offset * 2ull);
+	std::uniform_real_distribution<double> dist(0.0, 1.0);
+	for (long long i = 0; i < count; i++) {
+		const double x = dist(engine);
+		out[i] = x > 0.5 ? 1.0 : -1.0;
+	}
+}
+
 // ---------------------------------------------------------------------------
 // Device path.  MT19937 (Matsumoto & Nishimura 1998, ACM TOMACS 8(1)) with
 // the published parameters (n=624, m=397, a=0x9908b0df, tempering
@@ -104,6 +118,10 @@ int device_fill_probes(uint32_t seed, int nprobes, long long npts, int W, double
 }
 
 }  // namespace sedi
+
+extern "C" void sedi_fill_probe_range(uint32_t seed, long offset, long count, double *out) {
+	if (out && offset >= 0 && count > 0) sedi::host_fill_probe_range(seed, offset, count, out);
+}
 
 extern "C" int sedi_fill_probes_dev(uint32_t seed, int nprobes, long n, double *out_dev, void *stream) {
 	if (nprobes < 0 || n < 1 || !out_dev) return SEDI_ERR_ARG;

@@ -123,11 +123,15 @@ int batched_est_result(const Ctx *c);
 int batched_autotune(int solver, int precision, int batch, long long n1, long long n2, long long n3, int maxiter,
                      double tol, uint32_t seed, int flags, int *out, double *score_ms);
 int batched_config(const Ctx *c, int *out);
+// In-loop target factor of the mixed form (lanes stop on true err <= theta * tol).
+int batched_set_theta(Ctx *c, double theta);
+double batched_theta(const Ctx *c);
 // Device bytes a batched context allocates (0 for the single-vector form).
 size_t batched_bytes(int solver, int precision, int batch, long long n1, long long n2, long long n3);
 
 // rng.cu
 void host_fill_probe(uint32_t seed, long n, double *out);
+void host_fill_probe_range(uint32_t seed, long long offset, long long count, double *out);
 // Probes seed..seed+nprobes-1 on the device: lane-sliced (W > 0) or dense (W == 0).
 int device_fill_probes(uint32_t seed, int nprobes, long long npts, int W, double *out, cudaStream_t s);
 

@@ -100,7 +100,7 @@ namespace {
 int job_lanes(const sedi_server *S, int solver, int precision, int samples, long long n1, long long n2,
               long long n3) {
 	int b = samples < 1 ? 1 : samples;
-	const int cap = precision == SEDI_PREC_MIXED ? 256 : 128;
+	const int cap = precision == SEDI_PREC_FP64 ? 128 : 256;
 	if (b > cap) b = cap;
 	while (b > 2 && batched_bytes(solver, precision, b, n1, n2, n3) > S->job_cap) b = b > 16 ? b - 16 : b / 2;
 	return b < 2 ? 2 : b;  // one lane would select the single-vector form
@@ -280,7 +280,9 @@ void sedi_server_destroy(sedi_server *S) {
 
 long sedi_server_submit(sedi_server *S, int solver, int precision, long n1, long n2, long n3, int samples,
                         uint32_t seed, int maxiter, double tol) {
-	if (!S || solver < 1 || solver > 3 || (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED) || n1 < 1 ||
+	if (!S || solver < 1 || solver > 3 ||
+	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED && precision != SEDI_PREC_MIXED16) ||
+	    (precision == SEDI_PREC_MIXED16 && solver != SEDI_CG) || n1 < 1 ||
 	    n2 < 1 || n3 < 1 || samples < 0 || maxiter < 0 || !(tol >= 0.0))
 		return SEDI_ERR_ARG;
 	Job J;
@@ -355,7 +357,7 @@ int sedi_server_take(sedi_server *S, long id, double *D, int *iters, double *err
 
 int sedi_server_replay(sedi_server *S, int njobs, const double *arrival_s, const int *solver, const int *precision,
                        const long *edge, const int *samples, const uint32_t *seed, const double *tol, int maxiter,
-                       double *latency_s, int *rcs, double *makespan_s) {
+                       double *latency_s, int *rcs, double *makespan_s, long long *iterations) {
 	if (!S || njobs < 0 || (njobs && (!arrival_s || !solver || !precision || !edge || !samples || !seed || !tol ||
 	                                  !latency_s)))
 		return SEDI_ERR_ARG;
@@ -384,6 +386,11 @@ int sedi_server_replay(sedi_server *S, int njobs, const double *arrival_s, const
 				done++;
 				latency_s[k] = J.t_done - J.t_submit;
 				if (rcs) rcs[k] = J.rc;
+				if (iterations) {
+					long long it = 0;
+					for (int v : J.iters) it += v;
+					iterations[k] = it;
+				}
 			}
 		}
 		if (pending == 0 && next < njobs) {

@@ -21,6 +21,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -53,6 +54,18 @@ struct Vec {
 	T v[V];
 };
 
+// Storage element -> arithmetic type.  FP16 storage (the half-precision
+// Krylov fields of the mixed form) computes in FP32; a thread's vector is
+// four lanes (8 bytes) of a field.
+template <class E>
+struct Arith {
+	typedef E type;
+};
+template <>
+struct Arith<__half> {
+	typedef float type;
+};
+
 template <class T>
 __device__ __forceinline__ Vec<T> lds(const T *p) {
 	typedef typename VW<T>::raw R;
@@ -83,6 +96,29 @@ __device__ __forceinline__ void stg(T *p, const Vec<T> &x) {
 	memcpy(&r, &x, sizeof(R));
 	*reinterpret_cast<R *>(p) = r;
 }
+// FP16 storage: four lanes (8 bytes) <-> four FP32 values, round to nearest.
+__device__ __forceinline__ Vec<float> lds(const __half *p) {
+	const uint2 r = *reinterpret_cast<const uint2 *>(p);
+	__half2 h0, h1;
+	memcpy(&h0, &r.x, 4);
+	memcpy(&h1, &r.y, 4);
+	const float2 a = __half22float2(h0), b = __half22float2(h1);
+	Vec<float> o;
+	o.v[0] = a.x;
+	o.v[1] = a.y;
+	o.v[2] = b.x;
+	o.v[3] = b.y;
+	return o;
+}
+__device__ __forceinline__ void sts(__half *p, const Vec<float> &x) {
+	const __half2 h0 = __floats2half2_rn(x.v[0], x.v[1]), h1 = __floats2half2_rn(x.v[2], x.v[3]);
+	uint2 r;
+	memcpy(&r.x, &h0, 4);
+	memcpy(&r.y, &h1, 4);
+	*reinterpret_cast<uint2 *>(p) = r;
+}
+__device__ __forceinline__ Vec<float> ldg_rw(const __half *p) { return lds(p); }
+__device__ __forceinline__ void stg(__half *p, const Vec<float> &x) { sts(p, x); }
 template <class T>
 __device__ __forceinline__ Vec<T> vzero() {
 	Vec<T> o;
@@ -169,11 +205,16 @@ __host__ __device__ __forceinline__ long long sliced(long long i, int j, int W, 
 
 template <class T, int RB_, int P1_, int P2_, int THREADS_ = 512, int NSTR_ = 0>
 struct Cfg {
-	typedef T type;
+	typedef T type;                              // storage element of the streamed fields
+	typedef typename Arith<T>::type ctype;       // arithmetic type
 	static constexpr int NSTR = NSTR_;  // stages of a transforming sweep's ring (0: SEDI_STREAM_NST_RING)
-	static constexpr int V = Vec<T>::V;
+	static constexpr int V = Vec<ctype>::V;      // lanes per thread vector
 	static constexpr int RB = RB_;
 	static constexpr int LG = RB / V;  // lane groups per point
+	// Tensor-map elements per point: FP16 fields are mapped as 32-bit pairs
+	// of lanes, so every configuration moves 16 bytes per map element group
+	// and a point's first byte is 16-byte aligned.
+	static constexpr int ME = sizeof(T) == 2 ? RB / 2 : RB;
 	static constexpr int P1 = P1_, P2 = P2_;
 	static constexpr int H1 = P1 + 2, H2 = P2 + 2;
 	static constexpr int HALO = H1 * H2, INT = P1 * P2;
@@ -183,7 +224,7 @@ struct Cfg {
 	static constexpr int KO = (INT + NPS - 1) / NPS;                // output points per thread
 	static_assert(THREADS % LG == 0, "lane groups");
 	static_assert(RB * sizeof(T) % 16 == 0, "TMA inner box must be a multiple of 16 bytes");
-	static_assert(RB * (P1 + 2) <= 256, "TMA box dimension limit");
+	static_assert(ME * (P1 + 2) <= 256, "TMA box dimension limit");
 };
 
 // Pipeline of a sweep.  At step j the block computes the stencil input of

@@ -9,7 +9,10 @@ are committed and travel with the tests.
 Probe k of a run with seed S is std::mt19937(S + k) -> uniform_real(0,1) ->
 (x > 0.5 ? +1 : -1), the reference's own DistrRngStd code (DistrRngStd.hpp).
 
-Usage:  python tests/golden/make_golden.py [--full]
+Usage:  python tests/golden/make_golden.py [--full | --big]
+  --big  runs only the 256^3 CG configuration for 8 probes (one single-rank
+         process per probe) and stores its iteration counts, solve seconds
+         and a strided sample + checksums of D.
   --full also runs the 128^3 x 64-probe drop-in configuration for each solver
          (several CPU minutes, run as 8 parallel single-rank processes over
          disjoint probe ranges, t and q summed) and stores iteration counts,
@@ -102,12 +105,52 @@ def full_config(solver, procs=8, samples=64, grid=(128, 128, 128), tol=1e-9, max
         D_min=np.array(D.min()), D_max=np.array(D.max())))
 
 
+def big_config(solver=2, procs=8, grid=(256, 256, 256), tol=1e-9, maxiter=20000):
+    """The 256^3 batched configuration's grid: `procs` single-rank processes,
+    one probe each (seeds 1234..1234+procs-1), solved to tol.  Stores the
+    reference's per-probe iteration counts, errors and per-process solve
+    seconds, a strided sample and checksums of D over those probes."""
+    tmp = tempfile.mkdtemp()
+    jobs = []
+    for j in range(procs):
+        d = os.path.join(tmp, str(j))
+        cmd = [DRIVER, "-g", "x".join(map(str, grid)), "-S", str(solver), "-s", "1",
+               "-e", repr(tol), "-m", str(maxiter), "-q", "-o", d]
+        jobs.append((d, subprocess.Popen(cmd, env=dict(os.environ, SEDI_SEED=str(1234 + j)))))
+    t = q = None
+    iters, errs, results, secs = [], [], [], []
+    for d, p in jobs:
+        if p.wait() != 0:
+            raise SystemExit("ref_driver failed")
+        tj = np.fromfile(os.path.join(d, "t.f64"))
+        qj = np.fromfile(os.path.join(d, "q.f64"))
+        t = tj if t is None else t + tj
+        q = qj if q is None else q + qj
+        iters.append(np.fromfile(os.path.join(d, "iters.i32"), np.int32))
+        errs.append(np.fromfile(os.path.join(d, "errs.f64")))
+        results.append(np.fromfile(os.path.join(d, "results.i32"), np.int32))
+        secs.append(float(open(os.path.join(d, "time.txt")).read()))
+    D = t / q
+    stride = 4099
+    meta = dict(solver=solver, grid=grid, samples=procs, tol=tol, maxiter=maxiter, coeffs=(6.0, 1.0, 1.0),
+                seed=1234, procs=procs, sample_stride=stride)
+    save(f"big_{SOLVERS[solver]}_256", meta, dict(
+        iters=np.concatenate(iters), errs=np.concatenate(errs), results=np.concatenate(results),
+        seconds=np.array(secs), D_sample=D[::stride], D_sum=np.array(D.sum()), D_sumsq=np.array((D * D).sum()),
+        D_min=np.array(D.min()), D_max=np.array(D.max())))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--full", action="store_true")
+    ap.add_argument("--big", action="store_true",
+                    help="only the 256^3 CG run of 8 probes (about 5 CPU minutes on 8 cores)")
     args = ap.parse_args()
     if not os.path.exists(DRIVER):
         raise SystemExit("build the reference oracle first: make -C oracle ref")
+    if args.big:
+        big_config()
+        return
 
     # Probe generator pin: 5 probes of the 32^3 configuration, packed sign bits.
     r = run_ref(2, (32, 32, 32), 5, 1e-9, 1, dump_vx=True)

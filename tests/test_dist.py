@@ -20,6 +20,14 @@ def _oracle_local(solver, dims, count, seed, maxiter, tol, precision, batch, ste
     return O.estimate(solver, dims, count, seed, maxiter, tol)
 
 
+def _oracle_local_tensors(solver, dims, count, seed, maxiter, tol, precision, batch, stencil):
+    """As the benchmark's per-rank estimate: t and q come back as torch tensors
+    (its device buffers), reduced in place."""
+    import torch
+    r = O.estimate(solver, dims, count, seed, maxiter, tol)
+    return dict(r, t=torch.from_numpy(r["t"].copy()), q=torch.from_numpy(r["q"].copy()))
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
@@ -28,21 +36,23 @@ def _free_port():
     return p
 
 
-def _worker(rank, world, port, out_dir, samples):
+def _worker(rank, world, port, out_dir, samples, tensors):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    r = estimate_sharded(2, (9, 8, 7), samples, seed=1234, maxiter=300, tol=1e-10, local_estimate=_oracle_local)
-    np.savez(os.path.join(out_dir, f"r{rank}.npz"), **r)
+    local = _oracle_local_tensors if tensors else _oracle_local
+    r = estimate_sharded(2, (9, 8, 7), samples, seed=1234, maxiter=300, tol=1e-10, local_estimate=local)
+    np.savez(os.path.join(out_dir, f"r{rank}.npz"), **{k: (v.numpy() if hasattr(v, "numpy") and not
+                                                            isinstance(v, np.ndarray) else v) for k, v in r.items()})
     dist.barrier()
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("samples", [6, 5, 1])
-def test_two_ranks_match_one_process(tmp_path, samples):
+@pytest.mark.parametrize("samples,tensors", [(6, False), (5, False), (1, False), (6, True)])
+def test_two_ranks_match_one_process(tmp_path, samples, tensors):
     port = _free_port()
-    mp.start_processes(_worker, args=(2, port, str(tmp_path), samples), nprocs=2, start_method="spawn")
+    mp.start_processes(_worker, args=(2, port, str(tmp_path), samples, tensors), nprocs=2, start_method="spawn")
     full = O.estimate(2, (9, 8, 7), samples, 1234, 300, 1e-10)
     for rank in range(2):
         r = np.load(tmp_path / f"r{rank}.npz")

@@ -1,0 +1,113 @@
+"""Slab (i3) domain decomposition of CG on CPU ranks (gloo), -p 1x1xP.
+
+The host logic of sedi_b200.domain -- halo exchange between ranks, the
+plane-ordered dot reduction, the CG loop and the estimator -- runs with the
+NumPy stand-in for the slab kernels.  A run split over 2 or 3 ranks (or 3
+slabs in one process) must give the single-slab result bit for bit, and that
+result matches the oracle's CG (the reference method) to 1e-12.
+"""
+import ctypes
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import _oracle as O
+import sedi_b200 as S
+from sedi_b200.domain import SlabCg, parse_decomposition, slab_range
+from _slab_numpy import NumpySlabBackend
+
+DIMS = (9, 8, 7)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _run(parts, dims, samples, loopback=False, stencil=None, mode=0):
+    cg = SlabCg(dims, parts, stencil=stencil, backend=NumpySlabBackend(dims, stencil), loopback=loopback, mode=mode)
+    r = cg.estimate(samples, 1234, 300, 1e-10)
+    return dict(D=cg.gather(r["D"]), iters=r["iters"], errs=r["errs"], results=r["results"])
+
+
+def _worker(rank, world, port, out_dir, dims, samples, mode):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    r = _run(world, dims, samples, mode=mode)
+    np.savez(os.path.join(out_dir, f"r{rank}.npz"), **r)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_slab_ranges_and_decomposition_argument():
+    for n3 in (1, 7, 64):
+        for parts in range(1, min(n3, 5) + 1):
+            spans = [slab_range(n3, parts, s) for s in range(parts)]
+            assert [k for f, c in spans for k in range(f, f + c)] == list(range(n3))
+            assert min(c for _, c in spans) >= 1
+    assert parse_decomposition("1x1x4", 8) == 4
+    for bad in ("2x1x1", "1x2x2", "1x1x9", "1x1", "axbxc", "1x1x0"):
+        with pytest.raises(ValueError):
+            parse_decomposition(bad, 8)
+
+
+def test_probe_range_is_a_slice_of_the_global_probe():
+    n = 5000
+    full = S.fill_probe(77, n)
+    for off, cnt in ((0, 10), (1, 1), (1234, 999), (4000, 1000)):
+        part = np.empty(cnt)
+        S.load().sedi_fill_probe_range(77, off, cnt, part.ctypes.data_as(ctypes.c_void_p))
+        assert np.array_equal(part, full[off:off + cnt])
+
+
+def test_one_slab_matches_the_oracle_cg():
+    one = _run(1, DIMS, 3)
+    ref = O.estimate(2, DIMS, 3, 1234, 300, 1e-10)
+    assert np.array_equal(one["iters"], ref["iters"])
+    assert O.relmax(one["D"], ref["D"]) <= 1e-12
+
+
+@pytest.mark.parametrize("parts", [2, 3, 7])
+def test_slabs_in_one_process_are_bit_exact(parts):
+    one = _run(1, DIMS, 3)
+    many = _run(parts, DIMS, 3, loopback=True)
+    assert np.array_equal(many["D"], one["D"])
+    assert np.array_equal(many["iters"], one["iters"]) and np.array_equal(many["errs"], one["errs"])
+
+
+@pytest.mark.parametrize("world,mode", [(2, 0), (3, 0), (2, 1)])
+def test_ranks_are_bit_exact(tmp_path, world, mode):
+    port = _free_port()
+    mp.start_processes(_worker, args=(world, port, str(tmp_path), DIMS, 3, mode), nprocs=world, start_method="spawn")
+    one = _run(1, DIMS, 3)
+    for rank in range(world):
+        r = np.load(tmp_path / f"r{rank}.npz")
+        assert np.array_equal(r["D"], one["D"])
+        assert np.array_equal(r["iters"], one["iters"]) and np.array_equal(r["errs"], one["errs"])
+
+
+def test_nonsymmetric_stencil_and_apply():
+    st = S.Stencil(6.0, 1.3, 0.7)
+    dims = (6, 5, 8)
+    x_full = np.random.default_rng(3).standard_normal(int(np.prod(dims)))
+    outs = []
+    for parts in (1, 3):
+        cg = SlabCg(dims, parts, stencil=st, backend=NumpySlabBackend(dims, st), loopback=True)
+        xs, ys = cg.zeros(), cg.zeros()
+        plane = dims[0] * dims[1]
+        for j, s in enumerate(cg.local):
+            f, c = cg.ranges[s]
+            cg.backend.set_interior(xs[j], x_full[f * plane:(f + c) * plane])
+        cg.apply(xs, ys)
+        outs.append(cg.gather(ys))
+    assert np.array_equal(outs[0], outs[1])
+    ref = O.stencil(dims, x_full, (6.0, 1.3, 0.7))
+    assert np.array_equal(outs[0], ref)

@@ -61,8 +61,30 @@ def test_noalloc_zero_rhs_and_limit():
     z = np.zeros(n)
     rc, r, err = _noalloc(dims, z, z)
     assert rc == 0 and err == 0.0 and np.all(r == 0.0)
-    # ceil(n1/32) * ceil(n2/8) > 4096 blocks is rejected before any launch.
+    # ceil(n1/32) * ceil(n2/8) > 4096 blocks is rejected before any launch
+    # (three disjoint address ranges, never dereferenced).
     err = ctypes.c_double(0.0)
-    rc = S.load().sedi_residual_noalloc(32 * 4097, 8, 1, 6.0, 1.0, 1.0, ctypes.c_void_p(8), ctypes.c_void_p(8),
-                                        ctypes.c_void_p(8), ctypes.byref(err), None)
+    size = 32 * 4097 * 8 * 8
+    rc = S.load().sedi_residual_noalloc(32 * 4097, 8, 1, 6.0, 1.0, 1.0, ctypes.c_void_p(256),
+                                        ctypes.c_void_p(256 + size), ctypes.c_void_p(256 + 2 * size),
+                                        ctypes.byref(err), None)
     assert rc == -1
+
+
+def test_noalloc_rejects_output_overlapping_an_input():
+    import torch
+    dims = (16, 8, 4)
+    n = int(np.prod(dims))
+    x = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+    b = torch.zeros(n, dtype=torch.float64, device="cuda")
+    err = ctypes.c_double(0.0)
+    lib = S.load()
+    vp = ctypes.c_void_p
+    for r_ptr in (x.data_ptr(), x.data_ptr() + 8 * (n // 2), b.data_ptr()):
+        rc = lib.sedi_residual_noalloc(*dims, 6.0, 1.0, 1.0, vp(x.data_ptr()), vp(b.data_ptr()), vp(r_ptr),
+                                       ctypes.byref(err), None)
+        assert rc == -1
+    # The second half of x is disjoint from its first n elements: accepted.
+    rc = lib.sedi_residual_noalloc(*dims, 6.0, 1.0, 1.0, vp(x.data_ptr()), vp(b.data_ptr()),
+                                   vp(x.data_ptr() + 8 * n), ctypes.byref(err), None)
+    assert rc == 0 and err.value == 0.0
