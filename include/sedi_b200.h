@@ -79,7 +79,10 @@ typedef struct sedi_ctx sedi_ctx;
  *   a,b,c      stencil coefficients: y = a*x_c - c*(x_{i-1}+...) - b*(x_{i+1}+...)
  *   mode       SEDI_MODE_* bits (accepted, no effect on one GPU)
  *   precision  SEDI_PREC_FP64, SEDI_PREC_MIXED or SEDI_PREC_MIXED16 (CG only;
- *              SEDI_ERR_UNSUPPORTED for the other solvers)
+ *              SEDI_ERR_UNSUPPORTED for the other solvers).  The mixed
+ *              pipelined CG needs n1*n2*n3 >= 4096 (SEDI_ERR_UNSUPPORTED
+ *              below: its FP32 recurrences do not reach tol on a few hundred
+ *              unknowns; the FP64 form covers every grid).
  *   batch      right-hand sides in flight per launch (1 = single-vector form)
  *   err        out: 0 or a negative SEDI_ERR_* (may be NULL)
  * Returns NULL on error.
@@ -147,6 +150,9 @@ int sedi_set_stream(sedi_ctx *ctx, void *stream);
  * bytes[k] its algorithmic DRAM bytes per launch (compulsory reads + writes
  * of the Krylov vectors it streams), names (count*32 chars, NUL-terminated
  * slots).  The buffers' contents are scratch afterwards.  Returns 0 or error.
+ * A single-vector FP64 context (batch 1) times its streaming sweeps (names
+ * ending in _sv; SEDI_ERR_UNSUPPORTED when n1 is odd: those grids use the
+ * column-march kernels).
  */
 int sedi_time_kernels(sedi_ctx *ctx, int reps, double *ms, double *bytes, char *names, int *count);
 
@@ -267,7 +273,9 @@ sedi_server *sedi_server_create(double budget_bytes, int max_active, double job_
 void sedi_server_destroy(sedi_server *srv);
 
 /* Queue a job; returns its id (>= 0) or a negative error (SEDI_ERR_NOMEM
- * when even one batch of it exceeds the budget). */
+ * when even one batch of it exceeds the budget, SEDI_ERR_UNSUPPORTED for a
+ * combination sedi_create refuses: mixed pipelined CG below 4096 points,
+ * FP16 storage with another solver than CG). */
 long sedi_server_submit(sedi_server *srv, int solver, int precision, long n1, long n2, long n3, int samples,
                         uint32_t seed, int maxiter, double tol);
 

@@ -54,7 +54,19 @@ struct LaneState {
 	double *rho, *rho_prev, *omega, *s_norm2, *ts, *tt;         // BiCGStab
 	double *r_scale, *p_scale0, *p_scale1, *pp;                 // FP16 storage: field scales, <p,p>
 	int *done, *exit_iter, *reason, *pending, *s_exit;
+	double *hist;  // single-vector form: err after each iteration (lane 0), else null
 };
+
+// Single-vector (pairs) form: lane 1 is the odd i1 points of lane 0's vector
+// and carries the same scalars.
+__device__ __forceinline__ void mirror_lane0(const LaneState &ls) {
+	double *const d[] = {ls.bb, ls.rr, ls.err, ls.ru, ls.ru_new, ls.sp, ls.alpha, ls.beta, ls.gamma, ls.gamma_old,
+	                     ls.delta, ls.rr_top, ls.rho, ls.rho_prev, ls.omega, ls.s_norm2, ls.ts, ls.tt, ls.r_scale,
+	                     ls.p_scale0, ls.p_scale1, ls.pp};
+	for (double *a : d) a[1] = a[0];
+	int *const n[] = {ls.done, ls.exit_iter, ls.reason, ls.pending, ls.s_exit};
+	for (int *a : n) a[1] = a[0];
+}
 
 struct Global {
 	int iter;       // iteration the next launch executes
@@ -277,10 +289,18 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 				const Vec<T> xm3 = zm ? lds(cm + hc) : vzero<T>();
 				const Vec<T> xp3 = zp ? lds(cp + hc) : vzero<T>();
 				Vec<T> y;
+				if (C::PAIRS) {
+					// Points 2m, 2m+1 of one vector: i1 neighbours across the pair.
+					y.v[0] = st7<T>(op.ka, op.kb, op.kc, xc.v[0], xm1.v[1], xm2.v[0], xm3.v[0], xc.v[1], xp2.v[0],
+					                xp3.v[0]);
+					y.v[1] = st7<T>(op.ka, op.kb, op.kc, xc.v[1], xc.v[0], xm2.v[1], xm3.v[1], xp1.v[0], xp2.v[1],
+					                xp3.v[1]);
+				} else {
 #pragma unroll
-				for (int e = 0; e < V; e++)
-					y.v[e] = st7<T>(op.ka, op.kb, op.kc, xc.v[e], xm1.v[e], xm2.v[e], xm3.v[e], xp1.v[e], xp2.v[e],
-					                xp3.v[e]);
+					for (int e = 0; e < V; e++)
+						y.v[e] = st7<T>(op.ka, op.kb, op.kc, xc.v[e], xm1.v[e], xm2.v[e], xm3.v[e], xp1.v[e], xp2.v[e],
+						                xp3.v[e]);
+				}
 				Vec<T> qv[NQ > 0 ? NQ : 1];
 #pragma unroll
 				for (int qq = 0; qq < NQ; qq++) qv[qq] = lds(stz + NS * HE + qq * IE + qoff[k]);
@@ -353,14 +373,31 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 		}
 	}
 	__syncthreads();
-	for (int lane = t; lane < R; lane += C::THREADS) {
-		double tot[NDX];
-		for (int d = 0; d < ND; d++) {
-			double s = 0.0;
-			for (int q = 0; q < parts; q++) s += acc[((size_t)q * ND + d) * R + lane];
-			tot[d] = s;
+	if (C::PAIRS) {
+		// One vector: the even and odd points' sums are one dot product.
+		if (t == 0) {
+			double tot[NDX];
+			for (int d = 0; d < ND; d++) {
+				double s0 = 0.0, s1 = 0.0;
+				for (int q = 0; q < parts; q++) {
+					s0 += acc[((size_t)q * ND + d) * R + 0];
+					s1 += acc[((size_t)q * ND + d) * R + 1];
+				}
+				tot[d] = s0 + s1;
+			}
+			op.fin(0, tot, gl, ls);
+			mirror_lane0(ls);
 		}
-		op.fin(lane, tot, gl, ls);
+	} else {
+		for (int lane = t; lane < R; lane += C::THREADS) {
+			double tot[NDX];
+			for (int d = 0; d < ND; d++) {
+				double s = 0.0;
+				for (int q = 0; q < parts; q++) s += acc[((size_t)q * ND + d) * R + lane];
+				tot[d] = s;
+			}
+			op.fin(lane, tot, gl, ls);
+		}
 	}
 	__syncthreads();
 	if (t == 0) *ticket = 0u;
@@ -488,6 +525,7 @@ struct OpResid : OpBase<double> {
 		ls.rr[lane] = tot[1];
 		const double err = sqrt(__ddiv_rn(tot[1], bb));
 		ls.err[lane] = err;
+		if (ls.hist && lane == 0) ls.hist[0] = err;
 		ls.alpha[lane] = 0.0;
 		ls.beta[lane] = 0.0;
 		ls.omega[lane] = 1.0;
@@ -639,6 +677,7 @@ struct OpCgB : OpBase<T> {
 		ls.beta[lane] = __ddiv_rn(tot[0], ls.ru[lane]);           // :185
 		const double err = sqrt(__ddiv_rn(tot[1], ls.bb[lane]));  // :191
 		ls.err[lane] = err;
+		if (ls.hist && lane == 0) ls.hist[it] = err;              // :192
 		const double tol = gl->tol_in;
 		const int maxiter = gl->maxiter;
 		if (mixed) {
@@ -759,6 +798,7 @@ struct OpPcg : OpBase<T> {
 		// The stop test uses <r,r> from the top of this iteration (:173, :227).
 		const double err = sqrt(__ddiv_rn(ls.rr_top[lane], ls.bb[lane]));
 		ls.err[lane] = err;
+		if (ls.hist && lane == 0) ls.hist[it] = err;  // :228
 		const double g = ls.gamma[lane], d = ls.delta[lane];
 		double al;
 		const bool restarted = ls.s_exit[lane] == 2;
@@ -1102,6 +1142,7 @@ struct OpBicg3 : OpBicgS<T> {
 		ls.rr[lane] = tot[0];
 		const double err = sqrt(__ddiv_rn(tot[0], ls.bb[lane]));  // :226
 		ls.err[lane] = err;
+		if (ls.hist && lane == 0) ls.hist[it] = err;              // :228
 		const double om = ls.omega[lane];
 		if (mixed) {
 			ls.rho_prev[lane] = ls.rho[lane];
@@ -1632,6 +1673,9 @@ struct Batched {
 	int R = 0;
 	bool mixed = false;  // FP32 or FP16 Krylov fields, FP64 x_hi, reductions and reliable update
 	bool half = false;   // FP16 storage of r and p (CG), FP32 x_lo
+	bool pairs = false;  // single-vector FP64 form: lanes 0/1 = even/odd i1 points of one vector
+	bool aliased = false;  // the Krylov fields belong to the context (single-vector form)
+	const double *graph_hist = nullptr;  // history pointer the captured graph holds
 	size_t elems = 0;  // npts * R
 	// vectors ([point][R])
 	void *x = nullptr;     // FP64 form: x; MIXED: x_lo (FP32)
@@ -1718,11 +1762,11 @@ __host__ __device__ constexpr int tile_p2(int lg) {
 // barrier and latency are paid once per two points; 222 KB of shared
 // memory).  Measured on B200 at 128^3 x 64 lanes: CG A 449 -> 372 us,
 // BiCGStab 2 463 -> 353 us, BiCGStab 3 877 -> 787 us.
-template <class T, int RB, int KIND = 0>
+template <class T, int RB, int KIND = 0, bool PAIRS = false>
 struct CfgFor {
 	static constexpr int LG = RB * (int)sizeof(T) / 16;
 	static constexpr bool WIDE = KIND == 1 && LG == 1;
-	typedef Cfg<T, RB, tile_p1(LG), WIDE ? 32 : tile_p2(LG), kThr, WIDE ? 4 : 0> type;
+	typedef Cfg<T, RB, tile_p1(LG), WIDE ? 32 : tile_p2(LG), kThr, WIDE ? 4 : 0, PAIRS> type;
 };
 
 static int pick_R(int nrhs, bool mixed, bool half = false) {
@@ -1808,14 +1852,16 @@ static int launch(Ctx *c, Batched *B, const SGeo &sg, dim3 grid, const Maps &map
 }
 
 // Launch of a sweep over the T (Krylov) fields with the op's tile kind.
-template <class T, int RBT, class Op>
+template <class T, int RBT, bool PAIRS = false, class Op>
 static int launchT(Ctx *c, Batched *B, const Op &op, cudaStream_t s) {
-	typedef typename CfgFor<T, RBT, Op::KIND>::type C;
+	typedef typename CfgFor<T, RBT, Op::KIND, PAIRS>::type C;
 	if (Op::KIND == 1) return launch<C>(c, B, B->gT1, B->gridT1, B->mapsT1, op, s);
 	return launch<C>(c, B, B->gT, B->gridT, B->mapsT, op, s);
 }
 
 static void bind_impl(Batched *B);
+
+constexpr long long kMixedPcgMinPoints = 4096;  // smallest grid of the mixed pipelined CG
 
 // Default in-loop target of the mixed form, theta * tol on the FP64 true
 // residual.  Two solutions that both meet tol can differ by more than the
@@ -1858,6 +1904,14 @@ int batched_alloc(Ctx *c) {
 	B->mixed = c->precision == SEDI_PREC_MIXED || B->half;
 	if (B->half && c->solver != SEDI_CG) {
 		c->error = "FP16 Krylov storage is implemented for CG";
+		return SEDI_ERR_UNSUPPORTED;
+	}
+	if (B->mixed && c->solver == SEDI_PIPELINED_CG && c->g.n < kMixedPcgMinPoints) {
+		// On a few hundred unknowns the FP32 pipelined recurrences converge
+		// exactly within a few steps and then lose the residual faster than
+		// reliable updates restore it (5x7x9 at tol 1e-10 did not reach tol
+		// in 2,000 iterations); such grids take the FP64 form.
+		c->error = "mixed-precision pipelined CG needs at least 4096 grid points; use the FP64 form";
 		return SEDI_ERR_UNSUPPORTED;
 	}
 	if (c->batch > (B->mixed ? 256 : 128)) {
@@ -2016,6 +2070,24 @@ size_t batched_bytes(int solver, int precision, int batch, long long n1, long lo
 	return total;
 }
 
+static void free_batched(Batched *B) {
+	if (!B) return;
+	void *fields[] = {B->x, B->xh, B->b, B->r, B->p0, B->p1, B->t_acc, B->q_acc, B->w[0], B->w[1], B->u, B->q,
+	                  B->sv, B->z, B->r1, B->v[0], B->v[1], B->rhat};
+	if (!B->aliased)
+		for (void *p : fields)
+			if (p) cudaFree(p);
+	void *own[] = {B->partials, B->ticket, B->gl, B->lane_mem, B->lane_int};
+	for (void *p : own)
+		if (p) cudaFree(p);
+	if (B->gl_host) cudaFreeHost(B->gl_host);
+	if (B->lane_host) cudaFreeHost(B->lane_host);
+	if (B->lane_host_int) cudaFreeHost(B->lane_host_int);
+	if (B->ev) cudaEventDestroy(B->ev);
+	if (B->graph) cudaGraphExecDestroy(B->graph);
+	delete B;
+}
+
 void batched_free(Ctx *c) {
 	Batched *B = (Batched *)c->batched;
 	if (!B) return;
@@ -2033,10 +2105,10 @@ void batched_free(Ctx *c) {
 	c->batched = nullptr;
 }
 
-template <int RBD>
+template <int RBD, bool PAIRS = false>
 static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 	const int pcg = c->solver == 3 ? 1 : 0;
-	typedef typename CfgFor<double, RBD>::type CD;
+	typedef typename CfgFor<double, RBD, 0, PAIRS>::type CD;
 	cudaStream_t s = c->stream;
 	if (B->mixed) {
 		OpResid<float> op;
@@ -2073,7 +2145,7 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 	}
 }
 
-template <class T, int RBT, int RBD>
+template <class T, int RBT, int RBD, bool PAIRS = false>
 static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	cudaStream_t s = c->stream;
 	OpCgA<T> a;
@@ -2084,7 +2156,7 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	a.p0 = (T *)B->p0;
 	a.p1 = (T *)B->p1;
 	a.mixed = B->mixed ? 1 : 0;
-	launchT<T, RBT>(c, B, a, s);
+	launchT<T, RBT, PAIRS>(c, B, a, s);
 	OpCgB<T> bo;
 	bo.ka = (T)c->k.a;
 	bo.kb = (T)c->k.b;
@@ -2093,7 +2165,7 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	bo.x = (T *)B->x;
 	bo.r = (T *)B->r;
 	bo.mixed = B->mixed ? 1 : 0;
-	launchT<T, RBT>(c, B, bo, s);
+	launchT<T, RBT, PAIRS>(c, B, bo, s);
 	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
 	c->launches++;
 	if (B->mixed) {
@@ -2102,13 +2174,13 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 		                                                                 (float *)B->x, B->ls.pending,
 		                                                                 c->solver == 3 ? 1 : 0, B->gl);
 		c->launches++;
-		enqueue_resid<RBD>(c, B, true);
+		enqueue_resid<RBD, PAIRS>(c, B, true);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
 		c->launches++;
 	}
 }
 
-template <class T, int RBT>
+template <class T, int RBT, bool PAIRS = false>
 static void enqueue_pcg_uw(Ctx *c, Batched *B, int zero, int ru) {
 	OpPcgUW<T> o;
 	o.ka = (T)c->k.a;
@@ -2124,10 +2196,10 @@ static void enqueue_pcg_uw(Ctx *c, Batched *B, int zero, int ru) {
 	o.z = (T *)B->z;
 	o.zero = zero;
 	o.ru = ru;
-	launchT<T, RBT>(c, B, o, c->stream);
+	launchT<T, RBT, PAIRS>(c, B, o, c->stream);
 }
 
-template <class T, int RBT, int RBD>
+template <class T, int RBT, int RBD, bool PAIRS = false>
 static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 	cudaStream_t s = c->stream;
 	OpPcg<T> o;
@@ -2145,7 +2217,7 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 	o.w0 = (T *)B->w[0];
 	o.w1 = (T *)B->w[1];
 	o.mixed = B->mixed ? 1 : 0;
-	launchT<T, RBT>(c, B, o, s);
+	launchT<T, RBT, PAIRS>(c, B, o, s);
 	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
 	c->launches++;
 	if (B->mixed) {
@@ -2157,7 +2229,7 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 		                                                                 (float *)B->x, B->ls.pending,
 		                                                                 c->solver == 3 ? 1 : 0, B->gl);
 		c->launches++;
-		enqueue_resid<RBD>(c, B, true);
+		enqueue_resid<RBD, PAIRS>(c, B, true);
 		OpApply<T> a1;
 		a1.ka = (T)c->k.a;
 		a1.kb = (T)c->k.b;
@@ -2166,19 +2238,19 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 		a1.y = (T *)B->sv;
 		a1.y2 = (T *)B->q;
 		a1.map = MT_P0_HALO;
-		launchT<T, RBT>(c, B, a1, s);
+		launchT<T, RBT, PAIRS>(c, B, a1, s);
 		OpApply<T> a2 = a1;
 		a2.y = (T *)B->z;
 		a2.y2 = nullptr;
 		a2.map = MT_Q_HALO;
-		launchT<T, RBT>(c, B, a2, s);
-		enqueue_pcg_uw<T, RBT>(c, B, 0, 1);
+		launchT<T, RBT, PAIRS>(c, B, a2, s);
+		enqueue_pcg_uw<T, RBT, PAIRS>(c, B, 0, 1);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
 		c->launches++;
 	}
 }
 
-template <class T, int RBT, int RBD>
+template <class T, int RBT, int RBD, bool PAIRS = false>
 static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	cudaStream_t s = c->stream;
 	const T ka = (T)c->k.a, kb = (T)c->k.b, kc = (T)c->k.c, iMc = (T)(1.0 / c->k.a);
@@ -2192,13 +2264,13 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	o1.v0 = (T *)B->v[0];
 	o1.v1 = (T *)B->v[1];
 	o1.rhat = (T *)B->rhat;
-	launchT<T, RBT>(c, B, o1, s);
+	launchT<T, RBT, PAIRS>(c, B, o1, s);
 	OpBicg2<T> o2;
 	o2.ka = ka;
 	o2.kb = kb;
 	o2.kc = kc;
 	o2.iMc = iMc;
-	launchT<T, RBT>(c, B, o2, s);
+	launchT<T, RBT, PAIRS>(c, B, o2, s);
 	OpBicg3<T> o3;
 	o3.ka = ka;
 	o3.kb = kb;
@@ -2211,7 +2283,7 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	o3.p1 = (T *)B->p1;
 	o3.rhat = (T *)B->rhat;
 	o3.mixed = B->mixed ? 1 : 0;
-	launchT<T, RBT>(c, B, o3, s);
+	launchT<T, RBT, PAIRS>(c, B, o3, s);
 	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
 	c->launches++;
 	if (B->mixed) {
@@ -2222,7 +2294,7 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 		                                                                 (float *)B->x, B->ls.pending,
 		                                                                 c->solver == 3 ? 1 : 0, B->gl);
 		c->launches++;
-		enqueue_resid<RBD>(c, B, true);
+		enqueue_resid<RBD, PAIRS>(c, B, true);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
 		c->launches++;
 	}
@@ -2234,7 +2306,7 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 // the setup sweep runs under a +1 guard on `active` that kb_setup_done drops).
 // chunk: one launch of the captured graph of `chunk` iterations; lanes and
 // launches past the stop are no-ops.
-template <class T, int RBT, int RBD>
+template <class T, int RBT, int RBD, bool PAIRS = false>
 struct Impl {
 	static int setup(Ctx *c, Batched *B, int nrhs, int maxiter, double tol) {
 		cudaStream_t s = c->stream;
@@ -2248,10 +2320,10 @@ struct Impl {
 		g0.active = 1;
 		*B->g0_host = g0;  // read by the copy below; rewritten only after this batch is over
 		BTRY(cudaMemcpyAsync(B->gl, B->g0_host, sizeof(Global), cudaMemcpyHostToDevice, s));
-		enqueue_resid<RBD>(c, B, false);
+		enqueue_resid<RBD, PAIRS>(c, B, false);
 		kb_setup_done<<<1, 1, 0, s>>>(B->gl);
 		c->launches++;
-		if (c->solver == 3) enqueue_pcg_uw<T, RBT>(c, B, 1, 0);  // :138-149 (skipped when no lane is live)
+		if (c->solver == 3) enqueue_pcg_uw<T, RBT, PAIRS>(c, B, 1, 0);  // :138-149 (skipped when no lane is live)
 		BTRY(cudaGetLastError());
 		return 0;
 	}
@@ -2263,9 +2335,9 @@ struct Impl {
 			const long long before = c->launches;
 			BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
 			for (int i = 0; i < B->chunk; i++) {
-				if (c->solver == 3) enqueue_pcg_iteration<T, RBT, RBD>(c, B);
-				else if (c->solver == 1) enqueue_bicg_iteration<T, RBT, RBD>(c, B);
-				else enqueue_cg_iteration<T, RBT, RBD>(c, B);
+				if (c->solver == 3) enqueue_pcg_iteration<T, RBT, RBD, PAIRS>(c, B);
+				else if (c->solver == 1) enqueue_bicg_iteration<T, RBT, RBD, PAIRS>(c, B);
+				else enqueue_cg_iteration<T, RBT, RBD, PAIRS>(c, B);
 			}
 			BTRY(cudaStreamEndCapture(s, &graph));
 			B->graph_kernels = c->launches - before;
@@ -2415,6 +2487,112 @@ static void bind_impl(Batched *B) {
 	}
 }
 
+// Single-vector FP64 form on the streaming sweeps.  A dense vector with n1
+// even is the 2-lane sliced layout of the (n1/2, n2, n3) grid: lane 0 holds
+// the even i1 points, lane 1 the odd ones, so the sweeps of the batched FP64
+// form run on the context's own vectors (aliased, nothing copied), with the
+// stencil's i1 neighbours taken across each pair and the two lanes' sums
+// added into one dot product (Cfg::PAIRS).  Elementwise values round as the
+// reference's, as in the batched FP64 form.  Odd n1, and solves with a
+// vector iM, use the context's march kernels (plain.cu).
+int pairs_alloc(Ctx *c) {
+	c->pairs = nullptr;
+	if (c->g.n1 % 2 != 0 || !encode_fn()) return 0;
+	Batched *B = new (std::nothrow) Batched();
+	if (!B) return SEDI_ERR_NOMEM;
+	B->pairs = B->aliased = true;
+	B->R = 2;
+	B->rbT = B->rbD = 2;
+	B->elems = (size_t)c->g.n;
+	Geo g = c->g;
+	g.n1 = c->g.n1 / 2;
+	g.n = c->g.n / 2;
+	B->x = c->x;
+	B->b = c->b;
+	B->r = c->r;
+	B->p0 = c->p[0];
+	B->p1 = c->p[1];
+	B->w[0] = c->w[0];
+	B->w[1] = c->w[1];
+	B->u = c->u;
+	B->q = c->q;
+	B->sv = c->s;
+	B->z = c->z;
+	B->r1 = c->u;  // BiCGStab's second r buffer (it has no u)
+	B->v[0] = c->v[0];
+	B->v[1] = c->v[1];
+	B->rhat = c->rhat;
+	shape(g, 2, 2, 8, &B->gT, &B->gridT);
+	shape(g, 2, 2, 8, &B->gT1, &B->gridT1, 0, 1);
+	shape(g, 2, 2, 8, &B->gD, &B->gridD);
+	size_t nblk = (size_t)B->gridT.x * B->gridT.z;
+	if ((size_t)B->gridT1.x * B->gridT1.z > nblk) nblk = (size_t)B->gridT1.x * B->gridT1.z;
+	if (cudaMalloc(&B->partials, sizeof(double) * nblk * kMaxDots * B->R) != cudaSuccess ||
+	    cudaMalloc(&B->ticket, sizeof(unsigned)) != cudaSuccess || cudaMalloc(&B->gl, sizeof(Global)) != cudaSuccess ||
+	    cudaMallocHost(&B->gl_host, 2 * sizeof(Global)) != cudaSuccess ||
+	    cudaMallocHost(&B->lane_host, sizeof(double) * kLaneDoubles * B->R) != cudaSuccess ||
+	    cudaMallocHost(&B->lane_host_int, sizeof(int) * kLaneInts * B->R) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&B->ev, cudaEventDisableTiming) != cudaSuccess ||
+	    cudaMalloc(&B->lane_mem, sizeof(double) * kLaneDoubles * B->R) != cudaSuccess ||
+	    cudaMalloc(&B->lane_int, sizeof(int) * kLaneInts * B->R) != cudaSuccess) {
+		cudaGetLastError();
+		free_batched(B);
+		c->error = "device allocation failed (single-vector sweeps)";
+		return SEDI_ERR_NOMEM;
+	}
+	cudaMemsetAsync(B->ticket, 0, sizeof(unsigned), c->stream);
+	cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * kLaneDoubles * B->R, c->stream);
+	cudaMemsetAsync(B->lane_int, 0, sizeof(int) * kLaneInts * B->R, c->stream);
+	LaneState &ls = B->ls;
+	double **dp[] = {&ls.bb, &ls.rr, &ls.err, &ls.ru, &ls.ru_new, &ls.sp, &ls.alpha, &ls.beta, &ls.gamma,
+	                 &ls.gamma_old, &ls.delta, &ls.rr_top, &ls.rho, &ls.rho_prev, &ls.omega, &ls.s_norm2, &ls.ts,
+	                 &ls.tt, &ls.r_scale, &ls.p_scale0, &ls.p_scale1, &ls.pp};
+	for (size_t i = 0; i < sizeof(dp) / sizeof(dp[0]); i++) *dp[i] = B->lane_mem + i * B->R;
+	int **ip[] = {&ls.done, &ls.exit_iter, &ls.reason, &ls.pending, &ls.s_exit};
+	for (size_t i = 0; i < 5; i++) *ip[i] = B->lane_int + i * B->R;
+	ls.hist = nullptr;
+	auto t_maps = [&](Maps &M, int kind) {
+		int Q1, Q2;
+		tile_for(2, 8, &Q1, &Q2, kind);
+		bool k = make_map(&M.m[MT_R_HALO], B->r, 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
+		         make_map(&M.m[MT_P0_HALO], B->p0, 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
+		         make_map(&M.m[MT_P1_HALO], B->p1, 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
+		         make_map(&M.m[MT_X_INT], B->x, 8, g, 2, 2, Q1, Q2) &&
+		         make_map(&M.m[MT_R_INT], B->r, 8, g, 2, 2, Q1, Q2);
+		if (c->solver == 3)
+			k = k && make_map(&M.m[MT_W0_HALO], B->w[0], 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
+			    make_map(&M.m[MT_W1_HALO], B->w[1], 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
+			    make_map(&M.m[MT_Q_HALO], B->q, 8, g, 2, 2, Q1 + 2, Q2 + 2);
+		if (c->solver == 1)
+			k = k && make_map(&M.m[MT_R1_HALO], B->r1, 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
+			    make_map(&M.m[MT_V0_HALO], B->v[0], 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
+			    make_map(&M.m[MT_V1_HALO], B->v[1], 8, g, 2, 2, Q1 + 2, Q2 + 2);
+		return k;
+	};
+	int P1, P2;
+	tile_for(2, 8, &P1, &P2);
+	const bool ok = t_maps(B->mapsT, 0) && t_maps(B->mapsT1, 1) &&
+	                make_map(&B->mapsD.m[MD_X_HALO], B->x, 8, g, 2, 2, P1 + 2, P2 + 2) &&
+	                make_map(&B->mapsD.m[MD_B_INT], B->b, 8, g, 2, 2, P1, P2);
+	if (!ok) {
+		free_batched(B);
+		c->error = "tensor map encoding failed (single-vector sweeps)";
+		return SEDI_ERR_CUDA;
+	}
+	B->g0_host = B->gl_host + 1;
+	B->lane_res.assign(B->R, 0);
+	B->setup_fn = Impl<double, 2, 2, true>::setup;
+	B->chunk_fn = Impl<double, 2, 2, true>::chunk;
+	c->pairs = B;
+	if (cudaStreamSynchronize(c->stream) != cudaSuccess) return set_cuda_error(c, cudaGetLastError(), "pairs_alloc");
+	return 0;
+}
+
+void pairs_free(Ctx *c) {
+	free_batched((Batched *)c->pairs);
+	c->pairs = nullptr;
+}
+
 static int check_flags(Ctx *c, Batched *B) {
 	if (B->gl_host->err) {
 		c->error = "batched sweep timed out waiting for its data";
@@ -2537,6 +2715,32 @@ static int batched_run_resident(Ctx *c, int nrhs, int maxiter, double tol, doubl
 	return process_lanes(c, B, nrhs, maxiter, tol, final_err, final_iter, results);
 }
 
+// Single-vector solve on the streaming sweeps: b and x (the initial guess)
+// already in the context's vectors; the history of errors is written into
+// c->hist as the single-vector kernels do.
+int pairs_solve_resident(Ctx *c, int maxiter, double tol, double *final_err, int *final_iter) {
+	Batched *B = (Batched *)c->pairs;
+	B->ls.hist = c->hist;
+	if (B->graph && B->graph_hist != c->hist) {  // the graph holds the old history pointer
+		cudaGraphExecDestroy(B->graph);
+		B->graph = nullptr;
+	}
+	int rc = run_batched(c, B, 1, maxiter, tol);
+	B->graph_hist = c->hist;
+	if (rc) return rc;
+	if ((rc = enqueue_lane_copy(c, B))) return rc;
+	BTRY(cudaStreamSynchronize(c->stream));
+	int res = 0;
+	process_lanes(c, B, 1, maxiter, tol, final_err, final_iter, &res);
+	// Entries of the history: the initial err plus one per iteration that
+	// printed its err (the s-norm exit and the rho breakdown leave before).
+	const int reason = B->lane_host_int[2 * B->R], ex = B->lane_host_int[1 * B->R];
+	if (reason == STOP_EARLY) c->hist_len = 1;
+	else if (reason == STOP_SNORM || reason == STOP_RHO) c->hist_len = ex;
+	else c->hist_len = (ex > maxiter ? maxiter : ex) + 1;
+	return res;
+}
+
 static int blocks1d(long long n) {
 	long long b = (n + 255) / 256;
 	return (int)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
@@ -2564,7 +2768,7 @@ int batched_solve_dev(Ctx *c, int nrhs, const double *b, double *x, int maxiter,
 
 // Per-iteration kernels of the batched CG timed in isolation (see
 // sedi_time_kernels): every lane active, no lane stops, no reliable update.
-template <class T, int RBT>
+template <class T, int RBT, bool PAIRS = false>
 static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *bytes, char *names, int *count) {
 	cudaStream_t s = c->stream;
 	Global g = {};
@@ -2615,16 +2819,16 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		o.w0 = (T *)B->w[0];
 		o.w1 = (T *)B->w[1];
 		o.mixed = 0;
-		launchT<T, RBT>(c, B, o, s);
+		launchT<T, RBT, PAIRS>(c, B, o, s);
 		BTRY(cudaEventRecord(e0, s));
-		for (int i = 0; i < reps; i++) launchT<T, RBT>(c, B, o, s);
+		for (int i = 0; i < reps; i++) launchT<T, RBT, PAIRS>(c, B, o, s);
 		BTRY(cudaEventRecord(e1, s));
 		BTRY(cudaEventSynchronize(e1));
 		float t = 0.f;
 		BTRY(cudaEventElapsedTime(&t, e0, e1));
 		ms[0] = (double)t / reps;
 		bytes[0] = 16.0 * ts;  // w, q, s, p, z, r, x, u in and out
-		snprintf(names, 32, "%s", B->mixed ? "pcg_fp32" : "pcg_fp64");
+		snprintf(names, 32, "%s%s", B->mixed ? "pcg_fp32" : "pcg_fp64", PAIRS ? "_sv" : "");
 		cudaEventDestroy(e0);
 		cudaEventDestroy(e1);
 		*count = 1;
@@ -2667,9 +2871,9 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		                                          // 3: r, v, x, p, r_hat in, x, r out
 		for (int k = 0; k < 3; k++) {
 			auto one = [&]() {
-				if (k == 0) launchT<T, RBT>(c, B, o1, s);
-				else if (k == 1) launchT<T, RBT>(c, B, o2, s);
-				else launchT<T, RBT>(c, B, o3, s);
+				if (k == 0) launchT<T, RBT, PAIRS>(c, B, o1, s);
+				else if (k == 1) launchT<T, RBT, PAIRS>(c, B, o2, s);
+				else launchT<T, RBT, PAIRS>(c, B, o3, s);
 			};
 			one();
 			BTRY(cudaEventRecord(e0, s));
@@ -2680,7 +2884,7 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 			BTRY(cudaEventElapsedTime(&t, e0, e1));
 			ms[k] = (double)t / reps;
 			bytes[k] = words[k] * ts;
-			snprintf(names + 32 * k, 32, "%s_%s", nm[k], B->mixed ? "fp32" : "fp64");
+			snprintf(names + 32 * k, 32, "%s_%s%s", nm[k], B->mixed ? "fp32" : "fp64", PAIRS ? "_sv" : "");
 		}
 		cudaEventDestroy(e0);
 		cudaEventDestroy(e1);
@@ -2689,12 +2893,12 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		return 0;
 	}
 	for (int k = 0; k < 2; k++) {
-		if (k == 0) launchT<T, RBT>(c, B, a, s);
-		else launchT<T, RBT>(c, B, bo, s);
+		if (k == 0) launchT<T, RBT, PAIRS>(c, B, a, s);
+		else launchT<T, RBT, PAIRS>(c, B, bo, s);
 		BTRY(cudaEventRecord(e0, s));
 		for (int i = 0; i < reps; i++) {
-			if (k == 0) launchT<T, RBT>(c, B, a, s);
-			else launchT<T, RBT>(c, B, bo, s);
+			if (k == 0) launchT<T, RBT, PAIRS>(c, B, a, s);
+			else launchT<T, RBT, PAIRS>(c, B, bo, s);
 		}
 		BTRY(cudaEventRecord(e1, s));
 		BTRY(cudaEventSynchronize(e1));
@@ -2702,8 +2906,8 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		BTRY(cudaEventElapsedTime(&t, e0, e1));
 		ms[k] = (double)t / reps;
 		bytes[k] = (k == 0 ? 3.0 : 5.0) * ts;  // A: r, p_old in, p out; B: p, x, r in, x, r out
-		snprintf(names + 32 * k, 32, "%s", k == 0 ? (B->mixed ? "cg_a_fp32" : "cg_a_fp64")
-		                                           : (B->mixed ? "cg_b_fp32" : "cg_b_fp64"));
+		snprintf(names + 32 * k, 32, "%s%s", k == 0 ? (B->mixed ? "cg_a_fp32" : "cg_a_fp64")
+		                                             : (B->mixed ? "cg_b_fp32" : "cg_b_fp64"), PAIRS ? "_sv" : "");
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
@@ -2778,6 +2982,13 @@ static int time_cgh_kernels(Ctx *c, Batched *B, int reps, double *ms, double *by
 	}
 	*count = 2;
 	return 0;
+}
+
+// Single-vector form: its streaming sweeps timed alone (names end in _sv).
+int pairs_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count) {
+	Batched *B = (Batched *)c->pairs;
+	if (!B) return SEDI_ERR_UNSUPPORTED;
+	return time_cg_kernels<double, 2, true>(c, B, reps, ms, bytes, names, count);
 }
 
 int batched_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count) {

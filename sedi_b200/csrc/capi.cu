@@ -375,7 +375,7 @@ int sedi_time_kernels(sedi_ctx *h, int reps, double *ms, double *bytes, char *na
 	cudaSetDevice(c->device);
 	if (plain_form(c)) {
 		*count = 0;
-		return SEDI_ERR_UNSUPPORTED;
+		return pairs_time_kernels(c, reps, ms, bytes, names, count);  // unsupported for odd n1
 	}
 	return batched_time_kernels(c, reps, ms, bytes, names, count);
 }

@@ -513,10 +513,11 @@ int plain_alloc(Ctx *c) {
 	c->hist_cap = 0;
 	c->hist = nullptr;
 	c->chunk_iters = 16;
-	return 0;
+	return pairs_alloc(c);
 }
 
 void plain_free(Ctx *c) {
+	pairs_free(c);
 	double *vecs[] = {c->x, c->b, c->iM, c->r, c->rhat, c->p[0], c->p[1], c->v[0], c->v[1],
 	                  c->w[0], c->w[1], c->u, c->q, c->s, c->z, c->t_acc, c->q_acc, c->partials, c->hist};
 	for (double *p : vecs)
@@ -674,6 +675,11 @@ static int solve_impl(Ctx *c, IMv<VIM> im, int maxiter, double tol, double *fina
 
 // Solve with b, x (and iM when vim) already in the context's buffers.
 int plain_solve_resident(Ctx *c, bool vim, int maxiter, double tol, double *final_err, int *final_iter) {
+	if (!vim && c->pairs) {  // n1 even, constant iM: the streaming sweeps
+		const int rc = ensure_hist(c, maxiter);
+		if (rc) return rc;
+		return pairs_solve_resident(c, maxiter, tol, final_err, final_iter);
+	}
 	if (vim) {
 		IMv<true> im{c->iM, 0.0};
 		return solve_impl<true>(c, im, maxiter, tol, final_err, final_iter);

@@ -134,10 +134,13 @@ int main(int argc, char **argv) {
 		}
 	}
 	if (!have_g || !have_p) usage(argv[0]);
-	// DomainDecomposition.hpp:29-36 asserts ranks == np and divisibility; one
-	// GPU holds the whole grid, so the decomposition must be 1x1x1.
+	// DomainDecomposition.hpp:29-36 asserts ranks == np and divisibility; this
+	// driver holds the whole grid on one GPU (-p 1x1x1).  Slab decompositions
+	// over several GPUs (-p 1x1xP) run in the Python driver under torchrun.
 	if (np1 != 1 || np2 != 1 || np3 != 1) {
-		fprintf(stderr, "sedi: the grid runs on one GPU; use -p 1x1x1\n");
+		fprintf(stderr,
+		        "sedi: this driver runs the grid on one GPU (-p 1x1x1); for -p 1x1xP over P GPUs run\n"
+		        "      torchrun --nproc-per-node P -m sedi_b200.cli -g ... -p 1x1xP\n");
 		return 1;
 	}
 	printf("Global grid shape is (%ld, %ld, %ld)\n", ng1, ng2, ng3);

@@ -78,6 +78,7 @@ struct Ctx {
 	size_t stage_probe_bytes;
 
 	void *batched;  // batched-form state (batched.cu)
+	void *pairs;    // single-vector form on the streaming sweeps (n1 even; batched.cu)
 
 	long long launches;
 	std::string error;
@@ -98,6 +99,12 @@ int plain_divide(Ctx *c, double *D_dev);
 
 // batched.cu
 int batched_alloc(Ctx *c);
+// Single-vector form on the streaming sweeps (n1 even): state aliasing the
+// plain form's vectors; solve with b, x already in c->b, c->x (constant iM).
+int pairs_alloc(Ctx *c);
+void pairs_free(Ctx *c);
+int pairs_solve_resident(Ctx *c, int maxiter, double tol, double *final_err, int *final_iter);
+int pairs_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count);
 void batched_free(Ctx *c);
 int batched_solve_dev(Ctx *c, int nrhs, const double *b, double *x, int maxiter, double tol, double *final_err,
                       int *final_iter, int *results);

@@ -203,9 +203,14 @@ __host__ __device__ __forceinline__ long long sliced(long long i, int j, int W, 
 	return ((long long)(j / W) * npts + i) * W + (j % W);
 }
 
-template <class T, int RB_, int P1_, int P2_, int THREADS_ = 512, int NSTR_ = 0>
+// PAIRS_: the two lanes of a point are two consecutive i1 points of one
+// vector (a dense FP64 vector with even n1 is the 2-lane sliced layout of
+// the (n1/2, n2, n3) grid); the stencil takes its i1 neighbours across the
+// pair and the two lanes' sums are one reduction.
+template <class T, int RB_, int P1_, int P2_, int THREADS_ = 512, int NSTR_ = 0, bool PAIRS_ = false>
 struct Cfg {
 	typedef T type;                              // storage element of the streamed fields
+	static constexpr bool PAIRS = PAIRS_;
 	typedef typename Arith<T>::type ctype;       // arithmetic type
 	static constexpr int NSTR = NSTR_;  // stages of a transforming sweep's ring (0: SEDI_STREAM_NST_RING)
 	static constexpr int V = Vec<ctype>::V;      // lanes per thread vector

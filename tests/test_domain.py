@@ -111,3 +111,17 @@ def test_nonsymmetric_stencil_and_apply():
     assert np.array_equal(outs[0], outs[1])
     ref = O.stencil(dims, x_full, (6.0, 1.3, 0.7))
     assert np.array_equal(outs[0], ref)
+
+
+def test_decomposed_cli_rejects_bad_arguments_before_device_use():
+    import subprocess
+    import sys
+    for args in (["-g", "8x8x8", "-p", "2x1x1"], ["-g", "8x8x8", "-p", "1x1x9"], ["-g", "8x8", "-p", "1x1x1"],
+                 ["-g", "8x8x8", "-p", "1x1x2", "-f", "8"], ["-p", "1x1x1"]):
+        r = subprocess.run([sys.executable, "-m", "sedi_b200.cli"] + args, capture_output=True, text=True, timeout=120,
+                           cwd=O.REPO)
+        assert r.returncode == 2, (args, r.stderr)
+    # -p 1x1x2 without torchrun ranks or --loopback is refused.
+    r = subprocess.run([sys.executable, "-m", "sedi_b200.cli", "-g", "8x8x8", "-p", "1x1x2"], capture_output=True,
+                       text=True, timeout=120, cwd=O.REPO)
+    assert r.returncode == 1 and "--loopback" in r.stderr

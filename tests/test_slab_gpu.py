@@ -1,0 +1,100 @@
+"""Slab (i3) domain decomposition of CG on the GPU (sedi_slab_* kernels).
+
+Several slabs in one process on one GPU (halos by device copies): the
+solution must not depend on the number of slabs, bit for bit; the slab
+stencil is the single-vector stencil bit for bit; the estimate matches the
+oracle's CG (the reference method) and the single-vector GPU form.
+"""
+import numpy as np
+import pytest
+
+import _oracle as O
+import sedi_b200 as S
+from sedi_b200.domain import SlabCg
+
+pytestmark = pytest.mark.gpu
+
+
+def _estimate(dims, parts, samples=3, maxiter=400, tol=1e-10, mode=0):
+    cg = SlabCg(dims, parts, loopback=True, mode=mode)
+    r = cg.estimate(samples, 1234, maxiter, tol)
+    return dict(D=cg.gather(r["D"]), iters=r["iters"], errs=r["errs"], results=r["results"])
+
+
+@pytest.mark.parametrize("dims", [(24, 20, 18), (33, 17, 9), (16, 16, 64)])
+def test_slab_count_does_not_change_the_solution(dims):
+    one = _estimate(dims, 1)
+    assert np.all(one["results"] == 0)
+    for parts in (2, 3, dims[2]):
+        many = _estimate(dims, parts)
+        assert np.array_equal(many["D"], one["D"]), parts
+        assert np.array_equal(many["iters"], one["iters"]) and np.array_equal(many["errs"], one["errs"])
+    # Synchronous stencil mode (no overlap of inner planes) gives the same bits.
+    assert np.array_equal(_estimate(dims, 2, mode=1)["D"], one["D"])
+
+
+def test_slab_estimate_matches_oracle_and_single_vector_form():
+    dims = (24, 20, 18)
+    r = _estimate(dims, 3)
+    ref = O.estimate(2, dims, 3, 1234, 400, 1e-10)
+    assert np.array_equal(r["iters"], ref["iters"])
+    assert O.relmax(r["D"], ref["D"]) <= 1e-10
+    with S.Context("cg", dims) as c:
+        p = c.estimate(3, 1234, 400, 1e-10)
+    assert np.array_equal(r["iters"], p["iters"])
+    assert O.relmax(r["D"], p["D"]) <= 1e-12
+
+
+def test_slab_stencil_is_the_single_vector_stencil():
+    import torch
+    for dims, coeffs in (((20, 13, 11), (6.0, 1.0, 1.0)), ((7, 9, 12), (6.0, 1.3, 0.7))):
+        st = S.Stencil(*coeffs)
+        x = np.random.default_rng(9).standard_normal(int(np.prod(dims)))
+        with S.Context("cg", dims, st) as c:
+            y_ref = c.stencil_apply(x)
+        for parts in (1, 4):
+            cg = SlabCg(dims, parts, stencil=st, loopback=True)
+            xs, ys = cg.zeros(), cg.zeros()
+            plane = dims[0] * dims[1]
+            for j, s in enumerate(cg.local):
+                f, n = cg.ranges[s]
+                cg.backend.set_interior(xs[j], x[f * plane:(f + n) * plane])
+            cg.apply(xs, ys)
+            torch.cuda.synchronize()
+            assert np.array_equal(cg.gather(ys), y_ref), (dims, parts)
+
+
+def test_slab_maxiter_and_zero_rhs():
+    import torch
+    dims = (12, 10, 8)
+    cg = SlabCg(dims, 2, loopback=True)
+    x, b = cg.zeros(), cg.zeros()
+    res, err, it = cg.solve(x, b, 50, 1e-10)  # b = 0: <b,b> taken as 1, err 0 < tol
+    assert (res, err, it) == (0, 0.0, 0)
+    for j, s in enumerate(cg.local):
+        cg.backend.fill_probe(b[j], 1234, cg.ranges[s][0] * dims[0] * dims[1])
+    res, err, it = cg.solve(x, b, 5, 1e-14)
+    assert res == 1 and it == 5
+    ref = O.estimate(2, dims, 1, 1234, 5, 1e-14)
+    assert abs(err - ref["errs"][0]) <= 1e-12 * ref["errs"][0]
+
+
+def test_decomposed_cli_matches_the_one_gpu_driver(tmp_path):
+    import os
+    import subprocess
+    import sys
+    d_slab, d_one = tmp_path / "slab.f64", tmp_path / "one.f64"
+    common = ["-g", "16x12x10", "-s", "3", "-e", "1e-10", "-m", "400", "--quiet"]
+    r = subprocess.run([sys.executable, "-m", "sedi_b200.cli", "-p", "1x1x3", "--loopback", "--write-d", str(d_slab)]
+                       + common, capture_output=True, text=True, timeout=600, cwd=O.REPO)
+    assert r.returncode == 0, r.stderr
+    exe = os.path.join(O.REPO, "sedi_b200", "_lib", "sedi")
+    one = subprocess.run([exe, "-p", "1x1x1", "--write-d", str(d_one)] + common, capture_output=True, text=True,
+                         timeout=600)
+    assert one.returncode == 0, one.stderr
+    line = lambda out: [ln for ln in out.splitlines() if ln.startswith("Total solve time")][0].split("count")[1]
+    assert line(r.stdout) == line(one.stdout)
+    assert "Processor decomposition is (1, 1, 3)" in r.stdout
+    assert "Process block shape is (16, 12, 4)" in r.stdout
+    a, b = np.fromfile(d_slab), np.fromfile(d_one)
+    assert O.relmax(a, b) <= 1e-12
