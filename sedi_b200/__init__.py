@@ -26,7 +26,8 @@ import os
 import numpy as np
 
 __all__ = [
-    "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "Server", "autotune", "estimate", "fill_probe",
+    "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "Server", "autotune", "set_tuning", "estimate",
+    "fill_probe",
     "job_bytes", "library_path", "load", "SOLVER_IDS", "FP64", "MIXED", "MIXED16",
 ]
 
@@ -102,6 +103,7 @@ def load():
     lib.sedi_autotune.argtypes = [c_int, c_int, c_int, c_long, c_long, c_long, c_int, c_double, ctypes.c_uint32,
                                   c_int, vp, pd]
     lib.sedi_ctx_config.argtypes = [vp, vp]
+    lib.sedi_set_tuning.argtypes = [c_int, c_int, c_int, c_long, c_long, c_long, vp]
     lib.sedi_set_mixed_target.argtypes = [vp, c_double]
     lib.sedi_mixed_target.argtypes = [vp]
     lib.sedi_mixed_target.restype = c_double
@@ -206,10 +208,10 @@ class Context:
 
     def config(self):
         """Launch choices of a batched context (see autotune)."""
-        cf = np.zeros(5, np.int32)
+        cf = np.zeros(6, np.int32)
         self._check(load().sedi_ctx_config(self._h, _ptr(cf)), "config")
         return {"slice_width": int(cf[0]), "z_chunks": int(cf[1]), "period": int(cf[2]), "chunk": int(cf[3]),
-                "lanes": int(cf[4])}
+                "lanes": int(cf[4]), "prefetch_planes": int(cf[5])}
 
     @property
     def mixed_target(self):
@@ -374,14 +376,25 @@ def autotune(solver, dims, batch, precision=MIXED, maxiter=5000, tol=1e-9, seed=
     (sedi_autotune); contexts created afterwards use them.  Returns
     {"slice_width", "z_chunks", "period", "chunk", "score_ms"}."""
     sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
-    ch = np.zeros(4, np.int32)
+    ch = np.zeros(5, np.int32)
     ms = ctypes.c_double(0.0)
     rc = load().sedi_autotune(sid, int(precision), int(batch), *[int(d) for d in dims], int(maxiter), float(tol),
                               int(seed) & 0xFFFFFFFF, 1 if solve else 0, _ptr(ch), ctypes.byref(ms))
     if rc < 0:
         raise SediError(rc, "sedi_autotune")
     return {"slice_width": int(ch[0]), "z_chunks": int(ch[1]), "period": int(ch[2]), "chunk": int(ch[3]),
-            "score_ms": ms.value}
+            "prefetch_planes": int(ch[4]), "score_ms": ms.value}
+
+
+def set_tuning(solver, dims, batch, precision=MIXED, slice_width=0, z_chunks=0, period=0, chunk=0,
+               prefetch_planes=-1):
+    """Record launch choices for contexts of this shape without measuring
+    (sedi_set_tuning), e.g. an earlier autotune result."""
+    sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
+    ch = np.array([slice_width, z_chunks, period, chunk, prefetch_planes], np.int32)
+    rc = load().sedi_set_tuning(sid, int(precision), int(batch), *[int(d) for d in dims], _ptr(ch))
+    if rc < 0:
+        raise SediError(rc, "sedi_set_tuning")
 
 
 def job_bytes(solver, dims, lanes, precision=FP64):

@@ -202,6 +202,14 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 			tma_load3(st + s * HE, &maps.m[op.src_map(s)], b, (i1_0 - 1) * ME, i2_0 - 1, zoff + p);
 #pragma unroll
 		for (int q = 0; q < NQ; q++) tma_load3(st + NS * HE + q * IE, &maps.m[op.q_map(q)], b, i1_0 * ME, i2_0, zoff + p);
+		// The same tiles pfd planes further on, into L2 (within this block's planes).
+		const int pf = p + g.pfd;
+		if (g.pfd > 0 && pf <= z1 && pf < g.n3) {
+#pragma unroll
+			for (int s = 0; s < NS; s++) tma_prefetch3(&maps.m[op.src_map(s)], (i1_0 - 1) * ME, i2_0 - 1, zoff + pf);
+#pragma unroll
+			for (int q = 0; q < NQ; q++) tma_prefetch3(&maps.m[op.q_map(q)], i1_0 * ME, i2_0, zoff + pf);
+		}
 	};
 	int issued = 0;
 	if (t == 0)
@@ -1609,8 +1617,12 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 // grid): lane-slice width of the Krylov fields, i3 split of the sweeps,
 // reliable-update period and iterations per captured graph.  Zero fields
 // mean "default".  Filled by sedi_autotune, read when a context is created.
+#ifndef SEDI_STREAM_PFD
+#define SEDI_STREAM_PFD 0  // default L2 prefetch distance of the sweeps, in planes (0: none)
+#endif
 struct Tuning {
 	int W = 0, nz = 0, period = 0, chunk = 0;
+	int pfd = -1;  // L2 prefetch distance in planes (-1: SEDI_STREAM_PFD)
 };
 struct TuneKey {
 	int solver, precision, R;
@@ -1796,7 +1808,8 @@ static void tile_for(int rb, int eb, int *P1, int *P2, int kind = 0) {
 	*P2 = (kind == 1 && lg == 1) ? 32 : tile_p2(lg);
 }
 
-static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int nz_force = 0, int kind = 0) {
+static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int nz_force = 0, int kind = 0,
+                  int pfd = -1) {
 	int P1, P2;
 	tile_for(rb, eb, &P1, &P2, kind);
 	const int t1 = (g.n1 + P1 - 1) / P1, t2 = (g.n2 + P2 - 1) / P2;
@@ -1835,6 +1848,7 @@ static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int
 	sg->npts = g.n;
 	sg->zc = zc;
 	sg->tiles1 = t1;
+	sg->pfd = pfd >= 0 ? pfd : SEDI_STREAM_PFD;
 	*grid = dim3((unsigned)(t1 * t2), (unsigned)slices, (unsigned)nz);
 }
 
@@ -1933,9 +1947,9 @@ int batched_alloc(Ctx *c) {
 	if (tu.period > 0) B->period = tu.period;
 	B->theta = default_theta(c->solver);
 	if (tu.chunk > 0) B->chunk = tu.chunk;
-	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz);
-	shape(c->g, B->R, B->rbT, ebT, &B->gT1, &B->gridT1, tu.nz, 1);
-	shape(c->g, B->R, B->rbD, 8, &B->gD, &B->gridD, tu.nz);
+	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
+	shape(c->g, B->R, B->rbT, ebT, &B->gT1, &B->gridT1, tu.nz, 1, tu.pfd);
+	shape(c->g, B->R, B->rbD, 8, &B->gD, &B->gridD, tu.nz, 0, tu.pfd);
 	const size_t ts = (size_t)ebT;                                  // Krylov field element
 	const size_t xs = B->mixed ? sizeof(float) : sizeof(double);   // x (FP64 form) or x_lo (mixed)
 	const size_t nblkT = (size_t)B->gridT.x * B->gridT.z, nblkD = (size_t)B->gridD.x * B->gridD.z;
@@ -3267,6 +3281,16 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 		if (rc) return rc;
 		if (ms < 0.97 * best_ms) best_ms = ms, best = t;  // a clear win over the model's split
 	}
+	// L2 prefetch distance of the sweeps (planes ahead of the TMA loads).
+	const int pfds[] = {0, 2, 4, 8};
+	for (int pf : pfds) {
+		Tuning t = best;
+		t.pfd = pf;
+		double ms = 0.0;
+		const int rc = score(t, &ms);
+		if (rc) return rc;
+		if (ms < 0.98 * best_ms || (best.pfd < 0 && pf == SEDI_STREAM_PFD)) best_ms = ms, best = t;
+	}
 	double best_est = -1.0;
 	if (flags & 1) {
 		set_tuning(key, best);
@@ -3322,7 +3346,25 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 	out[1] = best.nz;
 	out[2] = best.period;
 	out[3] = best.chunk;
+	out[4] = best.pfd >= 0 ? best.pfd : SEDI_STREAM_PFD;
 	if (score_ms) *score_ms = best_est >= 0 ? best_est : best_ms;
+	return 0;
+}
+
+int batched_set_tuning(int solver, int precision, int batch, long long n1, long long n2, long long n3,
+                       const int *choice) {
+	const bool half = precision == SEDI_PREC_MIXED16;
+	const bool mixed = precision == SEDI_PREC_MIXED || half;
+	Tuning t;
+	t.W = choice[0];
+	t.nz = choice[1];
+	t.period = choice[2];
+	t.chunk = choice[3];
+	t.pfd = choice[4];
+	if (t.W < 0 || t.nz < 0 || t.period < 0 || t.chunk < 0 || t.pfd < -1 || t.pfd > 64 ||
+	    (t.period > 0 && (t.period < 1 || t.period > 1000)) || t.chunk > 256)
+		return SEDI_ERR_ARG;
+	set_tuning(TuneKey{solver, precision, pick_R(batch, mixed, half), n1, n2, n3}, t);
 	return 0;
 }
 
@@ -3334,6 +3376,7 @@ int batched_config(const Ctx *c, int *out) {
 	out[2] = B->period;
 	out[3] = B->chunk;
 	out[4] = B->R;
+	out[5] = B->gT.pfd;
 	return 0;
 }
 

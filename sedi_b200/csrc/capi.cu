@@ -117,6 +117,14 @@ int sedi_set_mixed_target(sedi_ctx *h, double theta) {
 
 double sedi_mixed_target(const sedi_ctx *h) { return h ? batched_theta(&h->c) : 1.0; }
 
+int sedi_set_tuning(int solver, int precision, int batch, long n1, long n2, long n3, const int *choice) {
+	if (solver < 1 || solver > 3 ||
+	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED && precision != SEDI_PREC_MIXED16) || batch < 1 ||
+	    n1 < 1 || n2 < 1 || n3 < 1 || !choice)
+		return SEDI_ERR_ARG;
+	return batched_set_tuning(solver, precision, batch, n1, n2, n3, choice);
+}
+
 int sedi_ctx_config(const sedi_ctx *h, int *config) {
 	if (!h || !config) return SEDI_ERR_ARG;
 	return batched_config(&h->c, config);

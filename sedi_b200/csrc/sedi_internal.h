@@ -130,6 +130,8 @@ int batched_est_result(const Ctx *c);
 int batched_autotune(int solver, int precision, int batch, long long n1, long long n2, long long n3, int maxiter,
                      double tol, uint32_t seed, int flags, int *out, double *score_ms);
 int batched_config(const Ctx *c, int *out);
+int batched_set_tuning(int solver, int precision, int batch, long long n1, long long n2, long long n3,
+                       const int *choice);
 // In-loop target factor of the mixed form (lanes stop on true err <= theta * tol).
 int batched_set_theta(Ctx *c, double theta);
 double batched_theta(const Ctx *c);

@@ -183,6 +183,16 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, uin
 	    : "memory");
 }
 
+// L2 prefetch of a tensor tile (no shared memory, no barrier): the plane a
+// later tma_load3 reads is already on its way from DRAM when that load is
+// issued, so the ring's few stages are not the only bytes in flight.
+__device__ __forceinline__ void tma_prefetch3(const CUtensorMap *map, int c0, int c1, int c2) {
+	asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+	                 reinterpret_cast<uint64_t>(map)),
+	             "r"(c0), "r"(c1), "r"(c2)
+	             : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Geometry of one batched sweep.
 // ---------------------------------------------------------------------------
@@ -197,6 +207,7 @@ struct SGeo {
 	int zc;         // planes per block
 	int tiles1;     // tiles along i1
 	long long npts; // n1*n2*n3
+	int pfd;        // planes the L2 prefetch runs ahead of the TMA loads (0: none)
 };
 
 __host__ __device__ __forceinline__ long long sliced(long long i, int j, int W, long long npts) {
