@@ -80,9 +80,9 @@ typedef struct sedi_ctx sedi_ctx;
  *   mode       SEDI_MODE_* bits (accepted, no effect on one GPU)
  *   precision  SEDI_PREC_FP64, SEDI_PREC_MIXED or SEDI_PREC_MIXED16 (CG only;
  *              SEDI_ERR_UNSUPPORTED for the other solvers).  The mixed
- *              pipelined CG needs n1*n2*n3 >= 4096 (SEDI_ERR_UNSUPPORTED
- *              below: its FP32 recurrences do not reach tol on a few hundred
- *              unknowns; the FP64 form covers every grid).
+ *              forms of CG and pipelined CG run the CG recurrence (one GPU
+ *              has no reduction latency for pipelining to hide; see
+ *              sedi_set_mixed_target for their accuracy).
  *   batch      right-hand sides in flight per launch (1 = single-vector form)
  *   err        out: 0 or a negative SEDI_ERR_* (may be NULL)
  * Returns NULL on error.
@@ -273,9 +273,8 @@ sedi_server *sedi_server_create(double budget_bytes, int max_active, double job_
 void sedi_server_destroy(sedi_server *srv);
 
 /* Queue a job; returns its id (>= 0) or a negative error (SEDI_ERR_NOMEM
- * when even one batch of it exceeds the budget, SEDI_ERR_UNSUPPORTED for a
- * combination sedi_create refuses: mixed pipelined CG below 4096 points,
- * FP16 storage with another solver than CG). */
+ * when even one batch of it exceeds the budget, SEDI_ERR_ARG for FP16
+ * storage with another solver than CG). */
 long sedi_server_submit(sedi_server *srv, int solver, int precision, long n1, long n2, long n3, int samples,
                         uint32_t seed, int maxiter, double tol);
 
@@ -347,11 +346,13 @@ int sedi_set_tuning(int solver, int precision, int batch, long n1, long n2, long
  * 0 < theta <= 1; result codes and final_err are still judged against tol
  * as the reference does (Cg.hpp:191-206), and the initial test stays
  * err < tol (Cg.hpp:130-134).  Two solutions that both meet tol differ by
- * the error each leaves behind the residual bound, which for the FP32
- * recurrences of pipelined CG and BiCGStab is larger than for FP64; a
- * tighter target brings the mixed solution within the FP64 form's own
- * truncation error of it, at the cost of the extra iterations.  The default
- * is chosen per solver by measurement (sedi_mixed_target reads it).
+ * the error each leaves behind the residual bound.  The FP32 CG iterates
+ * follow the FP64 ones, so theta = 1 keeps the CG and pipelined-CG
+ * diagonals within 1e-8 of the FP64 form's (measured 1.5e-9 at 128^3,
+ * 3.9e-9 at 256^3, tol 1e-9); BiCGStab's FP64 diagonal itself lies 1e-7
+ * to 4e-7 from the converged answer at tol 1e-9, and theta = 0.1 puts the
+ * mixed one ten times closer to it than that.  Defaults: CG and pipelined
+ * CG 1, BiCGStab 0.1, FP16 storage 0.1 (sedi_mixed_target reads them).
  * SEDI_ERR_UNSUPPORTED for FP64 contexts, SEDI_ERR_ARG for theta outside (0, 1].
  */
 int sedi_set_mixed_target(sedi_ctx *ctx, double theta);

@@ -1656,10 +1656,13 @@ constexpr int kLaneDoubles = 22, kLaneInts = 5;  // LaneState arrays
 #define SEDI_MIXED_THETA_CG 1.0
 #endif
 #ifndef SEDI_MIXED_THETA_PCG
-#define SEDI_MIXED_THETA_PCG 0.1
+#define SEDI_MIXED_THETA_PCG 1.0
 #endif
 #ifndef SEDI_MIXED_THETA_BICGSTAB
 #define SEDI_MIXED_THETA_BICGSTAB 0.1
+#endif
+#ifndef SEDI_MIXED_THETA_FP16
+#define SEDI_MIXED_THETA_FP16 0.1
 #endif
 
 struct Batched;
@@ -1686,6 +1689,7 @@ struct Batched {
 	bool mixed = false;  // FP32 or FP16 Krylov fields, FP64 x_hi, reductions and reliable update
 	bool half = false;   // FP16 storage of r and p (CG), FP32 x_lo
 	bool pairs = false;  // single-vector FP64 form: lanes 0/1 = even/odd i1 points of one vector
+	int ks = 0;          // solver whose sweeps run (the mixed pipelined CG runs the CG recurrence)
 	bool aliased = false;  // the Krylov fields belong to the context (single-vector form)
 	const double *graph_hist = nullptr;  // history pointer the captured graph holds
 	size_t elems = 0;  // npts * R
@@ -1875,14 +1879,28 @@ static int launchT(Ctx *c, Batched *B, const Op &op, cudaStream_t s) {
 
 static void bind_impl(Batched *B);
 
-constexpr long long kMixedPcgMinPoints = 4096;  // smallest grid of the mixed pipelined CG
+// Sweeps a context runs.  The mixed form of pipelined CG runs the CG
+// recurrence: pipelining hides the latency of a distributed reduction
+// (PipelinedCg.hpp:155-184), which one GPU, whose reductions end on the
+// device, does not have; in FP32 its extra recurrences (w, z, s, q) drift
+// from the FP64 iterates (27% more iterations and a diagonal 9e-8 from the
+// FP64 form's at 256^3 x 32 probes, tol 1e-9), while CG's FP32 iterates
+// follow the FP64 ones and FP64 CG and FP64 pipelined CG give the same
+// diagonal to about 1e-9.  It also moves 8 instead of 16 words per point
+// and iteration.
+static int kernel_solver(int solver, bool mixed) { return mixed && solver == SEDI_PIPELINED_CG ? SEDI_CG : solver; }
 
 // Default in-loop target of the mixed form, theta * tol on the FP64 true
-// residual.  Two solutions that both meet tol can differ by more than the
-// solver's own rounding: the FP32 recurrence takes a different path and
-// leaves a different error behind the same residual bound.  A tighter
-// target puts the mixed solution nearer the exact one, so its distance to
-// the FP64 form's solution is the FP64 form's own truncation error.
+// residual (measured at 48^3, 128^3 and 256^3, tol 1e-9, against the FP64
+// form and against a solve to 1e-13).  CG's FP32 iterates follow the FP64
+// ones, so theta = 1 gives the FP64 diagonal to 1.1e-9 .. 3.9e-9; a tighter
+// target moves the mixed solution towards the exact one and so away from
+// the FP64 form's, whose own truncation error is 4e-9 .. 4e-8.  BiCGStab's
+// FP64 diagonal lies 1e-7 .. 4e-7 from the exact one, and theta = 0.1 puts
+// the mixed diagonal ten times closer to it (10% more iterations).  FP16
+// storage of r and p leaves the FP64 path (9e-8 at theta = 1, 256^3);
+// theta = 0.1 puts it nearer the exact diagonal than the FP64 form
+// (1.3e-8 against 4.2e-8 at 256^3, 14% more iterations).
 static double default_theta(int solver) {
 	switch (solver) {
 	case 2: return SEDI_MIXED_THETA_CG;
@@ -1920,14 +1938,7 @@ int batched_alloc(Ctx *c) {
 		c->error = "FP16 Krylov storage is implemented for CG";
 		return SEDI_ERR_UNSUPPORTED;
 	}
-	if (B->mixed && c->solver == SEDI_PIPELINED_CG && c->g.n < kMixedPcgMinPoints) {
-		// On a few hundred unknowns the FP32 pipelined recurrences converge
-		// exactly within a few steps and then lose the residual faster than
-		// reliable updates restore it (5x7x9 at tol 1e-10 did not reach tol
-		// in 2,000 iterations); such grids take the FP64 form.
-		c->error = "mixed-precision pipelined CG needs at least 4096 grid points; use the FP64 form";
-		return SEDI_ERR_UNSUPPORTED;
-	}
+	B->ks = kernel_solver(c->solver, B->mixed);
 	if (c->batch > (B->mixed ? 256 : 128)) {
 		c->error = "batch too large for one context (max 256 FP32 / 128 FP64 right-hand sides)";
 		return SEDI_ERR_ARG;
@@ -1945,7 +1956,7 @@ int batched_alloc(Ctx *c) {
 	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
 	B->tuned = tu;
 	if (tu.period > 0) B->period = tu.period;
-	B->theta = default_theta(c->solver);
+	B->theta = B->half ? SEDI_MIXED_THETA_FP16 : default_theta(B->ks);
 	if (tu.chunk > 0) B->chunk = tu.chunk;
 	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
 	shape(c->g, B->R, B->rbT, ebT, &B->gT1, &B->gridT1, tu.nz, 1, tu.pfd);
@@ -1974,11 +1985,11 @@ int batched_alloc(Ctx *c) {
 		c->error = "device allocation failed (batched form)";
 		return SEDI_ERR_NOMEM;
 	}
-	if (c->solver == 3 || c->solver == 1) {
+	if (B->ks == 3 || B->ks == 1) {
 		void **pcg[] = {&B->w[0], &B->w[1], &B->u, &B->q, &B->sv, &B->z};
 		void **bicg[] = {&B->r1, &B->v[0], &B->v[1], &B->rhat};
-		void ***pv = c->solver == 3 ? pcg : bicg;
-		const int np = c->solver == 3 ? 6 : 4;
+		void ***pv = B->ks == 3 ? pcg : bicg;
+		const int np = B->ks == 3 ? 6 : 4;
 		for (int i = 0; i < np; i++) {
 			if (cudaMalloc(pv[i], B->elems * ts) != cudaSuccess) {
 				cudaGetLastError();
@@ -2025,11 +2036,11 @@ int batched_alloc(Ctx *c) {
 		         make_map(&M.m[MT_P1_HALO], B->p1, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_X_INT], B->x, ebT, c->g, R, B->rbT, Q1, Q2) &&
 		         make_map(&M.m[MT_R_INT], B->r, ebT, c->g, R, B->rbT, Q1, Q2);
-		if (c->solver == 3)
+		if (B->ks == 3)
 			k = k && make_map(&M.m[MT_W0_HALO], B->w[0], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_W1_HALO], B->w[1], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_Q_HALO], B->q, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2);
-		if (c->solver == 1)
+		if (B->ks == 1)
 			k = k && make_map(&M.m[MT_R1_HALO], B->r1, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_V0_HALO], B->v[0], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_V1_HALO], B->v[1], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2);
@@ -2077,7 +2088,8 @@ size_t batched_bytes(int solver, int precision, int batch, long long n1, long lo
 	size_t nblk = nblkT > nblkD ? nblkT : nblkD;
 	if (nblkT1 > nblk) nblk = nblkT1;
 	auto up = [](size_t b) { return (b + (2u << 20) - 1) / (2u << 20) * (2u << 20); };
-	const int nT = 3 + (solver == 3 ? 6 : 0) + (solver == 1 ? 4 : 0);  // r, p0, p1 and the solver's own
+	const int ks = kernel_solver(solver, mixed);
+	const int nT = 3 + (ks == 3 ? 6 : 0) + (ks == 1 ? 4 : 0);  // r, p0, p1 and the solver's own
 	size_t total = nT * up(elems * ts) + up(elems * xs) + up(elems * 8) * (mixed ? 2 : 1);
 	total += up(sizeof(double) * nblk * kMaxDots * R) + 3 * up(1) + up(sizeof(double) * kLaneDoubles * R) +
 	         up(sizeof(int) * 5 * R) + 2 * up(sizeof(double) * g.n);
@@ -2121,7 +2133,7 @@ void batched_free(Ctx *c) {
 
 template <int RBD, bool PAIRS = false>
 static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
-	const int pcg = c->solver == 3 ? 1 : 0;
+	const int pcg = B->ks == 3 ? 1 : 0;
 	typedef typename CfgFor<double, RBD, 0, PAIRS>::type CD;
 	cudaStream_t s = c->stream;
 	if (B->mixed) {
@@ -2136,7 +2148,7 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 		op.WT = B->rbT;
 		op.npts = c->g.n;
 		op.iMd = 1.0 / c->k.a;
-		op.solver = c->solver;
+		op.solver = B->ks;
 		op.ru = ru ? 1 : 0;
 		op.pcg = pcg;
 		launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, s);
@@ -2152,7 +2164,7 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 		op.WT = B->rbT;
 		op.npts = c->g.n;
 		op.iMd = 1.0 / c->k.a;
-		op.solver = c->solver;
+		op.solver = B->ks;
 		op.ru = 0;
 		op.pcg = pcg;
 		launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, s);
@@ -2186,7 +2198,7 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
 		                                                                 (float *)B->x, B->ls.pending,
-		                                                                 c->solver == 3 ? 1 : 0, B->gl);
+		                                                                 B->ks == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD, PAIRS>(c, B, true);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
@@ -2241,7 +2253,7 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
 		                                                                 (float *)B->x, B->ls.pending,
-		                                                                 c->solver == 3 ? 1 : 0, B->gl);
+		                                                                 B->ks == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD, PAIRS>(c, B, true);
 		OpApply<T> a1;
@@ -2306,7 +2318,7 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
 		                                                                 (float *)B->x, B->ls.pending,
-		                                                                 c->solver == 3 ? 1 : 0, B->gl);
+		                                                                 B->ks == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD, PAIRS>(c, B, true);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
@@ -2337,7 +2349,7 @@ struct Impl {
 		enqueue_resid<RBD, PAIRS>(c, B, false);
 		kb_setup_done<<<1, 1, 0, s>>>(B->gl);
 		c->launches++;
-		if (c->solver == 3) enqueue_pcg_uw<T, RBT, PAIRS>(c, B, 1, 0);  // :138-149 (skipped when no lane is live)
+		if (B->ks == 3) enqueue_pcg_uw<T, RBT, PAIRS>(c, B, 1, 0);  // :138-149 (skipped when no lane is live)
 		BTRY(cudaGetLastError());
 		return 0;
 	}
@@ -2349,8 +2361,8 @@ struct Impl {
 			const long long before = c->launches;
 			BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
 			for (int i = 0; i < B->chunk; i++) {
-				if (c->solver == 3) enqueue_pcg_iteration<T, RBT, RBD, PAIRS>(c, B);
-				else if (c->solver == 1) enqueue_bicg_iteration<T, RBT, RBD, PAIRS>(c, B);
+				if (B->ks == 3) enqueue_pcg_iteration<T, RBT, RBD, PAIRS>(c, B);
+				else if (B->ks == 1) enqueue_bicg_iteration<T, RBT, RBD, PAIRS>(c, B);
 				else enqueue_cg_iteration<T, RBT, RBD, PAIRS>(c, B);
 			}
 			BTRY(cudaStreamEndCapture(s, &graph));
@@ -2515,6 +2527,7 @@ int pairs_alloc(Ctx *c) {
 	Batched *B = new (std::nothrow) Batched();
 	if (!B) return SEDI_ERR_NOMEM;
 	B->pairs = B->aliased = true;
+	B->ks = c->solver;
 	B->R = 2;
 	B->rbT = B->rbD = 2;
 	B->elems = (size_t)c->g.n;
@@ -2573,11 +2586,11 @@ int pairs_alloc(Ctx *c) {
 		         make_map(&M.m[MT_P1_HALO], B->p1, 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_X_INT], B->x, 8, g, 2, 2, Q1, Q2) &&
 		         make_map(&M.m[MT_R_INT], B->r, 8, g, 2, 2, Q1, Q2);
-		if (c->solver == 3)
+		if (B->ks == 3)
 			k = k && make_map(&M.m[MT_W0_HALO], B->w[0], 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_W1_HALO], B->w[1], 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_Q_HALO], B->q, 8, g, 2, 2, Q1 + 2, Q2 + 2);
-		if (c->solver == 1)
+		if (B->ks == 1)
 			k = k && make_map(&M.m[MT_R1_HALO], B->r1, 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_V0_HALO], B->v[0], 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_V1_HALO], B->v[1], 8, g, 2, 2, Q1 + 2, Q2 + 2);
@@ -2697,7 +2710,7 @@ static int process_lanes(Ctx *c, Batched *B, int nrhs, int maxiter, double tol, 
 	const double *lm = B->lane_host;
 	const int *lint = B->lane_host_int;
 	auto at = [&](const double *dev, int j) { return lm[(size_t)(dev - B->lane_mem) + j]; };
-	const bool bicg = c->solver == 1 && !B->mixed;
+	const bool bicg = B->ks == 1 && !B->mixed;
 	int worst = 0;
 	for (int j = 0; j < nrhs; j++) {
 		LaneOut l;
@@ -2817,7 +2830,7 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 	BTRY(cudaEventCreate(&e0));
 	BTRY(cudaEventCreate(&e1));
 	const double ts = (double)sizeof(T) * (double)B->elems;
-	if (c->solver == 3) {
+	if (B->ks == 3) {
 		OpPcg<T> o;
 		o.ka = (T)c->k.a;
 		o.kb = (T)c->k.b;
@@ -2849,7 +2862,7 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		BTRY(cudaGetLastError());
 		return 0;
 	}
-	if (c->solver == 1) {
+	if (B->ks == 1) {
 		const T ka = (T)c->k.a, kb = (T)c->k.b, kc = (T)c->k.c, iMc = (T)(1.0 / c->k.a);
 		OpBicg1<T> o1;
 		o1.ka = ka;

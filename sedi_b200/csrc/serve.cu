@@ -285,8 +285,6 @@ long sedi_server_submit(sedi_server *S, int solver, int precision, long n1, long
 	    (precision == SEDI_PREC_MIXED16 && solver != SEDI_CG) || n1 < 1 ||
 	    n2 < 1 || n3 < 1 || samples < 0 || maxiter < 0 || !(tol >= 0.0))
 		return SEDI_ERR_ARG;
-	if (precision != SEDI_PREC_FP64 && solver == SEDI_PIPELINED_CG && (double)n1 * n2 * n3 < 4096.0)
-		return SEDI_ERR_UNSUPPORTED;  // the mixed pipelined CG's smallest grid (see sedi_create)
 	Job J;
 	J.id = S->next_id++;
 	J.key.solver = solver;

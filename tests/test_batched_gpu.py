@@ -241,24 +241,62 @@ def test_mixed_batch_bicgstab_true_residual(nrhs, tol):
     assert fi[0] <= fi64 * 1.5 + 10
 
 
-def test_mixed_bicgstab_estimator_diagonal_error():
-    """BiCGStab does not minimise an error norm, so two solves that both meet
-    tol land further apart than CG's: the bar is 1e-7 (the reference's own
-    BiCGStab D moves by 2e-7 between two floating-point contractions of the
-    same source at 128^3)."""
-    dims = (32, 32, 32)
+@pytest.mark.parametrize("dims", [(32, 32, 32), (48, 48, 48)])
+def test_mixed_bicgstab_closer_to_converged_diagonal_than_fp64(dims):
+    """BiCGStab's diagonal at tol 1e-9 is not reproducible to 1e-8 in any
+    precision: the FP64 form lies 1e-7 .. 4e-7 from the converged diagonal
+    (and two compilations of the reference differ by 2e-7).  The mixed lanes
+    stop on their FP64 true residual at 0.1 tol, which puts their diagonal
+    within 2e-8 of the converged one (FP64 CG to 1e-13 on the same probes),
+    several times closer than the FP64 form's."""
     samples = 16
+    with S.Context("cg", dims, batch=samples) as cx:
+        ex = cx.estimate(samples, 1234, 5000, 1e-13)
     with S.Context("bicgstab", dims, batch=samples) as c64:
         r64 = c64.estimate(samples, 1234, 3000, 1e-9)
     with S.Context("bicgstab", dims, precision=S.MIXED, batch=samples) as cm:
+        assert cm.mixed_target == 0.1
         rm = cm.estimate(samples, 1234, 3000, 1e-9)
     assert np.all(rm["results"] == 0)
-    assert O.relmax(rm["D"], r64["D"]) <= 1e-7, O.relmax(rm["D"], r64["D"])
+    e_mixed, e_fp64 = O.relmax(rm["D"], ex["D"]), O.relmax(r64["D"], ex["D"])
+    assert e_mixed <= 2e-8 and e_mixed <= 0.5 * e_fp64, (e_mixed, e_fp64)
 
 
-@pytest.mark.parametrize("solver,nk", [("cg", 2), ("pcg", 1), ("bicgstab", 3)])
-def test_time_kernels_lists_solver_sweeps(solver, nk):
-    with S.Context(solver, (64, 64, 64), precision=S.MIXED, batch=16) as c:
+@pytest.mark.parametrize("solver", ["cg", "pcg"])
+def test_mixed_estimator_within_1e8_of_fp64_48cube(solver):
+    """Diagonal error of the mixed form against the FP64 form on the same 32
+    probes, 48^3, tol 1e-9: <= 1e-8 relative max-norm (the mixed pipelined CG
+    runs the CG recurrence, whose FP32 iterates follow the FP64 ones)."""
+    dims, samples = (48, 48, 48), 32
+    with S.Context(solver, dims, batch=samples) as c64:
+        r64 = c64.estimate(samples, 4321, 5000, 1e-9)
+    with S.Context(solver, dims, precision=S.MIXED, batch=samples) as cm:
+        assert cm.mixed_target == 1.0
+        rm = cm.estimate(samples, 4321, 5000, 1e-9)
+    assert np.all(rm["results"] == 0) and np.all(r64["results"] == 0)
+    assert np.array_equal(rm["q"], r64["q"])
+    assert O.relmax(rm["D"], r64["D"]) <= 1e-8, O.relmax(rm["D"], r64["D"])
+
+
+@pytest.mark.parametrize("solver", ["cg", "pcg"])
+def test_mixed_estimator_within_1e8_of_fp64_256cube(solver):
+    """The batched mixed configuration's grid (256^3, tol 1e-9) with 32 of its
+    128 probes: D of the mixed form within 1e-8 of the FP64 form's."""
+    dims, samples = (256, 256, 256), 32
+    with S.Context(solver, dims, batch=samples) as c64:
+        r64 = c64.estimate(samples, 1234, 20000, 1e-9)
+    with S.Context(solver, dims, precision=S.MIXED, batch=samples) as cm:
+        rm = cm.estimate(samples, 1234, 20000, 1e-9)
+    assert np.all(rm["results"] == 0) and np.all(r64["results"] == 0)
+    assert O.relmax(rm["D"], r64["D"]) <= 1e-8, O.relmax(rm["D"], r64["D"])
+
+
+@pytest.mark.parametrize("solver,prec,nk", [("cg", S.MIXED, 2), ("pcg", S.MIXED, 2), ("bicgstab", S.MIXED, 3),
+                                            ("pcg", S.FP64, 1)])
+def test_time_kernels_lists_solver_sweeps(solver, prec, nk):
+    """Per-iteration sweeps: CG 2, BiCGStab 3, pipelined CG 1 in FP64 (its
+    mixed form runs the CG recurrence: 2)."""
+    with S.Context(solver, (64, 64, 64), precision=prec, batch=16) as c:
         ks = c.time_kernels(reps=2)
     assert len(ks) == nk and all(ms > 0 and by > 0 for _, ms, by in ks)
 
@@ -268,8 +306,8 @@ def test_autotuned_context_keeps_results(solver, prec):
     """The autotuner's choices (slice width, i3 split, graph chunk, reliable-update
     period) change only launch shapes and summation order: FP64 CG/PCG stay
     within 1e-10 of the untuned run with the same iteration counts, BiCGStab
-    FP64 within its 20-iteration bar, mixed CG within 1e-8 of FP64 (pipelined
-    CG 3e-8)."""
+    FP64 within its 20-iteration bar, mixed CG and pipelined CG within 1e-8
+    of FP64."""
     dims, samples = (40, 36, 48), 16
     maxiter, tol = (20, 0.0) if solver == "bicgstab" else (3000, 1e-9)
     with S.Context(solver, dims, precision=prec, batch=samples) as c:
@@ -288,11 +326,8 @@ def test_autotuned_context_keeps_results(solver, prec):
         assert 20 <= after["period"] <= 50
         with S.Context(solver, dims, precision=S.FP64, batch=samples) as c64:
             r64 = c64.estimate(samples, 321, maxiter, tol, ignore_errors=True)
-        # Pipelined CG's runs meeting tol 1e-9 stop anywhere below it; the D
-        # of two such runs differs by up to a few 1e-8 here.
-        bar = 1e-8 if solver == "cg" else 3e-8
-        assert O.relmax(got["D"], r64["D"]) <= bar
-        assert O.relmax(ref["D"], r64["D"]) <= bar
+        assert O.relmax(got["D"], r64["D"]) <= 1e-8
+        assert O.relmax(ref["D"], r64["D"]) <= 1e-8
     else:
         assert np.array_equal(got["iters"], ref["iters"]) and np.array_equal(got["results"], ref["results"])
         assert O.relmax(got["D"], ref["D"]) <= 1e-10

@@ -63,12 +63,12 @@ def test_fp64_batched_bicgstab_nonsymmetric():
 
 
 @pytest.mark.parametrize("dims", [(5, 7, 9), (1, 13, 1), (33, 17, 9), (2, 2, 40), (1, 1, 1)])
-@pytest.mark.parametrize("solver", ["cg", "bicgstab"])
+@pytest.mark.parametrize("solver", ["cg", "pcg", "bicgstab"])
 def test_mixed_batched_odd_shapes_true_residual(dims, solver):
     """Tiny systems converge exactly within a few FP32 steps; the recurrence
     then divides 0 by 0 or drifts far below the true residual.  Such lanes
     hold, take a reliable update and restart, and still stop on their FP64
-    true residual.  (The mixed pipelined CG is covered from 20x18x16 up.)"""
+    true residual.  (The mixed pipelined CG runs the CG recurrence.)"""
     B = _probes(dims, 6, 970)
     X = np.zeros_like(B)
     with S.Context(solver, dims, precision=S.MIXED, batch=6) as c:
@@ -78,24 +78,3 @@ def test_mixed_batched_odd_shapes_true_residual(dims, solver):
         r = B[k] - O.stencil(dims, X[k])
         assert np.sqrt((r @ r) / (B[k] @ B[k])) <= 1e-10 * 1.0000001
 
-
-def test_mixed_pcg_refuses_grids_below_4096_points():
-    """The mixed pipelined CG does not reach tol on a few hundred unknowns; it
-    is refused there (the FP64 form covers every grid) and runs from 16^3 up."""
-    for dims in ((5, 7, 9), (15, 16, 17)):
-        with pytest.raises(S.SediError) as e:
-            S.Context("pcg", dims, precision=S.MIXED, batch=4)
-        assert e.value.code == -5
-    with S.Server() as srv:
-        with pytest.raises(S.SediError) as e:
-            srv.submit("pcg", (5, 7, 9), 4, 1, 100, 1e-9, precision=S.MIXED)
-        assert e.value.code == -5
-    dims = (16, 16, 16)
-    B = _probes(dims, 6, 990)
-    X = np.zeros_like(B)
-    with S.Context("pcg", dims, precision=S.MIXED, batch=6) as c:
-        res, fe, fi = c.solve_batch(X, B, maxiter=3000, tol=1e-10)
-    assert np.all(res == 0)
-    for k in range(6):
-        r = B[k] - O.stencil(dims, X[k])
-        assert np.sqrt((r @ r) / (B[k] @ B[k])) <= 1e-10 * 1.0000001

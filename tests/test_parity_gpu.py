@@ -48,8 +48,10 @@ def test_fixed_iterations_match_oracle(solver, K):
         hist = c.history()
     assert (rc, fi) == (rc0, fi0)
     assert O.relmax(x, x0) <= 1e-10
-    # final_err: relative 1e-10 (1e-8 for BiCGStab) above an absolute 1e-15 floor.
-    assert abs(fe - fe0) <= (1e-10 if solver != "bicgstab" else 1e-8) * fe0 + 1e-15
+    # final_err: relative 1e-10 (1e-8 for BiCGStab) above an absolute 1e-14
+    # floor (after 200 iterations the residual is rounding noise, ~4e-15,
+    # whose digits depend on the dot products' summation order).
+    assert abs(fe - fe0) <= (1e-10 if solver != "bicgstab" else 1e-8) * fe0 + 1e-14
     assert len(hist) == K + 1
     assert O.relmax(hist[: min(K, 40) + 1], h0[: min(K, 40) + 1]) <= 1e-10
 
@@ -150,11 +152,15 @@ def test_vector_preconditioner_matches_constant_and_oracle():
     iM_var = 1.0 / (6.0 + rng.random(n))
     for solver in ("cg", "pcg", "bicgstab"):
         with _ctx(solver, dims) as c:
+            # iM = NULL runs the streaming sweeps (n1 even), a vector iM the
+            # column-march kernels: same elementwise rounding, dot products
+            # summed in another order.
             x1 = np.zeros(n)
             r1 = c.solve(x1, b, None, 30, 0.0)
             x2 = np.zeros(n)
             r2 = c.solve(x2, b, iM_const, 30, 0.0)
-            assert r1 == r2 and np.array_equal(x1, x2)
+            assert r1[0] == r2[0] and r1[2] == r2[2] and abs(r1[1] - r2[1]) <= 1e-10 * r2[1]
+            assert O.relmax(x1, x2) <= 1e-12 if solver != "bicgstab" else O.relmax(x1, x2) <= 1e-10
             x3 = np.zeros(n)
             rc, fe, fi = c.solve(x3, b, iM_var, 25 if solver != "bicgstab" else 12, 0.0)
         rc0, fe0, fi0, x0, _ = O.solve(SOLVERS[solver], dims, b, iM=iM_var, maxiter=25 if solver != "bicgstab" else 12,
