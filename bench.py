@@ -74,9 +74,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["sedi", "reference"], default="sedi")
-    ap.add_argument("--workload", choices=["batched256", "dropin", "large512"], default="batched256",
+    ap.add_argument("--workload", choices=["batched256", "dropin", "large512", "accuracy"], default="batched256",
                     help="batched256: the benchmark line (256^3 x 128 probes, mixed CG); dropin: 128^3 x 64 "
-                         "probes; large512: the 512^3 x 16-probe pipelined-CG configuration (one JSON line)")
+                         "probes; large512: the 512^3 x 16-probe pipelined-CG configuration (one JSON line); "
+                         "accuracy: diagonal error of the mixed forms per in-loop target (JSON lines)")
     ap.add_argument("--form", choices=["mixed", "mixed16", "fp64", "plain"], default=None,
                     help="mixed / mixed16 / fp64: batched forms; plain: the single-vector FP64 form (profiling "
                          "cases)")
@@ -486,6 +487,39 @@ def run_large512(S, args):
     print(json.dumps(out), flush=True)
 
 
+def run_accuracy(S, args):
+    """Diagonal error of the mixed forms against the FP64 form on the same
+    probes and against the converged diagonal (FP64 CG to 1e-13), per in-loop
+    target theta, tol 1e-9: 48^3 and 128^3 x 64 probes (every solver),
+    256^3 x 32 probes (CG, pipelined CG).  One JSON line per grid and solver."""
+    import numpy as np
+
+    def est(solver, g, k, tol, prec, theta=None):
+        with S.Context(solver, g, precision=prec, batch=k) as c:
+            if theta is not None:
+                c.mixed_target = theta
+            t0 = time.perf_counter()
+            r = c.estimate(k, SEED, 20000, tol)
+            return r, time.perf_counter() - t0
+
+    for g, k, solvers in (((48, 48, 48), 64, ("cg", "pcg", "bicgstab")),
+                          ((128, 128, 128), 64, ("cg", "pcg", "bicgstab")), ((256, 256, 256), 32, ("cg", "pcg"))):
+        ex, _ = est("cg", g, k, 1e-13, S.FP64)
+        for solver in solvers:
+            r64, dt64 = est(solver, g, k, 1e-9, S.FP64)
+            row = {"grid": list(g), "probes": k, "solver": solver, "fp64_vs_converged": _relmax(r64["D"], ex["D"]),
+                   "fp64_iterations": float(r64["iters"].mean()), "fp64_s": dt64, "mixed": []}
+            forms = [("mixed", S.MIXED)] + ([("mixed16", S.MIXED16)] if solver == "cg" else [])
+            for name, prec in forms:
+                for th in (1.0, 0.3, 0.1, 0.03):
+                    rm, dtm = est(solver, g, k, 1e-9, prec, th)
+                    row["mixed"].append({"form": name, "theta": th, "vs_fp64": _relmax(rm["D"], r64["D"]),
+                                         "vs_converged": _relmax(rm["D"], ex["D"]),
+                                         "iterations": float(rm["iters"].mean()), "s": dtm,
+                                         "results_nonzero": int(np.count_nonzero(rm["results"]))})
+            print(json.dumps(row), flush=True)
+
+
 def traffic_per_launch(kernel, grid, lanes):
     """DRAM bytes per launch of `kernel` at this size, from the committed ncu
     summary (profiles/ncu_traffic.txt lines '<kernel> <n1>x<n2>x<n3> <lanes>
@@ -517,9 +551,9 @@ def run_sedi(args):
 
     rank, world, local = dist_env()
     wl = args.wl
-    if args.workload == "large512":
+    if args.workload in ("large512", "accuracy"):
         if rank == 0:
-            run_large512(S, args)
+            (run_large512 if args.workload == "large512" else run_accuracy)(S, args)
         return
     if args.serve_only:
         if rank == 0:
