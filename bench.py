@@ -60,12 +60,9 @@ WORKLOADS = {
 }
 # Compulsory bytes per point, lane and iteration (x, r, p read and written once)
 # of CG: FP32 Krylov words for the mixed form, FP64 for the others.
-CG_BYTES = {"mixed": 24, "mixed16": 16, "fp64": 48, "plain": 48}
+CG_BYTES = {"mixed": 24, "fp64": 48, "plain": 48}
 # Arithmetic of each form (the JSON line's dtype).
-DTYPES = {"mixed": "f32 vectors / f64 reductions+reliable update",
-          "mixed16": "f16 storage of r, p (per-lane power-of-two scales) / f32 arithmetic and x / "
-                     "f64 reductions+reliable update",
-          "fp64": "f64", "plain": "f64"}
+DTYPES = {"mixed": "f32 vectors / f64 reductions+reliable update", "fp64": "f64", "plain": "f64"}
 
 
 def parse():
@@ -78,9 +75,8 @@ def parse():
                     help="batched256: the benchmark line (256^3 x 128 probes, mixed CG); dropin: 128^3 x 64 "
                          "probes; large512: the 512^3 x 16-probe pipelined-CG configuration (one JSON line); "
                          "accuracy: diagonal error of the mixed forms per in-loop target (JSON lines)")
-    ap.add_argument("--form", choices=["mixed", "mixed16", "fp64", "plain"], default=None,
-                    help="mixed / mixed16 / fp64: batched forms; plain: the single-vector FP64 form (profiling "
-                         "cases)")
+    ap.add_argument("--form", choices=["mixed", "fp64", "plain"], default=None,
+                    help="mixed / fp64: batched forms; plain: the single-vector FP64 form (profiling cases)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     # Small cases for profiler captures (not the benchmark configuration):
     ap.add_argument("--grid", default=None, help="override the grid, e.g. 128x128x64")
@@ -509,8 +505,7 @@ def run_accuracy(S, args):
             r64, dt64 = est(solver, g, k, 1e-9, S.FP64)
             row = {"grid": list(g), "probes": k, "solver": solver, "fp64_vs_converged": _relmax(r64["D"], ex["D"]),
                    "fp64_iterations": float(r64["iters"].mean()), "fp64_s": dt64, "mixed": []}
-            forms = [("mixed", S.MIXED)] + ([("mixed16", S.MIXED16)] if solver == "cg" else [])
-            for name, prec in forms:
+            for name, prec in (("mixed", S.MIXED),):
                 for th in (1.0, 0.3, 0.1, 0.03):
                     rm, dtm = est(solver, g, k, 1e-9, prec, th)
                     row["mixed"].append({"form": name, "theta": th, "vs_fp64": _relmax(rm["D"], r64["D"]),
@@ -568,7 +563,7 @@ def run_sedi(args):
     dev = torch.device("cuda", torch.cuda.current_device())
     n = GRID[0] * GRID[1] * GRID[2]
     stream = torch.cuda.current_stream()
-    prec = {"mixed": S.MIXED, "mixed16": S.MIXED16}.get(form, S.FP64)
+    prec = S.MIXED if form == "mixed" else S.FP64
     batch = 1 if form == "plain" else SAMPLES
     peak, peak_src = _peak()
 
@@ -670,7 +665,7 @@ def run_sedi(args):
         # against the compulsory bytes of CG (x, r, p read and written).
         kern = ctx.time_kernels(reps=10) if form != "plain" else []
         ctx_config = ctx.config() if form != "plain" else None
-        theta = ctx.mixed_target if form in ("mixed", "mixed16") else None
+        theta = ctx.mixed_target if form == "mixed" else None
         roofline = None
         if kern:
             dom = max(kern, key=lambda k: k[1])
@@ -689,7 +684,7 @@ def run_sedi(args):
         ctx.close()
         acc = {}
         forms = {}
-        if world == 1 and form in ("mixed", "mixed16"):
+        if world == 1 and form == "mixed":
             # The FP64 batched form on the same probes (two halves of the lanes:
             # t and q add up exactly), and the plain single-vector FP64 form.
             half = SAMPLES // 2
@@ -729,24 +724,6 @@ def run_sedi(args):
                     pass
             forms["mixed_vs_plain_fp64"] = value / forms["plain_fp64_single_vector"]
             forms["mixed_vs_batched_fp64"] = value / forms["batched_fp64"]
-            # The other mixed form on the same probes (FP32 or FP16 storage of r and p).
-            if solver == "cg":
-                other = "mixed16" if form == "mixed" else "mixed"
-                oprec = S.MIXED16 if other == "mixed16" else S.MIXED
-                with S.Context(solver, GRID, precision=oprec, batch=SAMPLES) as co:
-                    co.set_stream(stream)
-                    torch.cuda.synchronize()
-                    a = time.perf_counter()
-                    ro = co.estimate_dev(SAMPLES, probes, D, maxiter=MAXITER, tol=TOL)
-                    torch.cuda.synchronize()
-                    dt_o = time.perf_counter() - a
-                    forms[other] = {"probe_solves_per_s": SAMPLES / dt_o,
-                                    "D_rel_err_vs_batched_fp64": _relmax(D.cpu().numpy(), d64),
-                                    "iterations": [int(ro["iters"].min()), int(ro["iters"].max())],
-                                    "results_nonzero": int(np.count_nonzero(ro["results"])),
-                                    "kernels": [{"kernel": k, "ms": ms_, "GB/s": by / ms_ / 1e6,
-                                                 "frac": by / ms_ / 1e6 / peak}
-                                                for k, ms_, by in co.time_kernels(reps=5)]}
             # The reference's own converged run of probes 0..7 on this grid.
             if tuple(GRID) == (256, 256, 256) and os.path.exists(BIG_FIXTURE):
                 z = np.load(BIG_FIXTURE)

@@ -47,9 +47,6 @@ extern "C" {
 /* Arithmetic forms. */
 #define SEDI_PREC_FP64 0  /* the reference method in FP64, kernel by kernel */
 #define SEDI_PREC_MIXED 1 /* FP32 Krylov vectors, FP64 reductions, FP64 reliable update of x and r */
-/* As SEDI_PREC_MIXED with r and p stored in FP16 (per-lane power-of-two
- * scales, FP32 arithmetic, FP32 x correction); CG only. */
-#define SEDI_PREC_MIXED16 2
 
 /* Reference result_t values. */
 #define SEDI_SOLUTION_FOUND 0
@@ -78,10 +75,9 @@ typedef struct sedi_ctx sedi_ctx;
  *   n1,n2,n3   grid (every dimension >= 1)
  *   a,b,c      stencil coefficients: y = a*x_c - c*(x_{i-1}+...) - b*(x_{i+1}+...)
  *   mode       SEDI_MODE_* bits (accepted, no effect on one GPU)
- *   precision  SEDI_PREC_FP64, SEDI_PREC_MIXED or SEDI_PREC_MIXED16 (CG only;
- *              SEDI_ERR_UNSUPPORTED for the other solvers).  The mixed
- *              forms of CG and pipelined CG run the CG recurrence (one GPU
- *              has no reduction latency for pipelining to hide; see
+ *   precision  SEDI_PREC_FP64 or SEDI_PREC_MIXED.  The mixed forms of CG
+ *              and pipelined CG run the CG recurrence (one GPU has no
+ *              reduction latency for pipelining to hide; see
  *              sedi_set_mixed_target for their accuracy).
  *   batch      right-hand sides in flight per launch (1 = single-vector form)
  *   err        out: 0 or a negative SEDI_ERR_* (may be NULL)
@@ -151,8 +147,8 @@ int sedi_set_stream(sedi_ctx *ctx, void *stream);
  * of the Krylov vectors it streams), names (count*32 chars, NUL-terminated
  * slots).  The buffers' contents are scratch afterwards.  Returns 0 or error.
  * A single-vector FP64 context (batch 1) times its streaming sweeps (names
- * ending in _sv; SEDI_ERR_UNSUPPORTED when n1 is odd: those grids use the
- * column-march kernels).
+ * ending in _sv), which serve grids with n1 even and at least 2^22 points;
+ * SEDI_ERR_UNSUPPORTED for other grids, which use column-march kernels.
  */
 int sedi_time_kernels(sedi_ctx *ctx, int reps, double *ms, double *bytes, char *names, int *count);
 
@@ -273,8 +269,7 @@ sedi_server *sedi_server_create(double budget_bytes, int max_active, double job_
 void sedi_server_destroy(sedi_server *srv);
 
 /* Queue a job; returns its id (>= 0) or a negative error (SEDI_ERR_NOMEM
- * when even one batch of it exceeds the budget, SEDI_ERR_ARG for FP16
- * storage with another solver than CG). */
+ * when even one batch of it exceeds the budget). */
 long sedi_server_submit(sedi_server *srv, int solver, int precision, long n1, long n2, long n3, int samples,
                         uint32_t seed, int maxiter, double tol);
 
@@ -352,7 +347,7 @@ int sedi_set_tuning(int solver, int precision, int batch, long n1, long n2, long
  * 3.9e-9 at 256^3, tol 1e-9); BiCGStab's FP64 diagonal itself lies 1e-7
  * to 4e-7 from the converged answer at tol 1e-9, and theta = 0.1 puts the
  * mixed one ten times closer to it than that.  Defaults: CG and pipelined
- * CG 1, BiCGStab 0.1, FP16 storage 0.1 (sedi_mixed_target reads them).
+ * CG 1, BiCGStab 0.1 (sedi_mixed_target reads them).
  * SEDI_ERR_UNSUPPORTED for FP64 contexts, SEDI_ERR_ARG for theta outside (0, 1].
  */
 int sedi_set_mixed_target(sedi_ctx *ctx, double theta);

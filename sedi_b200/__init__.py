@@ -28,7 +28,7 @@ import numpy as np
 __all__ = [
     "SediError", "Stencil", "Cg", "PipelinedCg", "BiCgStab", "Context", "Server", "autotune", "set_tuning", "estimate",
     "fill_probe",
-    "job_bytes", "library_path", "load", "SOLVER_IDS", "FP64", "MIXED", "MIXED16",
+    "job_bytes", "library_path", "load", "SOLVER_IDS", "FP64", "MIXED",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -36,7 +36,7 @@ _LIB_PATH = os.path.join(_HERE, "_lib", "libsedi_b200.so")
 
 BICGSTAB, CG, PIPELINED_CG = 1, 2, 3
 SOLVER_IDS = {"bicgstab": BICGSTAB, "cg": CG, "pcg": PIPELINED_CG, "pipelined_cg": PIPELINED_CG}
-FP64, MIXED, MIXED16 = 0, 1, 2  # MIXED16: r and p stored in FP16 (CG)
+FP64, MIXED = 0, 1
 
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "device out of memory", -4: "no CUDA device",
           -5: "unsupported"}

@@ -52,7 +52,6 @@ struct LaneState {
 	double *bb, *rr, *err, *ru, *ru_new, *sp, *alpha, *beta;  // CG
 	double *gamma, *gamma_old, *delta, *rr_top;                 // pipelined CG
 	double *rho, *rho_prev, *omega, *s_norm2, *ts, *tt;         // BiCGStab
-	double *r_scale, *p_scale0, *p_scale1, *pp;                 // FP16 storage: field scales, <p,p>
 	int *done, *exit_iter, *reason, *pending, *s_exit;
 	double *hist;  // single-vector form: err after each iteration (lane 0), else null
 };
@@ -61,8 +60,7 @@ struct LaneState {
 // and carries the same scalars.
 __device__ __forceinline__ void mirror_lane0(const LaneState &ls) {
 	double *const d[] = {ls.bb, ls.rr, ls.err, ls.ru, ls.ru_new, ls.sp, ls.alpha, ls.beta, ls.gamma, ls.gamma_old,
-	                     ls.delta, ls.rr_top, ls.rho, ls.rho_prev, ls.omega, ls.s_norm2, ls.ts, ls.tt, ls.r_scale,
-	                     ls.p_scale0, ls.p_scale1, ls.pp};
+	                     ls.delta, ls.rr_top, ls.rho, ls.rho_prev, ls.omega, ls.s_norm2, ls.ts, ls.tt};
 	for (double *a : d) a[1] = a[0];
 	int *const n[] = {ls.done, ls.exit_iter, ls.reason, ls.pending, ls.s_exit};
 	for (int *a : n) a[1] = a[0];
@@ -164,19 +162,28 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 		hoff[k] = e < HALO * LG ? h * RB + lo : -1;
 		if (e < HALO * LG && gi1 >= 0 && gi1 < g.n1 && gi2 >= 0 && gi2 < g.n2) hval |= 1u << k;
 	}
+	// A thread's KO output points are KO consecutive rows of one column when
+	// the tile allows it (ROWS), so inside the group a point's i2 neighbour
+	// is another point's centre, already in registers.
+	constexpr bool ROWS = (NPS % P1 == 0) && (KO * NPS == INT);
 	int ooff[KO], qoff[KO];
 	long long obase[KO];
-	unsigned oval = 0;
+	unsigned oval = 0, oin = 0;
 #pragma unroll
 	for (int k = 0; k < KO; k++) {
-		const int q = ps + k * NPS;
+		const int q = ROWS ? (KO * (ps / P1) + k) * P1 + ps % P1 : ps + k * NPS;
 		const int q1 = q % P1, q2 = q / P1;
 		const int gi1 = i1_0 + q1, gi2 = i2_0 + q2;
 		ooff[k] = ((q2 + 1) * H1 + (q1 + 1)) * RB + lo;
 		qoff[k] = q * RB + lo;
 		obase[k] = (long long)gi2 * g.n1 + gi1;
+		if (q < INT) oin |= 1u << k;
 		if (q < INT && gi1 < g.n1 && gi2 < g.n2) oval |= 1u << k;
 	}
+	// Column centres of the stencil input at planes m-1, m, m+1 of the current
+	// output plane m: two of them were read one step earlier (the planes stay
+	// in the ring or the stages until then), so each step reads one new centre.
+	Vec<T> zprev[KO], zcur[KO], znext[KO];
 	const long long plane = (long long)g.n1 * g.n2;
 
 	if (t == 0) {
@@ -287,15 +294,27 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 			}
 #pragma unroll
 			for (int k = 0; k < KO; k++) {
+				if (!(oin >> k & 1u)) continue;
+				if (j > 3) {  // planes m-1 and m were planes m and m+1 of the previous step
+					zprev[k] = zcur[k];
+					zcur[k] = znext[k];
+				} else {
+					zprev[k] = zm ? lds(cm + ooff[k]) : vzero<T>();
+					zcur[k] = lds(c0 + ooff[k]);
+				}
+				znext[k] = zp ? lds(cp + ooff[k]) : vzero<T>();
+			}
+#pragma unroll
+			for (int k = 0; k < KO; k++) {
 				if (!(oval >> k & 1u)) continue;
 				const int hc = ooff[k];
-				const Vec<T> xc = lds(c0 + hc);
+				const Vec<T> &xc = zcur[k];
 				const Vec<T> xm1 = lds(c0 + hc - RB);
 				const Vec<T> xp1 = lds(c0 + hc + RB);
-				const Vec<T> xm2 = lds(c0 + hc - H1 * RB);
-				const Vec<T> xp2 = lds(c0 + hc + H1 * RB);
-				const Vec<T> xm3 = zm ? lds(cm + hc) : vzero<T>();
-				const Vec<T> xp3 = zp ? lds(cp + hc) : vzero<T>();
+				const Vec<T> xm2 = (ROWS && k > 0) ? zcur[k > 0 ? k - 1 : 0] : lds(c0 + hc - H1 * RB);
+				const Vec<T> xp2 = (ROWS && k + 1 < KO) ? zcur[k + 1 < KO ? k + 1 : k] : lds(c0 + hc + H1 * RB);
+				const Vec<T> &xm3 = zprev[k];
+				const Vec<T> &xp3 = znext[k];
 				Vec<T> y;
 				if (C::PAIRS) {
 					// Points 2m, 2m+1 of one vector: i1 neighbours across the pair.
@@ -1192,291 +1211,6 @@ struct OpBicg3 : OpBicgS<T> {
 	}
 };
 
-// ---------------------------------------------------------------------------
-// CG with FP16 storage of the Krylov fields r and p (mixed form, FP32
-// arithmetic, FP32 x_lo, FP64 reductions and reliable update).  A stored
-// value h of lane l means h * scale[l]; every scale is a power of two picked
-// from the lane's RMS (RMS / scale in [0.5, 1)), so scaling is exact and the
-// FP16 range (6e-5 .. 65504 at full precision) is centred on the field.  The
-// FP16 rounding of r and p (2^-11 relative) acts like the FP32 rounding of
-// the FP32 form, at a larger size; the FP64 reliable update bounds its effect
-// on the solution, and a lane still stops only on its FP64 true residual.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ float pow2_scale(double rms) {
-	if (!(rms > 0.0) || !isfinite(rms)) return 1.0f;
-	int e;
-	frexp(rms, &e);  // rms = m * 2^e, m in [0.5, 1)
-	e = e < -100 ? -100 : (e > 100 ? 100 : e);
-	return ldexpf(1.0f, e);
-}
-
-// p = u + beta p_old (u = r .* iM; p = u on iteration 1), s = A p, <s,p>,
-// <p,p> (next scale of p) and <r,u> on iteration 1 (Cg.hpp:150-166, :188).
-// The stencil input p is rounded to FP16 once, in the ring: the stored p and
-// the p that s = A p is computed from are the same values.
-struct OpCgAh : OpBase<float> {
-	static constexpr int KIND = 1;
-	static constexpr int NS = 2, NQ = 0, ND = 3;
-	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
-	static constexpr int V = 4;
-	float iMc;
-	double iMd;
-	long long npts;
-	__half *p0, *p1;
-	__half *pout;
-	int it;
-	bool first;
-	float beta[V], sr[V], spo[V], spn[V], ispn[V];
-	// Scale of the p written this iteration: an upper bound of its RMS by
-	// the triangle inequality, from <r,r> and the previous <p,p>.
-	__device__ static float p_scale(const LaneState &ls, int l, bool first, double iMd, long long n) {
-		double est = sqrt(ls.rr[l] / (double)n) * fabs(iMd);
-		if (!first) est += fabs(ls.beta[l]) * sqrt(ls.pp[l] / (double)n);
-		return pow2_scale(est);
-	}
-	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
-		it = gl->iter;
-		first = (it == 1);
-		pout = (it & 1) ? p1 : p0;
-		const double *so = (it & 1) ? ls.p_scale0 : ls.p_scale1;  // p_old is the other buffer
-#pragma unroll
-		for (int e = 0; e < V; e++) {
-			const int l = lane + e;
-			beta[e] = (float)ls.beta[l];
-			sr[e] = (float)ls.r_scale[l];
-			spo[e] = (float)so[l];
-			spn[e] = p_scale(ls, l, first, iMd, npts);
-			ispn[e] = 1.0f / spn[e];
-		}
-	}
-	__device__ bool raw_center() const { return first; }
-	__device__ int src_map(int s) const { return s == 0 ? MT_R_HALO : ((it & 1) ? MT_P0_HALO : MT_P1_HALO); }
-	__device__ int q_map(int) const { return 0; }
-	__device__ Vec<float> src(const Vec<float> *raw) const {
-		Vec<float> o;
-#pragma unroll
-		for (int e = 0; e < V; e++) {
-			const float u = (raw[0].v[e] * sr[e]) * iMc;
-			o.v[e] = (first ? u : u + beta[e] * (raw[1].v[e] * spo[e])) * ispn[e];
-		}
-		return o;
-	}
-	__device__ void out(long long o, long long, int, const Vec<float> &pc, const Vec<float> &s, const Vec<float> *,
-	                    const Vec<float> *rc, const Vec<float> *, double (&part)[ND][V]) const {
-		stg(pout + o, pc);  // FP16 values of the ring: stored exactly
-#pragma unroll
-		for (int e = 0; e < V; e++) {
-			const float pt = pc.v[e] * spn[e], st = s.v[e] * spn[e];
-			dacc(part[0][e], st, pt);
-			dacc(part[2][e], pt, pt);
-		}
-		if (first) {
-#pragma unroll
-			for (int e = 0; e < V; e++) {
-				const float r = rc[0].v[e] * sr[e];
-				dacc(part[1][e], r, r * iMc);
-			}
-		}
-	}
-	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
-		double *sn = (it & 1) ? ls.p_scale1 : ls.p_scale0;
-		sn[lane] = p_scale(ls, lane, first, iMd, npts);  // before <p,p> is replaced
-		ls.pp[lane] = tot[2];
-		if (ls.done[lane]) {
-			ls.alpha[lane] = 0.0;
-			return;
-		}
-		ls.sp[lane] = tot[0];
-		const double ru = first ? tot[1] : ls.ru_new[lane];
-		ls.ru[lane] = ru;
-		const double al = __ddiv_rn(ru, tot[0]);
-		if (!(tot[0] > 0.0 && isfinite(al))) {  // breakdown: restart after a reliable update (as OpCgA)
-			ls.alpha[lane] = 0.0;
-			ls.pending[lane] = 1;
-			ls.s_exit[lane] = 2;
-			gl->ru_due = 1;
-			return;
-		}
-		ls.alpha[lane] = al;
-	}
-};
-
-// s = A p, x += alpha p, r -= alpha s, u = r .* iM, <r,u>, <r,r>; beta,
-// err, reliable-update trigger (Cg.hpp:169-193).  p (FP16) is the stencil
-// source, r (FP16) a pointwise TMA field, x_lo (FP32) is read with plain
-// loads.  r is rewritten at the scale of the previous <r,r>.
-struct OpCgBh : OpBase<float> {
-	static constexpr int NS = 1, NQ = 1, ND = 2, NG = 1;
-	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
-	static constexpr int V = 4;
-	float iMc;
-	long long npts;
-	float *x;
-	__half *r;
-	int it;
-	float alpha[V], sp[V], sro[V], isrn[V];
-	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
-		it = gl->iter;
-		const double *ps = (it & 1) ? ls.p_scale1 : ls.p_scale0;  // p written by this iteration's sweep A
-#pragma unroll
-		for (int e = 0; e < V; e++) {
-			const int l = lane + e;
-			alpha[e] = (float)ls.alpha[l];
-			sp[e] = (float)ps[l];
-			sro[e] = (float)ls.r_scale[l];
-			isrn[e] = 1.0f / pow2_scale(sqrt(ls.rr[l] / (double)npts));
-		}
-	}
-	__device__ int src_map(int) const { return (it & 1) ? MT_P1_HALO : MT_P0_HALO; }
-	__device__ int q_map(int) const { return MT_R_INT; }
-	__device__ bool raw_center() const { return false; }
-	__device__ Vec<float> src(const Vec<float> *raw) const { return raw[0]; }
-	__device__ void gload(long long o, Vec<float> *gv) const { gv[0] = ldg_rw(x + o); }
-	__device__ void out(long long o, long long, int, const Vec<float> &pc, const Vec<float> &s, const Vec<float> *q,
-	                    const Vec<float> *, const Vec<float> *gv, double (&part)[ND][V]) const {
-		Vec<float> xv = gv[0], rv;
-#pragma unroll
-		for (int e = 0; e < V; e++) {
-			const float pt = pc.v[e] * sp[e], st = s.v[e] * sp[e];
-			xv.v[e] = xv.v[e] + alpha[e] * pt;                      // :169
-			const float r = q[0].v[e] * sro[e] - alpha[e] * st;     // :172
-			const float u = r * iMc;                                // :175
-			dacc(part[0][e], r, u);
-			dacc(part[1][e], r, r);
-			rv.v[e] = r * isrn[e];
-		}
-		stg(x + o, xv);
-		stg(r + o, rv);
-	}
-	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
-		ls.r_scale[lane] = pow2_scale(sqrt(ls.rr[lane] / (double)npts));  // the scale r was written at
-		if (ls.done[lane]) return;
-		ls.ru_new[lane] = tot[0];
-		ls.rr[lane] = tot[1];
-		ls.beta[lane] = __ddiv_rn(tot[0], ls.ru[lane]);           // :185
-		const double err = sqrt(__ddiv_rn(tot[1], ls.bb[lane]));  // :191
-		ls.err[lane] = err;
-		if (!(err == err)) ls.s_exit[lane] = 2;
-		if (err <= gl->tol_in || it >= gl->maxiter || !(err == err)) {
-			ls.pending[lane] = 1;
-			gl->ru_due = 1;
-		}
-		if (gl->period > 0 && it % gl->period == 0) gl->ru_due = gl->ru_all = 1;
-	}
-};
-
-// r = b - A x_hi in FP64 for the FP16 CG form (setup and reliable update,
-// Cg.hpp:119-134).  Two passes: `measure` computes each lane's <r,r> and
-// sets the scale r is stored at; the second pass stores r in FP16 at that
-// scale (and x_lo = 0 at setup) and runs the stop logic of OpResid.
-struct OpResidH : OpBase<double> {
-	static constexpr int NS = 1, NQ = 1, ND = 2;
-	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
-	__half *r;
-	float *xlo;
-	double iMd;
-	long long npts;
-	int ru, measure, WT;
-	int it;
-	int keep[2];
-	float isr[2];
-	__device__ bool enabled(const Global *gl) const { return !ru || gl->ru_due; }
-	__device__ bool slice_live(const Global *gl, const LaneState &ls, int lane0, int nl) const {
-		if (!ru || gl->ru_all) return true;
-		for (int l = lane0; l < lane0 + nl; l++)
-			if (ls.pending[l]) return true;
-		return false;
-	}
-	__device__ bool raw_center() const { return false; }
-	__device__ bool in_update(const Global *gl, const LaneState &ls, int l) const {
-		return !ru || (!ls.done[l] && (gl->ru_all || ls.pending[l]));
-	}
-	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
-		it = gl->iter;
-		for (int e = 0; e < 2; e++) {
-			keep[e] = !in_update(gl, ls, lane + e);
-			isr[e] = measure ? 1.0f : 1.0f / (float)ls.r_scale[lane + e];
-		}
-	}
-	__device__ int src_map(int) const { return MD_X_HALO; }
-	__device__ int q_map(int) const { return MD_B_INT; }
-	__device__ Vec<double> src(const Vec<double> *raw) const { return raw[0]; }
-	__device__ void out(long long, long long pidx, int lane, const Vec<double> &, const Vec<double> &ax,
-	                    const Vec<double> *q, const Vec<double> *, const Vec<double> *, double (&part)[ND][2]) const {
-		const long long ot = sliced(pidx, lane, WT, npts);  // lanes lane, lane+1 share a slice of r and x_lo
-#pragma unroll
-		for (int e = 0; e < 2; e++) {
-			const double bi = q[0].v[e];
-			const double ri = aadd(bi, -ax.v[e]);  // combine2(1.0, b, -1.0, r, r)
-			if (!measure) {
-				if (!keep[e]) r[ot + e] = __float2half_rn((float)ri * isr[e]);
-				if (!ru) xlo[ot + e] = 0.0f;
-			}
-			if (ru) part[0][e] = fma(ri, ri * iMd, part[0][e]);
-			else part[0][e] = fma(bi, bi, part[0][e]);
-			part[1][e] = fma(ri, ri, part[1][e]);
-		}
-	}
-	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
-		if (measure) {
-			if (in_update(gl, ls, lane)) ls.r_scale[lane] = pow2_scale(sqrt(tot[1] / (double)npts));
-			return;
-		}
-		const int maxiter = gl->maxiter;
-		if (ru) {
-			if (!in_update(gl, ls, lane)) return;
-			const bool lost = !(ls.rr[lane] >= 1e-6 * tot[1]);  // see OpResid
-			const double err = sqrt(tot[1] / ls.bb[lane]);
-			ls.err[lane] = err;
-			ls.rr[lane] = tot[1];
-			ls.pending[lane] = 0;
-			if (err <= gl->tol_in) {
-				ls.done[lane] = 1;
-				ls.exit_iter[lane] = it;
-				ls.reason[lane] = STOP_CONVERGED;
-				atomicSub(&gl->active, 1);
-			} else if (it >= maxiter) {
-				ls.done[lane] = 1;
-				ls.exit_iter[lane] = maxiter + 1;
-				ls.reason[lane] = STOP_MAXITER;
-				atomicSub(&gl->active, 1);
-			} else {
-				ls.ru_new[lane] = tot[0];  // continue from the replaced residual
-				double be = tot[0] / ls.ru[lane];
-				if (lost || ls.s_exit[lane] == 2 || !(be >= 0.0 && isfinite(be))) be = 0.0;  // restart: p = u
-				ls.beta[lane] = be;
-				ls.s_exit[lane] = 0;
-			}
-			return;
-		}
-		const double bb = tot[0] == 0.0 ? 1.0 : tot[0];  // Cg.hpp:112-115
-		ls.bb[lane] = bb;
-		ls.rr[lane] = tot[1];
-		const double err = sqrt(__ddiv_rn(tot[1], bb));
-		ls.err[lane] = err;
-		ls.alpha[lane] = 0.0;
-		ls.beta[lane] = 0.0;
-		ls.s_exit[lane] = 0;
-		ls.pending[lane] = 0;
-		ls.pp[lane] = 0.0;
-		int done = 0, reason = STOP_NONE, ex = 0;
-		if (lane >= gl->nrhs) {
-			done = 1;
-		} else if (err < gl->tol) {  // :130-134
-			done = 1;
-			reason = STOP_EARLY;
-		} else if (maxiter < 1) {
-			done = 1;
-			reason = STOP_MAXITER;
-			ex = 1;
-		}
-		ls.done[lane] = done;
-		ls.reason[lane] = reason;
-		ls.exit_iter[lane] = ex;
-		if (!done) atomicAdd(&gl->active, 1);
-	}
-};
-
 // Iteration bookkeeping between launches.
 __global__ void kb_next_iter(Global *gl) {
 	if (gl->active == 0) return;
@@ -1650,7 +1384,7 @@ static void set_tuning(const TuneKey &k, const Tuning &t) {
 	g_tune[k] = t;
 }
 
-constexpr int kLaneDoubles = 22, kLaneInts = 5;  // LaneState arrays
+constexpr int kLaneDoubles = 18, kLaneInts = 5;  // LaneState arrays
 
 #ifndef SEDI_MIXED_THETA_CG
 #define SEDI_MIXED_THETA_CG 1.0
@@ -1661,9 +1395,7 @@ constexpr int kLaneDoubles = 22, kLaneInts = 5;  // LaneState arrays
 #ifndef SEDI_MIXED_THETA_BICGSTAB
 #define SEDI_MIXED_THETA_BICGSTAB 0.1
 #endif
-#ifndef SEDI_MIXED_THETA_FP16
-#define SEDI_MIXED_THETA_FP16 0.1
-#endif
+
 
 struct Batched;
 typedef int (*SetupFn)(Ctx *, Batched *, int nrhs, int maxiter, double tol);
@@ -1686,8 +1418,7 @@ struct EstState {
 
 struct Batched {
 	int R = 0;
-	bool mixed = false;  // FP32 or FP16 Krylov fields, FP64 x_hi, reductions and reliable update
-	bool half = false;   // FP16 storage of r and p (CG), FP32 x_lo
+	bool mixed = false;  // FP32 Krylov fields, FP64 x_hi, reductions and reliable update
 	bool pairs = false;  // single-vector FP64 form: lanes 0/1 = even/odd i1 points of one vector
 	int ks = 0;          // solver whose sweeps run (the mixed pipelined CG runs the CG recurrence)
 	bool aliased = false;  // the Krylov fields belong to the context (single-vector form)
@@ -1785,8 +1516,7 @@ struct CfgFor {
 	typedef Cfg<T, RB, tile_p1(LG), WIDE ? 32 : tile_p2(LG), kThr, WIDE ? 4 : 0, PAIRS> type;
 };
 
-static int pick_R(int nrhs, bool mixed, bool half = false) {
-	if (half) return (nrhs + 7) / 8 * 8;  // whole 8-lane FP16 slices (16 bytes per point)
+static int pick_R(int nrhs, bool mixed) {
 	const int V = mixed ? 4 : 2, full = 8 * V;
 	if (nrhs <= V) return V;
 	if (nrhs <= 2 * V) return 2 * V;
@@ -1897,10 +1627,7 @@ static int kernel_solver(int solver, bool mixed) { return mixed && solver == SED
 // target moves the mixed solution towards the exact one and so away from
 // the FP64 form's, whose own truncation error is 4e-9 .. 4e-8.  BiCGStab's
 // FP64 diagonal lies 1e-7 .. 4e-7 from the exact one, and theta = 0.1 puts
-// the mixed diagonal ten times closer to it (10% more iterations).  FP16
-// storage of r and p leaves the FP64 path (9e-8 at theta = 1, 256^3);
-// theta = 0.1 puts it nearer the exact diagonal than the FP64 form
-// (1.3e-8 against 4.2e-8 at 256^3, 14% more iterations).
+// the mixed diagonal ten times closer to it (10% more iterations).
 static double default_theta(int solver) {
 	switch (solver) {
 	case 2: return SEDI_MIXED_THETA_CG;
@@ -1932,12 +1659,7 @@ int batched_alloc(Ctx *c) {
 	Batched *B = new (std::nothrow) Batched();
 	if (!B) return SEDI_ERR_NOMEM;
 	c->batched = B;
-	B->half = c->precision == SEDI_PREC_MIXED16;
-	B->mixed = c->precision == SEDI_PREC_MIXED || B->half;
-	if (B->half && c->solver != SEDI_CG) {
-		c->error = "FP16 Krylov storage is implemented for CG";
-		return SEDI_ERR_UNSUPPORTED;
-	}
+	B->mixed = c->precision == SEDI_PREC_MIXED;
 	B->ks = kernel_solver(c->solver, B->mixed);
 	if (c->batch > (B->mixed ? 256 : 128)) {
 		c->error = "batch too large for one context (max 256 FP32 / 128 FP64 right-hand sides)";
@@ -1947,16 +1669,16 @@ int batched_alloc(Ctx *c) {
 		c->error = "cuTensorMapEncodeTiled unavailable";
 		return SEDI_ERR_NODEV;
 	}
-	B->R = pick_R(c->batch, B->mixed, B->half);
+	B->R = pick_R(c->batch, B->mixed);
 	B->elems = (size_t)c->g.n * B->R;
-	const int ebT = B->half ? 2 : (B->mixed ? 4 : 8);
+	const int ebT = B->mixed ? 4 : 8;
 	const Tuning tu = tuning_for(TuneKey{c->solver, c->precision, B->R, c->g.n1, c->g.n2, c->g.n3});
-	B->rbT = B->half ? 8 : slice_for(B->R, !B->mixed);
-	if (!B->half && tu.W > 0 && tu.W <= B->R && B->R % tu.W == 0) B->rbT = tu.W;
+	B->rbT = slice_for(B->R, !B->mixed);
+	if (tu.W > 0 && tu.W <= B->R && B->R % tu.W == 0) B->rbT = tu.W;
 	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
 	B->tuned = tu;
 	if (tu.period > 0) B->period = tu.period;
-	B->theta = B->half ? SEDI_MIXED_THETA_FP16 : default_theta(B->ks);
+	B->theta = default_theta(B->ks);
 	if (tu.chunk > 0) B->chunk = tu.chunk;
 	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
 	shape(c->g, B->R, B->rbT, ebT, &B->gT1, &B->gridT1, tu.nz, 1, tu.pfd);
@@ -2012,7 +1734,7 @@ int batched_alloc(Ctx *c) {
 	LaneState &ls = B->ls;
 	double **dp[] = {&ls.bb, &ls.rr, &ls.err, &ls.ru, &ls.ru_new, &ls.sp, &ls.alpha, &ls.beta, &ls.gamma,
 	                 &ls.gamma_old, &ls.delta, &ls.rr_top, &ls.rho, &ls.rho_prev, &ls.omega, &ls.s_norm2, &ls.ts,
-	                 &ls.tt, &ls.r_scale, &ls.p_scale0, &ls.p_scale1, &ls.pp};
+	                 &ls.tt};
 	static_assert(sizeof(dp) / sizeof(dp[0]) == kLaneDoubles, "lane arrays");
 	for (size_t i = 0; i < sizeof(dp) / sizeof(dp[0]); i++) *dp[i] = B->lane_mem + i * R;
 	int **ip[] = {&ls.done, &ls.exit_iter, &ls.reason, &ls.pending, &ls.s_exit};
@@ -2022,15 +1744,6 @@ int batched_alloc(Ctx *c) {
 	auto t_maps = [&](Maps &M, int kind) {
 		int Q1, Q2;
 		tile_for(B->rbT, ebT, &Q1, &Q2, kind);
-		if (B->half) {
-			// FP16 fields as 32-bit pairs of lanes (the same 16 bytes per point
-			// as the FP32 4-lane slices); x_lo is read with plain loads.
-			const int Rp = R / 2, Wp = B->rbT / 2;
-			return make_map(&M.m[MT_R_HALO], B->r, 4, c->g, Rp, Wp, Q1 + 2, Q2 + 2) &&
-			       make_map(&M.m[MT_P0_HALO], B->p0, 4, c->g, Rp, Wp, Q1 + 2, Q2 + 2) &&
-			       make_map(&M.m[MT_P1_HALO], B->p1, 4, c->g, Rp, Wp, Q1 + 2, Q2 + 2) &&
-			       make_map(&M.m[MT_R_INT], B->r, 4, c->g, Rp, Wp, Q1, Q2);
-		}
 		bool k = make_map(&M.m[MT_R_HALO], B->r, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_P0_HALO], B->p0, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_P1_HALO], B->p1, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
@@ -2065,18 +1778,17 @@ int batched_alloc(Ctx *c) {
 // Device bytes batched_alloc takes for a context (each allocation rounded
 // up to the 2 MiB granularity of large device allocations).
 size_t batched_bytes(int solver, int precision, int batch, long long n1, long long n2, long long n3) {
-	const bool half = precision == SEDI_PREC_MIXED16;
-	const bool mixed = precision == SEDI_PREC_MIXED || half;
+	const bool mixed = precision == SEDI_PREC_MIXED;
 	Geo g;
 	g.n1 = (int)n1;
 	g.n2 = (int)n2;
 	g.n3 = (int)n3;
 	g.n = n1 * n2 * n3;
-	const int R = pick_R(batch, mixed, half);
-	const size_t elems = (size_t)g.n * R, ts = half ? 2 : (mixed ? 4 : 8), xs = mixed ? 4 : 8;
+	const int R = pick_R(batch, mixed);
+	const size_t elems = (size_t)g.n * R, ts = mixed ? 4 : 8, xs = mixed ? 4 : 8;
 	const Tuning tu = tuning_for(TuneKey{solver, precision, R, n1, n2, n3});
-	int wT = half ? 8 : slice_for(R, !mixed);
-	if (!half && tu.W > 0 && tu.W <= R && R % tu.W == 0) wT = tu.W;
+	int wT = slice_for(R, !mixed);
+	if (tu.W > 0 && tu.W <= R && R % tu.W == 0) wT = tu.W;
 	SGeo sT, sD;
 	dim3 gT, gD;
 	shape(g, R, wT, (int)ts, &sT, &gT, tu.nz);
@@ -2381,110 +2093,7 @@ struct Impl {
 	}
 };
 
-// FP16 storage form of CG: the residual sweep runs twice (scale of r, then
-// the stores), so setup and every reliable update know r's scale before r
-// is written.
-template <int RBD>
-static void enqueue_resid_h(Ctx *c, Batched *B, bool ru) {
-	typedef typename CfgFor<double, RBD>::type CD;
-	OpResidH op;
-	op.ka = c->k.a;
-	op.kb = c->k.b;
-	op.kc = c->k.c;
-	op.r = (__half *)B->r;
-	op.xlo = (float *)B->x;
-	op.iMd = 1.0 / c->k.a;
-	op.npts = c->g.n;
-	op.ru = ru ? 1 : 0;
-	op.WT = B->rbT;
-	op.measure = 1;
-	launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, c->stream);
-	op.measure = 0;
-	launch<CD>(c, B, B->gD, B->gridD, B->mapsD, op, c->stream);
-}
-
-template <int RBD>
-static void enqueue_cgh_iteration(Ctx *c, Batched *B) {
-	cudaStream_t s = c->stream;
-	OpCgAh a;
-	a.ka = (float)c->k.a;
-	a.kb = (float)c->k.b;
-	a.kc = (float)c->k.c;
-	a.iMc = (float)(1.0 / c->k.a);
-	a.iMd = 1.0 / c->k.a;
-	a.npts = c->g.n;
-	a.p0 = (__half *)B->p0;
-	a.p1 = (__half *)B->p1;
-	launchT<__half, 8>(c, B, a, s);
-	OpCgBh bo;
-	bo.ka = (float)c->k.a;
-	bo.kb = (float)c->k.b;
-	bo.kc = (float)c->k.c;
-	bo.iMc = (float)(1.0 / c->k.a);
-	bo.npts = c->g.n;
-	bo.x = (float *)B->x;
-	bo.r = (__half *)B->r;
-	launchT<__half, 8>(c, B, bo, s);
-	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
-	c->launches++;
-	const long long nb = ((long long)B->elems / 2 + 255) / 256;
-	kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
-	                                                                 (float *)B->x, B->ls.pending, 0, B->gl);
-	c->launches++;
-	enqueue_resid_h<RBD>(c, B, true);
-	kb_ru_done<<<1, 1, 0, s>>>(B->gl);
-	c->launches++;
-}
-
-template <int RBD>
-struct ImplH {
-	static int setup(Ctx *c, Batched *B, int nrhs, int maxiter, double tol) {
-		cudaStream_t s = c->stream;
-		Global g0 = {};
-		g0.iter = 1;
-		g0.maxiter = maxiter;
-		g0.tol = tol;
-		g0.tol_in = B->theta * tol;
-		g0.period = B->period;
-		g0.nrhs = nrhs;
-		g0.active = 1;
-		*B->g0_host = g0;
-		BTRY(cudaMemcpyAsync(B->gl, B->g0_host, sizeof(Global), cudaMemcpyHostToDevice, s));
-		enqueue_resid_h<RBD>(c, B, false);
-		kb_setup_done<<<1, 1, 0, s>>>(B->gl);
-		c->launches++;
-		BTRY(cudaGetLastError());
-		return 0;
-	}
-	static int chunk(Ctx *c, Batched *B) {
-		cudaStream_t s = c->stream;
-		if (!B->graph) {
-			cudaGraph_t graph;
-			const long long before = c->launches;
-			BTRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-			for (int i = 0; i < B->chunk; i++) enqueue_cgh_iteration<RBD>(c, B);
-			BTRY(cudaStreamEndCapture(s, &graph));
-			B->graph_kernels = c->launches - before;
-			c->launches = before;
-			cudaError_t e = cudaGraphInstantiate(&B->graph, graph, 0);
-			cudaGraphDestroy(graph);
-			if (e != cudaSuccess) {
-				B->graph = nullptr;
-				return set_cuda_error(c, e, "cudaGraphInstantiate");
-			}
-		}
-		BTRY(cudaGraphLaunch(B->graph, s));
-		c->launches += B->graph_kernels;
-		return 0;
-	}
-};
-
 static void bind_impl(Batched *B) {
-	if (B->half) {  // R >= 8: the FP64 fields use 8-lane slices
-		B->setup_fn = ImplH<8>::setup;
-		B->chunk_fn = ImplH<8>::chunk;
-		return;
-	}
 	if (B->mixed) {
 		if (B->rbT == 4 && B->rbD == 4) {
 			B->setup_fn = Impl<float, 4, 4>::setup;
@@ -2513,6 +2122,8 @@ static void bind_impl(Batched *B) {
 	}
 }
 
+constexpr long long kPairsMinPoints = 1LL << 22;  // smallest grid of the streaming single-vector form
+
 // Single-vector FP64 form on the streaming sweeps.  A dense vector with n1
 // even is the 2-lane sliced layout of the (n1/2, n2, n3) grid: lane 0 holds
 // the even i1 points, lane 1 the odd ones, so the sweeps of the batched FP64
@@ -2523,7 +2134,11 @@ static void bind_impl(Batched *B) {
 // vector iM, use the context's march kernels (plain.cu).
 int pairs_alloc(Ctx *c) {
 	c->pairs = nullptr;
-	if (c->g.n1 % 2 != 0 || !encode_fn()) return 0;
+	// Small grids stay on the march kernels: below about 4M points the
+	// single-vector working set sits in the 126 MB L2 and a plane-streaming
+	// block gets too few planes (128^3 CG: 34 probe-solves/s streaming, 43
+	// marching; 256^3: 4.1 against 2.2).
+	if (c->g.n1 % 2 != 0 || c->g.n < kPairsMinPoints || !encode_fn()) return 0;
 	Batched *B = new (std::nothrow) Batched();
 	if (!B) return SEDI_ERR_NOMEM;
 	B->pairs = B->aliased = true;
@@ -2573,7 +2188,7 @@ int pairs_alloc(Ctx *c) {
 	LaneState &ls = B->ls;
 	double **dp[] = {&ls.bb, &ls.rr, &ls.err, &ls.ru, &ls.ru_new, &ls.sp, &ls.alpha, &ls.beta, &ls.gamma,
 	                 &ls.gamma_old, &ls.delta, &ls.rr_top, &ls.rho, &ls.rho_prev, &ls.omega, &ls.s_norm2, &ls.ts,
-	                 &ls.tt, &ls.r_scale, &ls.p_scale0, &ls.p_scale1, &ls.pp};
+	                 &ls.tt};
 	for (size_t i = 0; i < sizeof(dp) / sizeof(dp[0]); i++) *dp[i] = B->lane_mem + i * B->R;
 	int **ip[] = {&ls.done, &ls.exit_iter, &ls.reason, &ls.pending, &ls.s_exit};
 	for (size_t i = 0; i < 5; i++) *ip[i] = B->lane_int + i * B->R;
@@ -2948,69 +2563,6 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 	return 0;
 }
 
-// FP16 storage form: sweeps A and B timed alone (every lane active, unit
-// scales, no lane stops).
-static int time_cgh_kernels(Ctx *c, Batched *B, int reps, double *ms, double *bytes, char *names, int *count) {
-	cudaStream_t s = c->stream;
-	Global g = {};
-	g.iter = 2;
-	g.active = B->R;
-	g.maxiter = 1 << 30;
-	g.nrhs = B->R;
-	*B->gl_host = g;
-	BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
-	BTRY(cudaMemsetAsync(B->ls.done, 0, sizeof(int) * B->R, s));
-	BTRY(cudaMemsetAsync(B->lane_mem, 0, sizeof(double) * kLaneDoubles * B->R, s));
-	OpCgAh a;
-	a.ka = (float)c->k.a;
-	a.kb = (float)c->k.b;
-	a.kc = (float)c->k.c;
-	a.iMc = (float)(1.0 / c->k.a);
-	a.iMd = 1.0 / c->k.a;
-	a.npts = c->g.n;
-	a.p0 = (__half *)B->p0;
-	a.p1 = (__half *)B->p1;
-	OpCgBh bo;
-	bo.ka = (float)c->k.a;
-	bo.kb = (float)c->k.b;
-	bo.kc = (float)c->k.c;
-	bo.iMc = (float)(1.0 / c->k.a);
-	bo.npts = c->g.n;
-	bo.x = (float *)B->x;
-	bo.r = (__half *)B->r;
-	cudaEvent_t e0, e1;
-	BTRY(cudaEventCreate(&e0));
-	BTRY(cudaEventCreate(&e1));
-	const double el = (double)B->elems;
-	for (int k = 0; k < 2; k++) {
-		auto one = [&]() {
-			if (k == 0) launchT<__half, 8>(c, B, a, s);
-			else launchT<__half, 8>(c, B, bo, s);
-		};
-		one();
-		BTRY(cudaEventRecord(e0, s));
-		for (int i = 0; i < reps; i++) one();
-		BTRY(cudaEventRecord(e1, s));
-		BTRY(cudaEventSynchronize(e1));
-		float t = 0.f;
-		BTRY(cudaEventElapsedTime(&t, e0, e1));
-		ms[k] = (double)t / reps;
-		// A: r, p_old in, p out (FP16); B: p, r in and r out (FP16), x_lo in and out (FP32).
-		bytes[k] = (k == 0 ? 6.0 : 14.0) * el;
-		snprintf(names + 32 * k, 32, "%s", k == 0 ? "cg_a_fp16" : "cg_b_fp16");
-	}
-	cudaEventDestroy(e0);
-	cudaEventDestroy(e1);
-	BTRY(cudaGetLastError());
-	if (cudaMemcpyAsync(B->gl_host, B->gl, sizeof(Global), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
-	    cudaStreamSynchronize(s) == cudaSuccess && B->gl_host->err) {
-		c->error = "batched sweep timed out waiting for its data";
-		return SEDI_ERR_CUDA;
-	}
-	*count = 2;
-	return 0;
-}
-
 // Single-vector form: its streaming sweeps timed alone (names end in _sv).
 int pairs_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count) {
 	Batched *B = (Batched *)c->pairs;
@@ -3020,7 +2572,6 @@ int pairs_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names,
 
 int batched_time_kernels(Ctx *c, int reps, double *ms, double *bytes, char *names, int *count) {
 	Batched *B = (Batched *)c->batched;
-	if (B->half) return time_cgh_kernels(c, B, reps, ms, bytes, names, count);
 	if (B->mixed) {
 		switch (B->rbT) {
 		case 4: return time_cg_kernels<float, 4>(c, B, reps, ms, bytes, names, count);
@@ -3247,16 +2798,12 @@ static int tune_sweep_ms(sedi_ctx *h, double *ms_sum) {
 
 int batched_autotune(int solver, int precision, int batch, long long n1, long long n2, long long n3, int maxiter,
                      double tol, uint32_t seed, int flags, int *out, double *score_ms) {
-	const bool half = precision == SEDI_PREC_MIXED16;
-	const bool mixed = precision == SEDI_PREC_MIXED || half;
+	const bool mixed = precision == SEDI_PREC_MIXED;
 	if (batch < 2 && !mixed) return SEDI_ERR_ARG;  // one FP64 lane is the single-vector form
-	if (half && solver != SEDI_CG) return SEDI_ERR_UNSUPPORTED;
-	const int R = pick_R(batch, mixed, half);
+	const int R = pick_R(batch, mixed);
 	const TuneKey key{solver, precision, R, n1, n2, n3};
 	std::vector<int> Ws;
-	if (half) {
-		Ws.push_back(8);  // FP16 fields: 8-lane slices only
-	} else if (R >= 8) {
+	if (R >= 8) {
 		Ws.push_back(8);
 		Ws.push_back(4);
 		if (!mixed) Ws.push_back(2);
@@ -3366,8 +2913,7 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 
 int batched_set_tuning(int solver, int precision, int batch, long long n1, long long n2, long long n3,
                        const int *choice) {
-	const bool half = precision == SEDI_PREC_MIXED16;
-	const bool mixed = precision == SEDI_PREC_MIXED || half;
+	const bool mixed = precision == SEDI_PREC_MIXED;
 	Tuning t;
 	t.W = choice[0];
 	t.nz = choice[1];
@@ -3377,7 +2923,7 @@ int batched_set_tuning(int solver, int precision, int batch, long long n1, long 
 	if (t.W < 0 || t.nz < 0 || t.period < 0 || t.chunk < 0 || t.pfd < -1 || t.pfd > 64 ||
 	    (t.period > 0 && (t.period < 1 || t.period > 1000)) || t.chunk > 256)
 		return SEDI_ERR_ARG;
-	set_tuning(TuneKey{solver, precision, pick_R(batch, mixed, half), n1, n2, n3}, t);
+	set_tuning(TuneKey{solver, precision, pick_R(batch, mixed), n1, n2, n3}, t);
 	return 0;
 }
 

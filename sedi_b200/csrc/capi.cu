@@ -37,8 +37,7 @@ sedi_ctx *sedi_create(int solver, long n1, long n2, long n3, double a, double b,
 	if (!err) err = &dummy;
 	*err = 0;
 	if (solver < 1 || solver > 3 || n1 < 1 || n2 < 1 || n3 < 1 || batch < 1 ||
-	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED && precision != SEDI_PREC_MIXED16) ||
-	    (mode & ~3) != 0 ||
+	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED) || (mode & ~3) != 0 ||
 	    n1 > (1L << 30) || n2 > (1L << 30) || n3 > (1L << 30) || (double)n1 * n2 * n3 > 4.0e9) {
 		*err = SEDI_ERR_ARG;
 		return nullptr;
@@ -104,7 +103,7 @@ long long sedi_launch_count(const sedi_ctx *h) { return h ? h->c.launches : 0; }
 int sedi_autotune(int solver, int precision, int batch, long n1, long n2, long n3, int maxiter, double tol,
                   uint32_t seed, int flags, int *choice, double *score_ms) {
 	if (solver < 1 || solver > 3 ||
-	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED && precision != SEDI_PREC_MIXED16) || batch < 1 ||
+	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED) || batch < 1 ||
 	    n1 < 1 || n2 < 1 || n3 < 1 || maxiter < 0 || !choice)
 		return SEDI_ERR_ARG;
 	return batched_autotune(solver, precision, batch, n1, n2, n3, maxiter, tol, seed, flags, choice, score_ms);
@@ -119,7 +118,7 @@ double sedi_mixed_target(const sedi_ctx *h) { return h ? batched_theta(&h->c) : 
 
 int sedi_set_tuning(int solver, int precision, int batch, long n1, long n2, long n3, const int *choice) {
 	if (solver < 1 || solver > 3 ||
-	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED && precision != SEDI_PREC_MIXED16) || batch < 1 ||
+	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED) || batch < 1 ||
 	    n1 < 1 || n2 < 1 || n3 < 1 || !choice)
 		return SEDI_ERR_ARG;
 	return batched_set_tuning(solver, precision, batch, n1, n2, n3, choice);

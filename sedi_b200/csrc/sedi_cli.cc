@@ -8,7 +8,7 @@
 // validation).  The reference picks the solver at compile time (-DSOLVER);
 // here --solver bicgstab|cg|pcg (default cg) or the program name suffix
 // (sedi.cg, sedi.pipelined_cg, sedi.bicgstab) selects it.  Extra options:
-// --precision fp64|mixed|mixed16, --batch B (right-hand sides per launch), --seed S
+// --precision fp64|mixed, --batch B (right-hand sides per launch), --seed S
 // (probe k uses std::mt19937(S + k), default 1234), --quiet (no
 // per-iteration lines), --write-d FILE (the estimate D as raw doubles, i1
 // fastest).
@@ -47,7 +47,7 @@ namespace {
 	fprintf(stderr, "\t-F : don't enable floating point exceptions (accepted; the GPU does not trap)\n");
 	fprintf(stderr, "\t-V ARCHIVE : enable solver validation mode against a validation archive\n");
 	fprintf(stderr, "\t-E ARCHIVE : enable estimator validation mode against a validation archive\n");
-	fprintf(stderr, "\t--solver cg|pcg|bicgstab  --precision fp64|mixed|mixed16  --batch B  --seed S  --quiet  --write-d FILE\n");
+	fprintf(stderr, "\t--solver cg|pcg|bicgstab  --precision fp64|mixed  --batch B  --seed S  --quiet  --write-d FILE\n");
 	exit(1);
 }
 
@@ -123,8 +123,7 @@ int main(int argc, char **argv) {
 			else usage(argv[0]);
 			break;
 		case 2:
-			precision = !strcmp(optarg, "mixed") ? SEDI_PREC_MIXED
-			            : !strcmp(optarg, "mixed16") ? SEDI_PREC_MIXED16 : SEDI_PREC_FP64;
+			precision = !strcmp(optarg, "mixed") ? SEDI_PREC_MIXED : SEDI_PREC_FP64;
 			break;
 		case 3: batch = atoi(optarg); break;
 		case 4: seed = (unsigned)strtoul(optarg, nullptr, 10); break;

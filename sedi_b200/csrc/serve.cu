@@ -280,9 +280,7 @@ void sedi_server_destroy(sedi_server *S) {
 
 long sedi_server_submit(sedi_server *S, int solver, int precision, long n1, long n2, long n3, int samples,
                         uint32_t seed, int maxiter, double tol) {
-	if (!S || solver < 1 || solver > 3 ||
-	    (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED && precision != SEDI_PREC_MIXED16) ||
-	    (precision == SEDI_PREC_MIXED16 && solver != SEDI_CG) || n1 < 1 ||
+	if (!S || solver < 1 || solver > 3 || (precision != SEDI_PREC_FP64 && precision != SEDI_PREC_MIXED) || n1 < 1 ||
 	    n2 < 1 || n3 < 1 || samples < 0 || maxiter < 0 || !(tol >= 0.0))
 		return SEDI_ERR_ARG;
 	Job J;

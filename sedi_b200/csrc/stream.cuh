@@ -21,7 +21,6 @@
 #pragma once
 
 #include <cuda.h>
-#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -54,18 +53,6 @@ struct Vec {
 	T v[V];
 };
 
-// Storage element -> arithmetic type.  FP16 storage (the half-precision
-// Krylov fields of the mixed form) computes in FP32; a thread's vector is
-// four lanes (8 bytes) of a field.
-template <class E>
-struct Arith {
-	typedef E type;
-};
-template <>
-struct Arith<__half> {
-	typedef float type;
-};
-
 template <class T>
 __device__ __forceinline__ Vec<T> lds(const T *p) {
 	typedef typename VW<T>::raw R;
@@ -96,29 +83,6 @@ __device__ __forceinline__ void stg(T *p, const Vec<T> &x) {
 	memcpy(&r, &x, sizeof(R));
 	*reinterpret_cast<R *>(p) = r;
 }
-// FP16 storage: four lanes (8 bytes) <-> four FP32 values, round to nearest.
-__device__ __forceinline__ Vec<float> lds(const __half *p) {
-	const uint2 r = *reinterpret_cast<const uint2 *>(p);
-	__half2 h0, h1;
-	memcpy(&h0, &r.x, 4);
-	memcpy(&h1, &r.y, 4);
-	const float2 a = __half22float2(h0), b = __half22float2(h1);
-	Vec<float> o;
-	o.v[0] = a.x;
-	o.v[1] = a.y;
-	o.v[2] = b.x;
-	o.v[3] = b.y;
-	return o;
-}
-__device__ __forceinline__ void sts(__half *p, const Vec<float> &x) {
-	const __half2 h0 = __floats2half2_rn(x.v[0], x.v[1]), h1 = __floats2half2_rn(x.v[2], x.v[3]);
-	uint2 r;
-	memcpy(&r.x, &h0, 4);
-	memcpy(&r.y, &h1, 4);
-	*reinterpret_cast<uint2 *>(p) = r;
-}
-__device__ __forceinline__ Vec<float> ldg_rw(const __half *p) { return lds(p); }
-__device__ __forceinline__ void stg(__half *p, const Vec<float> &x) { sts(p, x); }
 template <class T>
 __device__ __forceinline__ Vec<T> vzero() {
 	Vec<T> o;
@@ -220,17 +184,14 @@ __host__ __device__ __forceinline__ long long sliced(long long i, int j, int W, 
 // pair and the two lanes' sums are one reduction.
 template <class T, int RB_, int P1_, int P2_, int THREADS_ = 512, int NSTR_ = 0, bool PAIRS_ = false>
 struct Cfg {
-	typedef T type;                              // storage element of the streamed fields
+	typedef T type;                              // element of the streamed fields
 	static constexpr bool PAIRS = PAIRS_;
-	typedef typename Arith<T>::type ctype;       // arithmetic type
+	typedef T ctype;                             // arithmetic type
 	static constexpr int NSTR = NSTR_;  // stages of a transforming sweep's ring (0: SEDI_STREAM_NST_RING)
 	static constexpr int V = Vec<ctype>::V;      // lanes per thread vector
 	static constexpr int RB = RB_;
 	static constexpr int LG = RB / V;  // lane groups per point
-	// Tensor-map elements per point: FP16 fields are mapped as 32-bit pairs
-	// of lanes, so every configuration moves 16 bytes per map element group
-	// and a point's first byte is 16-byte aligned.
-	static constexpr int ME = sizeof(T) == 2 ? RB / 2 : RB;
+	static constexpr int ME = RB;      // tensor-map elements per point
 	static constexpr int P1 = P1_, P2 = P2_;
 	static constexpr int H1 = P1 + 2, H2 = P2 + 2;
 	static constexpr int HALO = H1 * H2, INT = P1 * P2;
