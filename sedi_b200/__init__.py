@@ -208,10 +208,10 @@ class Context:
 
     def config(self):
         """Launch choices of a batched context (see autotune)."""
-        cf = np.zeros(6, np.int32)
+        cf = np.zeros(7, np.int32)
         self._check(load().sedi_ctx_config(self._h, _ptr(cf)), "config")
         return {"slice_width": int(cf[0]), "z_chunks": int(cf[1]), "period": int(cf[2]), "chunk": int(cf[3]),
-                "lanes": int(cf[4]), "prefetch_planes": int(cf[5])}
+                "lanes": int(cf[4]), "prefetch_planes": int(cf[5]), "sweep_a_form": int(cf[6])}
 
     @property
     def mixed_target(self):
@@ -376,22 +376,22 @@ def autotune(solver, dims, batch, precision=MIXED, maxiter=5000, tol=1e-9, seed=
     (sedi_autotune); contexts created afterwards use them.  Returns
     {"slice_width", "z_chunks", "period", "chunk", "score_ms"}."""
     sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
-    ch = np.zeros(5, np.int32)
+    ch = np.zeros(6, np.int32)
     ms = ctypes.c_double(0.0)
     rc = load().sedi_autotune(sid, int(precision), int(batch), *[int(d) for d in dims], int(maxiter), float(tol),
                               int(seed) & 0xFFFFFFFF, 1 if solve else 0, _ptr(ch), ctypes.byref(ms))
     if rc < 0:
         raise SediError(rc, "sedi_autotune")
     return {"slice_width": int(ch[0]), "z_chunks": int(ch[1]), "period": int(ch[2]), "chunk": int(ch[3]),
-            "prefetch_planes": int(ch[4]), "score_ms": ms.value}
+            "prefetch_planes": int(ch[4]), "sweep_a_form": int(ch[5]), "score_ms": ms.value}
 
 
 def set_tuning(solver, dims, batch, precision=MIXED, slice_width=0, z_chunks=0, period=0, chunk=0,
-               prefetch_planes=-1):
+               prefetch_planes=-1, sweep_a_form=0):
     """Record launch choices for contexts of this shape without measuring
     (sedi_set_tuning), e.g. an earlier autotune result."""
     sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
-    ch = np.array([slice_width, z_chunks, period, chunk, prefetch_planes], np.int32)
+    ch = np.array([slice_width, z_chunks, period, chunk, prefetch_planes, sweep_a_form], np.int32)
     rc = load().sedi_set_tuning(sid, int(precision), int(batch), *[int(d) for d in dims], _ptr(ch))
     if rc < 0:
         raise SediError(rc, "sedi_set_tuning")

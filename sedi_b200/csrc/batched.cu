@@ -119,15 +119,15 @@ enum { MD_X_HALO = 0, MD_B_INT };                                     // FP64 fi
 // raw_c[NS], part); fin(lane, tot[ND], gl, ls).
 // ---------------------------------------------------------------------------
 template <class C, class Op>
-__global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_constant__ Maps maps, Op op,
+__global__ void __launch_bounds__(C::THREADS, C::MINB) k_stream(SGeo g, const __grid_constant__ Maps maps, Op op,
                                                        double *partials, unsigned *ticket, Global *gl, LaneState ls) {
 	typedef typename C::type E;   // storage element of the streamed fields
 	typedef typename C::ctype T;  // arithmetic type
 	constexpr int V = C::V, LG = C::LG, RB = C::RB, P1 = C::P1, H1 = C::H1, HALO = C::HALO, INT = C::INT,
 	              NPS = C::NPS, KC = C::KC, KO = C::KO, ME = C::ME;
 	constexpr int NS = Op::NS, NQ = Op::NQ, ND = Op::ND, NGX = Op::NG > 0 ? Op::NG : 1;
-	constexpr bool IDENT = Op::IDENT;
-	typedef Layout<C, NS, NQ, ND, IDENT> Lay;
+	constexpr bool IDENT = Op::IDENT, INPLACE = Op::INPLACE, STAGED = IDENT || INPLACE;
+	typedef Layout<C, NS, NQ, ND, IDENT, INPLACE> Lay;
 	constexpr int NST = Lay::NST, KEEP = Lay::KEEP;
 	extern __shared__ __align__(128) unsigned char smem[];
 	if (gl->active == 0 || !op.enabled(gl)) return;
@@ -252,8 +252,10 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 		// Phase 1: stencil input of plane j (transforming ops only).
 		if (!IDENT && j < np) {
 			const int p = z0 - 1 + j;
-			E *cr = ring + (j & 3) * HE;
-			const E *st = stage0 + sj * SE;
+			E *const st = stage0 + sj * SE;
+			// In place: over the source field INPLACE_SLOT of this plane's stage
+			// (each thread rewrites only the points it read).
+			E *cr = INPLACE ? st + Op::INPLACE_SLOT * HE : ring + (j & 3) * HE;
 			const bool pin = p >= 0 && p < g.n3;
 #pragma unroll
 			for (int k = 0; k < KC; k++) {
@@ -269,6 +271,9 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 				}
 				sts(cr + hoff[k], cv);
 			}
+			// The stage is refilled by TMA later: order these generic writes
+			// before those async-proxy writes.
+			if (INPLACE) fence_async_smem();
 		}
 		// Phase 2: outputs of plane m = j-2 from planes m-1, m, m+1.
 		if (j >= 3) {
@@ -281,10 +286,11 @@ __global__ void __launch_bounds__(C::THREADS) k_stream(SGeo g, const __grid_cons
 			const E *stz = stage0 + s0 * SE;
 			const E *cm, *c0, *cp;
 			bool zm = true, zp = true;  // planes m-1, m+1 inside the grid
-			if (IDENT) {
-				cm = stage0 + sm1 * SE;
-				c0 = stz;
-				cp = stage0 + sp1 * SE;
+			if (STAGED) {
+				const int off = INPLACE ? Op::INPLACE_SLOT * HE : 0;
+				cm = stage0 + sm1 * SE + off;
+				c0 = stz + off;
+				cp = stage0 + sp1 * SE + off;
 				zm = z - 1 >= 0;
 				zp = z + 1 < g.n3;
 			} else {
@@ -434,6 +440,8 @@ template <class T>
 struct OpBase {
 	static constexpr int KIND = 0;  // tile configuration (see CfgFor)
 	static constexpr int NG = 0;    // pointwise fields read with plain loads, prefetched by gload
+	static constexpr bool INPLACE = false;  // stencil input written over source INPLACE_SLOT (no ring)
+	static constexpr int INPLACE_SLOT = 1;
 	T ka, kb, kc;
 	__device__ void gload(long long, Vec<T> *) const {}
 	__device__ bool enabled(const Global *) const { return true; }
@@ -658,6 +666,19 @@ struct OpCgA : OpBase<T> {
 		}
 		ls.alpha[lane] = al;
 	}
+};
+
+// Sweep A with the stencil input p written over p_old in the stage (KIND 2:
+// two blocks per SM on 32x16 tiles; KIND 3: 32x32 tiles, 6 stages).  p_old
+// is dead once p is formed at a point, and r (slot 0) stays for iteration
+// 1's <r,u>.  The values computed are those of OpCgA.
+template <class T, int K>
+struct OpCgAv : OpCgA<T> {
+	static constexpr int KIND = K;
+	static constexpr bool INPLACE = true;
+	static constexpr int INPLACE_SLOT = 1;
+	OpCgAv() = default;
+	explicit OpCgAv(const OpCgA<T> &o) : OpCgA<T>(o) {}
 };
 
 // ---------------------------------------------------------------------------
@@ -1354,9 +1375,13 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 #ifndef SEDI_STREAM_PFD
 #define SEDI_STREAM_PFD 0  // default L2 prefetch distance of the sweeps, in planes (0: none)
 #endif
+#ifndef SEDI_CGA_FORM
+#define SEDI_CGA_FORM 1  // CG sweep A: 1 ring (32x32), 2 in place (32x16, 2 blocks/SM), 3 in place (32x32)
+#endif
 struct Tuning {
 	int W = 0, nz = 0, period = 0, chunk = 0;
-	int pfd = -1;  // L2 prefetch distance in planes (-1: SEDI_STREAM_PFD)
+	int pfd = -1;   // L2 prefetch distance in planes (-1: SEDI_STREAM_PFD)
+	int acfg = 0;   // form of CG's sweep A (0: SEDI_CGA_FORM)
 };
 struct TuneKey {
 	int solver, precision, R;
@@ -1420,6 +1445,7 @@ struct Batched {
 	int R = 0;
 	bool mixed = false;  // FP32 Krylov fields, FP64 x_hi, reductions and reliable update
 	bool pairs = false;  // single-vector FP64 form: lanes 0/1 = even/odd i1 points of one vector
+	int acfg = SEDI_CGA_FORM;  // form of CG's sweep A (see CfgFor, OpCgAv)
 	int ks = 0;          // solver whose sweeps run (the mixed pipelined CG runs the CG recurrence)
 	bool aliased = false;  // the Krylov fields belong to the context (single-vector form)
 	const double *graph_hist = nullptr;  // history pointer the captured graph holds
@@ -1509,11 +1535,17 @@ __host__ __device__ constexpr int tile_p2(int lg) {
 // barrier and latency are paid once per two points; 222 KB of shared
 // memory).  Measured on B200 at 128^3 x 64 lanes: CG A 449 -> 372 us,
 // BiCGStab 2 463 -> 353 us, BiCGStab 3 877 -> 787 us.
+// KIND 2 and 3 are the in-place forms of CG's sweep A (no ring): KIND 2 the
+// 32x16 tile with a 5-stage ring, small enough for two blocks per SM
+// (98 KB each, 64 registers per thread); KIND 3 the 32x32 tile with a
+// 6-stage ring (three planes of TMA lookahead instead of two).
 template <class T, int RB, int KIND = 0, bool PAIRS = false>
 struct CfgFor {
 	static constexpr int LG = RB * (int)sizeof(T) / 16;
-	static constexpr bool WIDE = KIND == 1 && LG == 1;
-	typedef Cfg<T, RB, tile_p1(LG), WIDE ? 32 : tile_p2(LG), kThr, WIDE ? 4 : 0, PAIRS> type;
+	static constexpr bool WIDE = (KIND == 1 || KIND == 3) && LG == 1;
+	static constexpr int NSTR = LG != 1 ? 0 : (KIND == 1 ? 4 : (KIND == 2 ? 5 : (KIND == 3 ? 6 : 0)));
+	static constexpr int MINB = (KIND == 2 && LG == 1) ? 2 : 1;
+	typedef Cfg<T, RB, tile_p1(LG), WIDE ? 32 : tile_p2(LG), kThr, NSTR, PAIRS, MINB> type;
 };
 
 static int pick_R(int nrhs, bool mixed) {
@@ -1588,7 +1620,7 @@ static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int
 
 template <class C, class Op>
 static int launch(Ctx *c, Batched *B, const SGeo &sg, dim3 grid, const Maps &maps, const Op &op, cudaStream_t s) {
-	const size_t sm = Layout<C, Op::NS, Op::NQ, Op::ND, Op::IDENT>::BYTES;
+	const size_t sm = Layout<C, Op::NS, Op::NQ, Op::ND, Op::IDENT, Op::INPLACE>::BYTES;
 	static bool attr_set = false;
 	if (!attr_set) {
 		cudaFuncSetAttribute(k_stream<C, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -1603,7 +1635,7 @@ static int launch(Ctx *c, Batched *B, const SGeo &sg, dim3 grid, const Maps &map
 template <class T, int RBT, bool PAIRS = false, class Op>
 static int launchT(Ctx *c, Batched *B, const Op &op, cudaStream_t s) {
 	typedef typename CfgFor<T, RBT, Op::KIND, PAIRS>::type C;
-	if (Op::KIND == 1) return launch<C>(c, B, B->gT1, B->gridT1, B->mapsT1, op, s);
+	if (Op::KIND == 1 || Op::KIND == 3) return launch<C>(c, B, B->gT1, B->gridT1, B->mapsT1, op, s);
 	return launch<C>(c, B, B->gT, B->gridT, B->mapsT, op, s);
 }
 
@@ -1678,6 +1710,7 @@ int batched_alloc(Ctx *c) {
 	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
 	B->tuned = tu;
 	if (tu.period > 0) B->period = tu.period;
+	if (tu.acfg >= 1 && tu.acfg <= 3) B->acfg = tu.acfg;
 	B->theta = default_theta(B->ks);
 	if (tu.chunk > 0) B->chunk = tu.chunk;
 	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
@@ -1883,6 +1916,15 @@ static void enqueue_resid(Ctx *c, Batched *B, bool ru) {
 	}
 }
 
+template <class T, int RBT, bool PAIRS = false>
+static void launch_cg_a(Ctx *c, Batched *B, const OpCgA<T> &a, cudaStream_t s) {
+	switch (B->acfg) {
+	case 2: launchT<T, RBT, PAIRS>(c, B, OpCgAv<T, 2>(a), s); break;
+	case 3: launchT<T, RBT, PAIRS>(c, B, OpCgAv<T, 3>(a), s); break;
+	default: launchT<T, RBT, PAIRS>(c, B, a, s);
+	}
+}
+
 template <class T, int RBT, int RBD, bool PAIRS = false>
 static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	cudaStream_t s = c->stream;
@@ -1894,7 +1936,7 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	a.p0 = (T *)B->p0;
 	a.p1 = (T *)B->p1;
 	a.mixed = B->mixed ? 1 : 0;
-	launchT<T, RBT, PAIRS>(c, B, a, s);
+	launch_cg_a<T, RBT, PAIRS>(c, B, a, s);
 	OpCgB<T> bo;
 	bo.ka = (T)c->k.a;
 	bo.kb = (T)c->k.b;
@@ -2535,11 +2577,11 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		return 0;
 	}
 	for (int k = 0; k < 2; k++) {
-		if (k == 0) launchT<T, RBT, PAIRS>(c, B, a, s);
+		if (k == 0) launch_cg_a<T, RBT, PAIRS>(c, B, a, s);
 		else launchT<T, RBT, PAIRS>(c, B, bo, s);
 		BTRY(cudaEventRecord(e0, s));
 		for (int i = 0; i < reps; i++) {
-			if (k == 0) launchT<T, RBT, PAIRS>(c, B, a, s);
+			if (k == 0) launch_cg_a<T, RBT, PAIRS>(c, B, a, s);
 			else launchT<T, RBT, PAIRS>(c, B, bo, s);
 		}
 		BTRY(cudaEventRecord(e1, s));
@@ -2851,6 +2893,17 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 		if (rc) return rc;
 		if (ms < 0.98 * best_ms || (best.pfd < 0 && pf == SEDI_STREAM_PFD)) best_ms = ms, best = t;
 	}
+	// Form of CG's sweep A (ring, or in place with two blocks per SM or six stages).
+	if (kernel_solver(solver, mixed) == SEDI_CG) {
+		for (int ac = 1; ac <= 3; ac++) {
+			Tuning t = best;
+			t.acfg = ac;
+			double ms = 0.0;
+			const int rc = score(t, &ms);
+			if (rc) return rc;
+			if (ms < 0.98 * best_ms || (best.acfg == 0 && ac == SEDI_CGA_FORM)) best_ms = ms, best = t;
+		}
+	}
 	double best_est = -1.0;
 	if (flags & 1) {
 		set_tuning(key, best);
@@ -2907,6 +2960,7 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 	out[2] = best.period;
 	out[3] = best.chunk;
 	out[4] = best.pfd >= 0 ? best.pfd : SEDI_STREAM_PFD;
+	out[5] = best.acfg ? best.acfg : SEDI_CGA_FORM;
 	if (score_ms) *score_ms = best_est >= 0 ? best_est : best_ms;
 	return 0;
 }
@@ -2920,7 +2974,8 @@ int batched_set_tuning(int solver, int precision, int batch, long long n1, long 
 	t.period = choice[2];
 	t.chunk = choice[3];
 	t.pfd = choice[4];
-	if (t.W < 0 || t.nz < 0 || t.period < 0 || t.chunk < 0 || t.pfd < -1 || t.pfd > 64 ||
+	t.acfg = choice[5];
+	if (t.W < 0 || t.nz < 0 || t.period < 0 || t.chunk < 0 || t.pfd < -1 || t.pfd > 64 || t.acfg < 0 || t.acfg > 3 ||
 	    (t.period > 0 && (t.period < 1 || t.period > 1000)) || t.chunk > 256)
 		return SEDI_ERR_ARG;
 	set_tuning(TuneKey{solver, precision, pick_R(batch, mixed), n1, n2, n3}, t);
@@ -2936,6 +2991,7 @@ int batched_config(const Ctx *c, int *out) {
 	out[3] = B->chunk;
 	out[4] = B->R;
 	out[5] = B->gT.pfd;
+	out[6] = B->acfg;
 	return 0;
 }
 

@@ -182,8 +182,9 @@ __host__ __device__ __forceinline__ long long sliced(long long i, int j, int W, 
 // vector (a dense FP64 vector with even n1 is the 2-lane sliced layout of
 // the (n1/2, n2, n3) grid); the stencil takes its i1 neighbours across the
 // pair and the two lanes' sums are one reduction.
-template <class T, int RB_, int P1_, int P2_, int THREADS_ = 512, int NSTR_ = 0, bool PAIRS_ = false>
+template <class T, int RB_, int P1_, int P2_, int THREADS_ = 512, int NSTR_ = 0, bool PAIRS_ = false, int MINB_ = 1>
 struct Cfg {
+	static constexpr int MINB = MINB_;  // blocks per SM the launch bounds ask for
 	typedef T type;                              // element of the streamed fields
 	static constexpr bool PAIRS = PAIRS_;
 	typedef T ctype;                             // arithmetic type
@@ -220,11 +221,16 @@ struct Cfg {
 
 // Shared-memory carve-up for a kernel with NS source and NQ pointwise fields
 // and ND reduced dot products.
-template <class C, int NS, int NQ, int ND, bool IDENT>
+// INPLACE: a transforming sweep that writes the stencil input over one of
+// its source fields in the stage (no ring); the stencil then reads the
+// stages, which live as long as a raw source's (KEEP 3).
+template <class C, int NS, int NQ, int ND, bool IDENT, bool INPLACE = false>
 struct Layout {
 	typedef typename C::type T;
-	static constexpr int NST = IDENT ? SEDI_STREAM_NST_IDENT : (C::NSTR > 0 ? C::NSTR : SEDI_STREAM_NST_RING);
-	static constexpr int KEEP = IDENT ? 3 : 2;  // steps a stage outlives its arrival
+	static constexpr bool STAGED = IDENT || INPLACE;  // the stencil reads the stages
+	static constexpr int NST = IDENT ? SEDI_STREAM_NST_IDENT
+	                                 : (C::NSTR > 0 ? C::NSTR : (INPLACE ? SEDI_STREAM_NST_IDENT : SEDI_STREAM_NST_RING));
+	static constexpr int KEEP = STAGED ? 3 : 2;  // steps a stage outlives its arrival
 	static_assert(NST > KEEP + 1, "ring too shallow");
 	// Every TMA destination starts on a 128-byte boundary.
 	static constexpr size_t HALO_PAD = ((size_t)C::HALO * C::RB * sizeof(T) + 127) / 128 * 128;
@@ -233,7 +239,7 @@ struct Layout {
 	static constexpr size_t INT_ELEMS = INT_PAD / sizeof(T);    // element offset between pointwise fields
 	static constexpr size_t STAGE_BYTES = (size_t)(NS * C::HALO + NQ * C::INT) * C::RB * sizeof(T);
 	static constexpr size_t STAGE_PAD = NS * HALO_PAD + NQ * INT_PAD;
-	static constexpr int RING = IDENT ? 0 : 4;  // computed stencil-input planes
+	static constexpr int RING = STAGED ? 0 : 4;  // computed stencil-input planes
 	static constexpr size_t OFF_RING = NST * STAGE_PAD;
 	static constexpr size_t OFF_BAR = OFF_RING + RING * HALO_PAD;
 	static constexpr size_t BYTES = OFF_BAR + NST * sizeof(uint64_t);
