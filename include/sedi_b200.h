@@ -176,34 +176,61 @@ int sedi_residual_noalloc(long n1, long n2, long n3, double a, double b, double 
                           const double *b_dev, double *r_dev, double *err_out, void *stream);
 
 /*
- * Slab (i3) domain decomposition of the FP64 CG method: the kernels one rank
- * runs on its slab (the host loop, halo exchange and collectives are in
- * sedi_b200/domain.py).  Replaces, for a decomposition -p 1x1xP, the
- * reference's DomainDecomposition (DomainDecomposition.hpp:51-80), the halo
- * exchange (CommHalo.hpp:84-181) -- a halo is one contiguous ghost plane --,
- * the inner/border stencil split (DistrAsyncStencil.hpp:52-100) and the
- * local part of DistrAsyncDotProds (DistrAsyncDotProds.hpp:85-136).
- * Every slab vector is [nloc + 2][n2][n1] doubles (device), i1 fastest, with
- * ghost planes 0 and nloc+1; ghost planes on the global boundary are zero.
- *
+ * Slab (i3) domain decomposition of the FP64 solvers (CG, pipelined CG,
+ * BiCGStab): the kernels one rank runs on its slab (the host loop, halo
+ * exchange and collectives are in sedi_b200/domain.py).  Replaces, for a
+ * decomposition -p 1x1xP, the reference's DomainDecomposition
+ * (DomainDecomposition.hpp:51-80), the halo exchange (CommHalo.hpp:84-181) --
+ * a halo is one contiguous ghost plane --, the inner/border stencil split
+ * (DistrAsyncStencil.hpp:52-100) and the local part of DistrAsyncDotProds
+ * (DistrAsyncDotProds.hpp:85-136).  Every slab vector is [nloc + 2][n2][n1]
+ * doubles (device), i1 fastest, with ghost planes 0 and nloc+1; ghost planes
+ * on the global boundary are zero.
+ */
+typedef struct sedi_slab_args {
+	const double *src;  /* stencil input (ghost planes current), or the mode's first vector */
+	const double *b;
+	const double *rhat;
+	double *x, *r, *y, *u, *w, *wn, *q, *s, *p, *z, *v, *t;
+	double iM;     /* constant Jacobi preconditioner 1/a */
+	double alpha, beta;
+	double bo;     /* BiCGStab: -beta*omega */
+	double omega;
+	int first;     /* first iteration */
+} sedi_slab_args;
+
+/*
  * sedi_slab_sweep: for ghosted planes z in [z_lo, z_hi) (1 <= z_lo <= z_hi
- * <= nloc+1), with the stencil applied to src:
- *   mode 0  r = b - A src; dots <b,b>, <r,r>                 (Cg.hpp:112-129)
- *   mode 1  dots <A src, src> and, when first, <r, r*iM>     (Cg.hpp:152-166)
- *   mode 2  x += alpha src; r -= alpha A src; dots <r, r*iM>, <r,r>
- *                                                             (Cg.hpp:169-182)
- *   mode 3  y = A src                                         (Stencil.hpp:38-54)
- * plane_part[(z-1)*2 + d] receives plane z's dot d, summed in an order fixed
- * by n1 and n2 only (sedi_slab_chunks() row chunks per plane, scratch
- * chunk_part of nloc*chunks*2 doubles), so plane sums, and the solve, do not
- * depend on how the planes are split into slabs.  Elementwise values round
- * as the reference's.  Runs on `stream` (cudaStream_t as void*).
+ * <= nloc+1), with A the stencil applied to src (or to src .* iM where noted):
+ *   mode  0  r = b - A src; dots <b,b>, <r,r>                       (Cg.hpp:112-129)
+ *   mode  1  dots <A src, src> and, when first, <r, r*iM>          (Cg.hpp:152-166)
+ *   mode  2  x += alpha src; r -= alpha A src; dots <r, r*iM>, <r,r> (Cg.hpp:169-182)
+ *   mode  3  y = A src                                              (Stencil.hpp:38-54)
+ *   mode  4  u = src*iM, w = A(src*iM), q = s = p = z = 0;
+ *            dots <src,u>, <w,u>, <src,src>                         (PipelinedCg.hpp:138-155)
+ *   mode  5  m = src*iM, n = A m; q = m + beta q, s = src + beta s,
+ *            p = u + beta p, z = n + beta z, r -= alpha s, x += alpha p,
+ *            u -= alpha q, wn = src - alpha z; dots <r,u>, <wn,u>, <r,r>
+ *            (src is w; wn must not be src)                         (PipelinedCg.hpp:155-223)
+ *   mode  6  p = r (first) or r + beta p + bo v                     (BiCgStab.hpp:165-173)
+ *   mode  7  v = A(src*iM); dot <v, rhat>                           (BiCgStab.hpp:175-187)
+ *   mode  8  s = r - alpha v                                        (BiCgStab.hpp:189)
+ *   mode  9  t = A(src*iM); dots <src,src>, <t,src>, <t,t>          (BiCgStab.hpp:192-212)
+ *   mode 10  x += alpha p*iM + omega s*iM; r = s - omega t;
+ *            dots <r,r>, <r,rhat>                                   (BiCgStab.hpp:216-224)
+ *   mode 11  x += alpha p*iM                                        (BiCgStab.hpp:193-199)
+ *   mode 12  p = r*iM (first) or r*iM + beta p                      (Cg.hpp:144-147, :188)
+ * Modes 6, 8, 11 and 12 are elementwise; 3 returns no dots.  The others
+ * write plane_part[(z-1)*3 + d], plane z's dot d (0 for unused d), summed in
+ * an order fixed by n1 and n2 only (sedi_slab_chunks() row chunks per plane,
+ * scratch chunk_part of nloc*chunks*3 doubles), so plane sums, and the
+ * solves, do not depend on how the planes are split into slabs.  Elementwise
+ * values round as the reference's.  Pointers a mode does not use may be
+ * NULL; a missing one it uses returns SEDI_ERR_ARG.  Runs on `stream`
+ * (cudaStream_t as void*).
  */
 int sedi_slab_sweep(int mode, long n1, long n2, long nloc, double a, double b, double c, long z_lo, long z_hi,
-                    double iM, double alpha, int first, const double *src, double *x, double *r, const double *bvec,
-                    double *y, double *chunk_part, double *plane_part, void *stream);
-/* p = u + beta p, u = r .* iM (p = u when first), over n elements (Cg.hpp:144-147, :188). */
-int sedi_slab_p(long n, const double *r, double *p, double iM, double beta, int first, void *stream);
+                    const sedi_slab_args *args, double *chunk_part, double *plane_part, void *stream);
 /* t += x .* v, q += v .* v (t = x .* v, q = v .* v when reset) over n elements
  * (stochastic-estimator.cc:195, :198). */
 int sedi_slab_accumulate(long n, const double *x, const double *v, double *t, double *q, int reset, void *stream);

@@ -1,13 +1,16 @@
 """Decomposed-grid command-line driver: ``-p 1x1xP`` over P GPUs.
 
     torchrun --nproc-per-node P -m sedi_b200.cli -g N1xN2xN3 -p 1x1xP [-s S] [-e TOL] [-m MAXITER] [-i] [-f MODE]
+                                                 [--solver cg|pcg|bicgstab]
     python -m sedi_b200.cli -g ... -p 1x1xP --loopback      # P slabs in one process on one GPU
 
 The counterpart of ``mpirun -n P stochastic-estimator.cg.exe -g ... -p ...``
 (README.md:74-82) for slab decompositions along i3: the options and printed
 lines are the reference's (CmdLineParser.hpp:43-136, stochastic-estimator.cc,
-DomainDecomposition.hpp:43-48, Cg.hpp:192, Timers.hpp:57-70) and the solver
-is the reference CG in FP64 (sedi_b200.domain.SlabCg).  Probe k is the global
+DomainDecomposition.hpp:43-48, Cg.hpp:192, PipelinedCg.hpp:228,
+BiCgStab.hpp:228, Timers.hpp:57-70) and the solver is the reference's CG,
+pipelined CG or BiCGStab in FP64 (sedi_b200.domain; the reference picks it at
+compile time, here --solver, default cg).  Probe k is the global
 std::mt19937(seed + k) probe (--seed, default 1234).  The one-GPU driver with
 every solver and precision is the ``sedi`` binary (-p 1x1x1).
 """
@@ -29,6 +32,7 @@ def parse(argv=None):
     ap.add_argument("-i", action="store_true", help="ignore solver convergence errors and keep going")
     ap.add_argument("-f", type=int, default=0, help="solver operation mode bits (Cg::mode_t)")
     ap.add_argument("-F", action="store_true", help="accepted; the GPU does not trap floating-point exceptions")
+    ap.add_argument("--solver", default="cg", choices=["cg", "pcg", "pipelined_cg", "bicgstab"])
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--quiet", action="store_true", help="no per-iteration lines")
     ap.add_argument("--loopback", action="store_true", help="all slabs in this process, on one GPU")
@@ -54,7 +58,7 @@ def main(argv=None):
     a = parse(argv)
     import torch
     import torch.distributed as dist
-    from sedi_b200.domain import SlabCg
+    from sedi_b200.domain import slab_solver
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     distributed = world > 1 and not a.loopback
@@ -66,7 +70,7 @@ def main(argv=None):
         print(f"sedi_b200.cli: -p {a.p} needs {a.parts} ranks (torchrun --nproc-per-node {a.parts}) or --loopback",
               file=sys.stderr)
         return 1
-    cg = SlabCg(a.dims, a.parts, loopback=not distributed, mode=a.f)
+    cg = slab_solver(a.solver, a.dims, a.parts, loopback=not distributed, mode=a.f)
     rank0 = cg.rank == 0
     out = (lambda *x: print(*x, flush=True)) if rank0 else (lambda *x: None)
     n1, n2, n3 = a.dims
@@ -74,10 +78,10 @@ def main(argv=None):
     out(f"Domain decomposition across {a.parts} MPI ranks")
     out(f"Processor decomposition is (1, 1, {a.parts})")
     out(f"Process block shape is ({n1}, {n2}, {cg.ranges[0][1]})")
-    out(f"Initialized Cg solver, sync_dotprod={int(bool(a.f & 2))}, sync_stencil={int(bool(a.f & 1))}")
+    out(f"Initialized {cg.NAME} solver, sync_dotprod={int(bool(a.f & 2))}, sync_stencil={int(bool(a.f & 1))}")
 
     x, b, t, q = cg.zeros(), cg.zeros(), cg.zeros(), cg.zeros()
-    work = (cg.zeros(), cg.zeros())
+    work = cg.work()
     plane = n1 * n2
     iters = []
     t_rng = 0.0
@@ -92,7 +96,7 @@ def main(argv=None):
         res, err, it = cg.solve(x, b, a.m, a.e, work)
         if not a.quiet:
             for i, e in enumerate(cg.last_history[1:], 1):
-                out(f"Cg: after iter={i}, err={e:.10e}")
+                out(f"{cg.NAME}: after iter={i}, err={e:.10e}")
         for j in range(len(cg.local)):
             cg.backend.accumulate(x[j], b[j], t[j], q[j], k == 0)
         iters.append(it)

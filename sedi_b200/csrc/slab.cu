@@ -1,4 +1,4 @@
-// Slab (i3) domain decomposition of the FP64 CG method: the per-rank kernels.
+// Slab (i3) domain decomposition of the FP64 solvers: the per-rank kernels.
 //
 // The reference decomposes the grid into blocks, one per MPI rank, with a
 // ghost layer filled by a halo exchange (DomainDecomposition.hpp:51-80,
@@ -17,7 +17,9 @@
 // sum is the same whichever rank holds the plane; the host adds the planes
 // in global order.  The solution therefore does not depend on the number of
 // slabs, bit for bit.  Elementwise values round as the reference's
-// (operator by operator, no FMA contraction), like the single-vector form.
+// (operator by operator, no FMA contraction), like the single-vector form:
+// a stencil input the reference stores (u = r .* iM, m = w .* iM, p_hat,
+// s_hat) is formed at each neighbour read with the same rounding.
 #include "sedi_internal.h"
 
 namespace sedi {
@@ -26,6 +28,7 @@ namespace {
 
 constexpr int kSlabThreads = 256;
 constexpr int kSlabChunks = 8;  // row chunks per plane (fixed: the summation order depends on it)
+constexpr int kSlabDots = 3;    // dot products per plane
 
 struct SlabGeo {
 	int n1, n2, nloc;
@@ -38,17 +41,20 @@ __device__ __forceinline__ void chunk_rows(const SlabGeo &g, int c, int *r0, int
 	*r1 = min(g.n2, *r0 + per);
 }
 
-// 7-point stencil at ghosted plane z (1..nloc), row i2, column i1 of the slab.
-__device__ __forceinline__ double slab_stencil(const SlabGeo &g, const Coef &k, const double *__restrict__ x,
-                                               int z, int i2, int i1) {
+// 7-point stencil at ghosted plane z (1..nloc), row i2, column i1 of the
+// slab, applied to f = scale .* src when `scaled` (the stencil input the
+// reference stores as a vector), else to src.
+__device__ __forceinline__ double slab_stencil(const SlabGeo &g, const Coef &k, const double *__restrict__ src,
+                                               bool scaled, double scale, int z, int i2, int i1) {
 	const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + i1;
-	const double xc = __ldg(x + i);
-	const double xm1 = i1 > 0 ? __ldg(x + i - 1) : 0.0;
-	const double xm2 = i2 > 0 ? __ldg(x + i - g.n1) : 0.0;
-	const double xm3 = __ldg(x + i - g.plane);  // ghost plane 0 at the slab's lower side
-	const double xp1 = i1 < g.n1 - 1 ? __ldg(x + i + 1) : 0.0;
-	const double xp2 = i2 < g.n2 - 1 ? __ldg(x + i + g.n1) : 0.0;
-	const double xp3 = __ldg(x + i + g.plane);  // ghost plane nloc+1 at the upper side
+	auto f = [&](long long j) { return scaled ? mul(__ldg(src + j), scale) : __ldg(src + j); };
+	const double xc = f(i);
+	const double xm1 = i1 > 0 ? f(i - 1) : 0.0;
+	const double xm2 = i2 > 0 ? f(i - g.n1) : 0.0;
+	const double xm3 = f(i - g.plane);  // ghost plane 0 at the slab's lower side
+	const double xp1 = i1 < g.n1 - 1 ? f(i + 1) : 0.0;
+	const double xp2 = i2 < g.n2 - 1 ? f(i + g.n1) : 0.0;
+	const double xp3 = f(i + g.plane);  // ghost plane nloc+1 at the upper side
 	return stencil7(k, xc, xm1, xm2, xm3, xp1, xp2, xp3);
 }
 
@@ -73,61 +79,143 @@ __device__ __forceinline__ void block_total(double (&v)[ND]) {
 	__syncthreads();
 }
 
-// Modes of the fused stencil sweep (one block per (plane, row chunk)).
 enum SlabMode {
-	SLAB_SETUP = 0,  // r = b - A x; <b,b>, <r,r>            (Cg.hpp:112-129)
-	SLAB_SP = 1,     // s = A p; <s,p> (+ <r,u> when first)  (Cg.hpp:152-166)
-	SLAB_UPDATE = 2, // s = A p; x += alpha p; r -= alpha s; <r,u>, <r,r>  (Cg.hpp:169-182)
-	SLAB_APPLY = 3,  // y = A x                                (Stencil.hpp:38-54)
+	SLAB_SETUP = 0,       // r = b - A src; <b,b>, <r,r>                          (Cg.hpp:112-129)
+	SLAB_CG_SP = 1,       // <A src, src> (+ <r, r iM> when first)                (Cg.hpp:152-166)
+	SLAB_CG_UPDATE = 2,   // x += alpha src; r -= alpha A src; <r, r iM>, <r,r>   (Cg.hpp:169-182)
+	SLAB_APPLY = 3,       // y = A src                                            (Stencil.hpp:38-54)
+	SLAB_PCG_SETUP = 4,   // u = r iM, w = A u, q = s = p = z = 0; <r,u>, <w,u>, <r,r>  (PipelinedCg.hpp:138-155)
+	SLAB_PCG_ITER = 5,    // m = w iM, n = A m, the eight updates, w' in wn; next <r,u>, <w',u>, <r,r>
+	                      //                                                      (PipelinedCg.hpp:155-223)
+	SLAB_BICG_P = 6,      // p = r (first) or r + beta p + bo v                   (BiCgStab.hpp:165-173)
+	SLAB_BICG_V = 7,      // v = A (p iM); <v, r_hat>                             (BiCgStab.hpp:175-187)
+	SLAB_BICG_S = 8,      // s = r - alpha v                                      (BiCgStab.hpp:189)
+	SLAB_BICG_T = 9,      // t = A (s iM); <s,s>, <t,s>, <t,t>                    (BiCgStab.hpp:192-212)
+	SLAB_BICG_XR = 10,    // x += alpha p iM + omega s iM; r = s - omega t; <r,r>, <r, r_hat>  (:216-224)
+	SLAB_BICG_X = 11,     // x += alpha p iM (early exit on s)                    (BiCgStab.hpp:193-199)
+	SLAB_CG_P = 12,       // p = r iM (first) or r iM + beta p                    (Cg.hpp:144-147, :188)
+	SLAB_MODES = 13
 };
 
+__host__ __device__ constexpr bool mode_stencil(int m) { return m <= 5 || m == 7 || m == 9; }
+__host__ __device__ constexpr bool mode_scaled(int m) { return m == 4 || m == 5 || m == 7 || m == 9; }
+__host__ __device__ constexpr int mode_dots(int m) {
+	switch (m) {
+	case SLAB_SETUP: case SLAB_CG_SP: case SLAB_CG_UPDATE: case SLAB_BICG_XR: return 2;
+	case SLAB_PCG_SETUP: case SLAB_PCG_ITER: case SLAB_BICG_T: return 3;
+	case SLAB_BICG_V: return 1;
+	default: return 0;
+	}
+}
+
 template <int MODE>
-__global__ void __launch_bounds__(kSlabThreads) k_slab_sweep(SlabGeo g, Coef k, int z_lo, int z_hi, double iM,
-                                                             double alpha, int first, const double *__restrict__ src,
-                                                             double *x, double *r, const double *__restrict__ b,
-                                                             double *y, double *chunk_part) {
+__global__ void __launch_bounds__(kSlabThreads) k_slab_sweep(SlabGeo g, Coef k, int z_lo, int z_hi,
+                                                             sedi_slab_args a, double *chunk_part) {
 	const int z = z_lo + (int)blockIdx.y;
 	if (z >= z_hi) return;
 	const int c = blockIdx.x;
 	int r0, r1;
 	chunk_rows(g, c, &r0, &r1);
-	double v[2] = {0.0, 0.0};
+	constexpr int ND = mode_dots(MODE) > 0 ? mode_dots(MODE) : 1;
+	double v[ND];
+#pragma unroll
+	for (int d = 0; d < ND; d++) v[d] = 0.0;
+	const double iM = a.iM;
 	const long long n_in = (long long)(r1 - r0) * g.n1;
 	for (long long t = threadIdx.x; t < n_in; t += kSlabThreads) {
 		const int i2 = r0 + (int)(t / g.n1), i1 = (int)(t % g.n1);
 		const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + i1;
-		const double a = slab_stencil(g, k, src, z, i2, i1);
+		double st = 0.0;
+		if (mode_stencil(MODE)) st = slab_stencil(g, k, a.src, mode_scaled(MODE), iM, z, i2, i1);
 		if (MODE == SLAB_SETUP) {
-			const double bi = b[i];
-			const double ri = add(bi, mul(-1.0, a));  // combine2(1.0, b, -1.0, Ax, r)
-			r[i] = ri;
+			const double bi = a.b[i];
+			const double ri = add(bi, mul(-1.0, st));  // combine2(1.0, b, -1.0, Ax, r)
+			a.r[i] = ri;
 			v[0] = fma(bi, bi, v[0]);
 			v[1] = fma(ri, ri, v[1]);
-		} else if (MODE == SLAB_SP) {
-			const double pi = src[i];
-			v[0] = fma(a, pi, v[0]);
-			if (first) {
-				const double ri = r[i];
+		} else if (MODE == SLAB_CG_SP) {
+			const double pi = a.src[i];
+			v[0] = fma(st, pi, v[0]);
+			if (a.first) {
+				const double ri = a.r[i];
 				v[1] = fma(ri, mul(ri, iM), v[1]);
 			}
-		} else if (MODE == SLAB_UPDATE) {
-			const double pi = src[i];
-			x[i] = add(x[i], mul(alpha, pi));              // :169
-			const double ri = add(r[i], mul(-alpha, a));   // :172
-			r[i] = ri;
-			const double ui = mul(ri, iM);                 // :175
+		} else if (MODE == SLAB_CG_UPDATE) {
+			const double pi = a.src[i];
+			a.x[i] = add(a.x[i], mul(a.alpha, pi));          // :169
+			const double ri = add(a.r[i], mul(-a.alpha, st));  // :172
+			a.r[i] = ri;
+			const double ui = mul(ri, iM);                     // :175
 			v[0] = fma(ri, ui, v[0]);
 			v[1] = fma(ri, ri, v[1]);
-		} else {
-			y[i] = a;
+		} else if (MODE == SLAB_APPLY) {
+			a.y[i] = st;
+		} else if (MODE == SLAB_PCG_SETUP) {
+			const double ri = a.src[i];
+			const double ui = mul(ri, iM);  // :138
+			a.u[i] = ui;
+			a.w[i] = st;                    // :141-143
+			a.q[i] = a.s[i] = a.p[i] = a.z[i] = 0.0;  // :146-149
+			v[0] = fma(ri, ui, v[0]);
+			v[1] = fma(st, ui, v[1]);
+			v[2] = fma(ri, ri, v[2]);
+		} else if (MODE == SLAB_PCG_ITER) {
+			const double wi = a.src[i];
+			const double mi = mul(wi, iM);                            // :158
+			const double qi = add(mi, mul(a.beta, a.q[i]));          // :200
+			const double si = add(wi, mul(a.beta, a.s[i]));          // :203
+			const double ui0 = a.u[i];
+			const double pi = add(ui0, mul(a.beta, a.p[i]));         // :206
+			const double zi = add(st, mul(a.beta, a.z[i]));          // :209
+			const double ri = add(a.r[i], mul(-a.alpha, si));        // :212
+			const double xi = add(a.x[i], mul(a.alpha, pi));         // :215
+			const double ui = add(ui0, mul(-a.alpha, qi));           // :218
+			const double wni = add(wi, mul(-a.alpha, zi));           // :221
+			a.q[i] = qi;
+			a.s[i] = si;
+			a.p[i] = pi;
+			a.z[i] = zi;
+			a.r[i] = ri;
+			a.x[i] = xi;
+			a.u[i] = ui;
+			a.wn[i] = wni;
+			v[0] = fma(ri, ui, v[0]);   // next <r,u>
+			v[1] = fma(wni, ui, v[1]);  // next <w,u>
+			v[2] = fma(ri, ri, v[2]);   // next <r,r>
+		} else if (MODE == SLAB_BICG_P) {
+			const double ri = a.r[i];
+			a.p[i] = a.first ? ri : add(add(ri, mul(a.beta, a.p[i])), mul(a.bo, a.v[i]));  // :168, :171
+		} else if (MODE == SLAB_BICG_V) {
+			a.v[i] = st;  // v = A p_hat (:178-180)
+			v[0] = fma(st, a.rhat[i], v[0]);
+		} else if (MODE == SLAB_BICG_S) {
+			a.s[i] = add(a.r[i], mul(-a.alpha, a.v[i]));  // :189
+		} else if (MODE == SLAB_BICG_T) {
+			const double si = a.src[i];
+			a.t[i] = st;  // t = A s_hat (:204-206)
+			v[0] = fma(si, si, v[0]);
+			v[1] = fma(st, si, v[1]);
+			v[2] = fma(st, st, v[2]);
+		} else if (MODE == SLAB_BICG_XR) {
+			const double si = a.s[i];
+			const double phi = mul(a.p[i], iM), shi = mul(si, iM);
+			a.x[i] = add(add(a.x[i], mul(a.alpha, phi)), mul(a.omega, shi));  // :216
+			const double ri = add(si, mul(-a.omega, a.t[i]));                   // :219
+			a.r[i] = ri;
+			v[0] = fma(ri, ri, v[0]);
+			v[1] = fma(ri, a.rhat[i], v[1]);
+		} else if (MODE == SLAB_BICG_X) {
+			a.x[i] = add(a.x[i], mul(a.alpha, mul(a.p[i], iM)));  // :196
+		} else {  // SLAB_CG_P
+			const double ui = mul(a.r[i], iM);
+			a.p[i] = a.first ? ui : add(ui, mul(a.beta, a.p[i]));
 		}
 	}
-	if (MODE == SLAB_APPLY) return;
-	block_total<2>(v);
+	if (mode_dots(MODE) == 0) return;
+	block_total<ND>(v);
 	if (threadIdx.x == 0) {
-		double *o = chunk_part + ((size_t)(z - 1) * kSlabChunks + c) * 2;
-		o[0] = v[0];
-		o[1] = v[1];
+		double *o = chunk_part + ((size_t)(z - 1) * kSlabChunks + c) * kSlabDots;
+		for (int d = 0; d < kSlabDots; d++) o[d] = d < mode_dots(MODE) ? v[d < ND ? d : 0] : 0.0;
 	}
 }
 
@@ -135,20 +223,10 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_sweep(SlabGeo g, Coef k, 
 __global__ void k_slab_plane_sums(int z_lo, int z_hi, const double *chunk_part, double *plane_part) {
 	const int z = z_lo + blockIdx.x * blockDim.x + threadIdx.x;
 	if (z >= z_hi) return;
-	for (int d = 0; d < 2; d++) {
+	for (int d = 0; d < kSlabDots; d++) {
 		double s = 0.0;
-		for (int c = 0; c < kSlabChunks; c++) s += chunk_part[((size_t)(z - 1) * kSlabChunks + c) * 2 + d];
-		plane_part[(size_t)(z - 1) * 2 + d] = s;
-	}
-}
-
-// p = u + beta p with u = r .* iM (p = u on the first iteration) on the
-// slab's own planes (Cg.hpp:144-147, :175, :188).
-__global__ void __launch_bounds__(kSlabThreads) k_slab_p(long long n, const double *__restrict__ r, double *p,
-                                                         double iM, double beta, int first) {
-	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-		const double u = mul(r[i], iM);
-		p[i] = first ? u : add(u, mul(beta, p[i]));
+		for (int c = 0; c < kSlabChunks; c++) s += chunk_part[((size_t)(z - 1) * kSlabChunks + c) * kSlabDots + d];
+		plane_part[(size_t)(z - 1) * kSlabDots + d] = s;
 	}
 }
 
@@ -179,6 +257,33 @@ bool slab_args(long n1, long n2, long nloc) {
 	       (double)n1 * n2 * (nloc + 2) < 4.0e9;
 }
 
+// Pointers each mode reads or writes (src is the stencil input or the mode's
+// first vector).
+bool mode_args_ok(int mode, const sedi_slab_args &a) {
+	switch (mode) {
+	case SLAB_SETUP: return a.src && a.r && a.b;
+	case SLAB_CG_SP: return a.src && (!a.first || a.r);
+	case SLAB_CG_UPDATE: return a.src && a.x && a.r;
+	case SLAB_APPLY: return a.src && a.y;
+	case SLAB_PCG_SETUP: return a.src && a.u && a.w && a.q && a.s && a.p && a.z;
+	case SLAB_PCG_ITER: return a.src && a.x && a.r && a.u && a.wn && a.q && a.s && a.p && a.z && a.wn != a.src;
+	case SLAB_BICG_P: return a.r && a.p && (a.first || a.v);
+	case SLAB_BICG_V: return a.src && a.v && a.rhat;
+	case SLAB_BICG_S: return a.r && a.v && a.s;
+	case SLAB_BICG_T: return a.src && a.t;
+	case SLAB_BICG_XR: return a.x && a.p && a.s && a.t && a.r && a.rhat;
+	case SLAB_BICG_X: return a.x && a.p;
+	case SLAB_CG_P: return a.r && a.p;
+	default: return false;
+	}
+}
+
+template <int MODE>
+void launch_mode(SlabGeo g, Coef k, int z_lo, int z_hi, const sedi_slab_args &a, double *chunk, cudaStream_t s) {
+	const dim3 grid(kSlabChunks, (unsigned)(z_hi - z_lo));
+	k_slab_sweep<MODE><<<grid, kSlabThreads, 0, s>>>(g, k, z_lo, z_hi, a, chunk);
+}
+
 }  // namespace
 
 }  // namespace sedi
@@ -188,47 +293,34 @@ using namespace sedi;
 extern "C" {
 
 int sedi_slab_sweep(int mode, long n1, long n2, long nloc, double a, double b, double c, long z_lo, long z_hi,
-                    double iM, double alpha, int first, const double *src, double *x, double *r, const double *bvec,
-                    double *y, double *chunk_part, double *plane_part, void *stream) {
-	if (!slab_args(n1, n2, nloc) || mode < 0 || mode > 3 || z_lo < 1 || z_hi > nloc + 1 || z_lo > z_hi || !src)
+                    const sedi_slab_args *args, double *chunk_part, double *plane_part, void *stream) {
+	if (!slab_args(n1, n2, nloc) || !args || mode < 0 || mode >= SLAB_MODES || z_lo < 1 || z_hi > nloc + 1 ||
+	    z_lo > z_hi)
 		return SEDI_ERR_ARG;
-	if (mode != SLAB_APPLY && (!chunk_part || !plane_part)) return SEDI_ERR_ARG;
-	if ((mode == SLAB_SETUP && (!r || !bvec)) || (mode == SLAB_SP && first && !r) ||
-	    (mode == SLAB_UPDATE && (!x || !r)) || (mode == SLAB_APPLY && !y))
-		return SEDI_ERR_ARG;
+	if (!mode_args_ok(mode, *args)) return SEDI_ERR_ARG;
+	const bool dots = mode_dots(mode) > 0;
+	if (dots && (!chunk_part || !plane_part)) return SEDI_ERR_ARG;
 	if (z_lo == z_hi) return 0;
 	SlabGeo g{(int)n1, (int)n2, (int)nloc, (long long)n1 * n2};
 	const Coef k{a, b, c};
 	cudaStream_t s = (cudaStream_t)stream;
-	const dim3 grid(kSlabChunks, (unsigned)(z_hi - z_lo));
+	const int lo = (int)z_lo, hi = (int)z_hi;
 	switch (mode) {
-	case SLAB_SETUP:
-		k_slab_sweep<SLAB_SETUP><<<grid, kSlabThreads, 0, s>>>(g, k, (int)z_lo, (int)z_hi, iM, alpha, first, src, x, r,
-		                                                       bvec, y, chunk_part);
-		break;
-	case SLAB_SP:
-		k_slab_sweep<SLAB_SP><<<grid, kSlabThreads, 0, s>>>(g, k, (int)z_lo, (int)z_hi, iM, alpha, first, src, x, r,
-		                                                    bvec, y, chunk_part);
-		break;
-	case SLAB_UPDATE:
-		k_slab_sweep<SLAB_UPDATE><<<grid, kSlabThreads, 0, s>>>(g, k, (int)z_lo, (int)z_hi, iM, alpha, first, src, x,
-		                                                        r, bvec, y, chunk_part);
-		break;
-	default:
-		k_slab_sweep<SLAB_APPLY><<<grid, kSlabThreads, 0, s>>>(g, k, (int)z_lo, (int)z_hi, iM, alpha, first, src, x,
-		                                                       r, bvec, y, chunk_part);
-		break;
+	case 0: launch_mode<0>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 1: launch_mode<1>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 2: launch_mode<2>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 3: launch_mode<3>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 4: launch_mode<4>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 5: launch_mode<5>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 6: launch_mode<6>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 7: launch_mode<7>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 8: launch_mode<8>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 9: launch_mode<9>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 10: launch_mode<10>(g, k, lo, hi, *args, chunk_part, s); break;
+	case 11: launch_mode<11>(g, k, lo, hi, *args, chunk_part, s); break;
+	default: launch_mode<12>(g, k, lo, hi, *args, chunk_part, s); break;
 	}
-	if (mode != SLAB_APPLY) {
-		const int nz = (int)(z_hi - z_lo);
-		k_slab_plane_sums<<<(nz + 127) / 128, 128, 0, s>>>((int)z_lo, (int)z_hi, chunk_part, plane_part);
-	}
-	return cudaGetLastError() == cudaSuccess ? 0 : SEDI_ERR_CUDA;
-}
-
-int sedi_slab_p(long n, const double *r, double *p, double iM, double beta, int first, void *stream) {
-	if (n < 1 || !r || !p) return SEDI_ERR_ARG;
-	k_slab_p<<<blocks_for(n), kSlabThreads, 0, (cudaStream_t)stream>>>(n, r, p, iM, beta, first);
+	if (dots) k_slab_plane_sums<<<(hi - lo + 127) / 128, 128, 0, s>>>(lo, hi, chunk_part, plane_part);
 	return cudaGetLastError() == cudaSuccess ? 0 : SEDI_ERR_CUDA;
 }
 

@@ -1,4 +1,4 @@
-"""Slab (i3) domain decomposition of the FP64 CG method across GPUs (``-p 1x1xP``).
+"""Slab (i3) domain decomposition of the FP64 solvers across GPUs (``-p 1x1xP``).
 
 The reference scales one grid over many processes with a block domain
 decomposition (DomainDecomposition.hpp:51-80), a ghost layer refreshed by a
@@ -16,17 +16,22 @@ device copies).
   nloc -- the reference's inner/border split.
 * Dot products come back per plane, each summed in an order that depends only
   on (n1, n2); the planes are gathered from all slabs and added in global
-  plane order with ``math.fsum``.  x, r and p are therefore identical bit for
-  bit for every P, including P = 1.
+  plane order with ``math.fsum``.  Every vector of the solve is therefore
+  identical bit for bit for every P, including P = 1.
+* The three solvers are the reference's CG (Cg.hpp), pipelined CG
+  (PipelinedCg.hpp) and BiCGStab (BiCgStab.hpp) with the constant Jacobi
+  preconditioner 1/a; each sweep fuses a stencil with the elementwise updates
+  and dot products around it.
 * The probe of a decomposed run is the global probe (std::mt19937(seed + k)
   over the whole grid, i1 fastest); each slab fills its own range of it.  The
   reference instead fills each rank's cells from the rank's own generator
   (DistrRngStd.hpp:22-42), so its probes depend on -p.
 
 The per-slab work runs in the CUDA library (``sedi_slab_*`` in the C ABI);
-``GpuSlabBackend`` binds it.  The loop itself (``SlabCg``) only sequences
-kernels and collectives, so any object with the backend's methods can run
-it (the CPU tests use a NumPy one on gloo ranks).
+``GpuSlabBackend`` binds it.  The solver loops (``SlabCg``,
+``SlabPipelinedCg``, ``SlabBiCgStab``) only sequence kernels and
+collectives, so any object with the backend's methods can run them (the CPU
+tests use a NumPy one on gloo ranks).
 """
 import ctypes
 import math
@@ -34,9 +39,26 @@ import time
 
 import numpy as np
 
-__all__ = ["slab_range", "parse_decomposition", "GpuSlabBackend", "SlabCg"]
+__all__ = ["slab_range", "parse_decomposition", "GpuSlabBackend", "SlabCg", "SlabPipelinedCg", "SlabBiCgStab",
+           "slab_solver", "MODE_DOTS"]
 
-SETUP, SP, UPDATE, APPLY = 0, 1, 2, 3  # sedi_slab_sweep modes
+# sedi_slab_sweep modes (include/sedi_b200.h)
+(SETUP, CG_SP, CG_UPDATE, APPLY, PCG_SETUP, PCG_ITER, BICG_P, BICG_V, BICG_S, BICG_T, BICG_XR, BICG_X,
+ CG_P) = range(13)
+MODE_DOTS = {SETUP: 2, CG_SP: 2, CG_UPDATE: 2, PCG_SETUP: 3, PCG_ITER: 3, BICG_V: 1, BICG_T: 3, BICG_XR: 2}
+DOTS = 3  # dot products per plane in a plane_part row
+VECTORS = ("src", "b", "rhat", "x", "r", "y", "u", "w", "wn", "q", "s", "p", "z", "v", "t")
+SCALARS = ("iM", "alpha", "beta", "bo", "omega")
+
+
+def _fdiv(a, b):
+    """a / b with IEEE semantics (inf or nan on a zero divisor), as the reference's C++ divides."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return float(np.float64(a) / np.float64(b))
+
+
+def _sqrt(a):
+    return math.sqrt(a) if a >= 0.0 else float("nan")
 
 
 def slab_range(n3, parts, index):
@@ -60,6 +82,12 @@ def parse_decomposition(text, n3):
     return p[2]
 
 
+class _SlabArgs(ctypes.Structure):
+    """sedi_slab_args (include/sedi_b200.h)."""
+    _fields_ = ([(n, ctypes.c_void_p) for n in VECTORS] + [(n, ctypes.c_double) for n in SCALARS]
+                + [("first", ctypes.c_int)])
+
+
 class GpuSlabBackend:
     """Slab vectors as CUDA float64 tensors; the sweeps are the library's
     sedi_slab_* kernels on the current torch stream."""
@@ -72,8 +100,7 @@ class GpuSlabBackend:
         vp, c_long, c_double, c_int = ctypes.c_void_p, ctypes.c_long, ctypes.c_double, ctypes.c_int
         L = self.lib
         L.sedi_slab_sweep.argtypes = [c_int, c_long, c_long, c_long, c_double, c_double, c_double, c_long, c_long,
-                                      c_double, c_double, c_int, vp, vp, vp, vp, vp, vp, vp, vp]
-        L.sedi_slab_p.argtypes = [c_long, vp, vp, c_double, c_double, c_int, vp]
+                                      ctypes.POINTER(_SlabArgs), vp, vp, vp]
         L.sedi_slab_accumulate.argtypes = [c_long, vp, vp, vp, vp, c_int, vp]
         L.sedi_slab_divide.argtypes = [c_long, vp, vp, vp, vp]
         self.chunks = int(L.sedi_slab_chunks())
@@ -98,36 +125,38 @@ class GpuSlabBackend:
     def set_interior(self, buf, host):
         buf[1:-1].copy_(self.torch.from_numpy(np.ascontiguousarray(host).reshape(buf.shape[0] - 2, self.n2, self.n1)))
 
+    def copy(self, dst, src):
+        dst.copy_(src)
+
     def to_numpy(self, t):
         return t.detach().cpu().numpy()
 
-    def _parts(self, nloc):
+    def _chunk(self, nloc):
         if nloc not in self._scratch:
-            self._scratch[nloc] = (self.torch.zeros(nloc * self.chunks * 2, dtype=self.torch.float64,
-                                                    device=self.device),
-                                   self.torch.zeros((nloc, 2), dtype=self.torch.float64, device=self.device))
+            self._scratch[nloc] = self.torch.zeros(nloc * self.chunks * DOTS, dtype=self.torch.float64,
+                                                   device=self.device)
         return self._scratch[nloc]
 
     def new_plane_part(self, nloc):
-        return self.torch.zeros((nloc, 2), dtype=self.torch.float64, device=self.device)
+        return self.torch.zeros((nloc, DOTS), dtype=self.torch.float64, device=self.device)
 
-    def sweep(self, mode, src, z_lo, z_hi, plane_part=None, x=None, r=None, b=None, y=None, iM=1.0 / 6.0,
-              alpha=0.0, first=False):
-        nloc = src.shape[0] - 2
-        chunk, _ = self._parts(nloc)
+    def sweep(self, mode, nloc, z_lo, z_hi, plane_part=None, first=False, **kw):
+        """sedi_slab_sweep over ghosted planes [z_lo, z_hi): vectors (slab
+        tensors) and scalars by their sedi_slab_args names."""
+        args = _SlabArgs()
+        for k, v in kw.items():
+            if k in SCALARS:
+                setattr(args, k, float(v))
+            elif v is not None:
+                setattr(args, k, v.data_ptr())
+        args.first = int(bool(first))
+        dots = mode in MODE_DOTS
         a, bb, c = self.coef
-        rc = self.lib.sedi_slab_sweep(mode, self.n1, self.n2, nloc, a, bb, c, z_lo, z_hi, iM, alpha, int(first),
-                                      self._ptr(src), self._ptr(x), self._ptr(r), self._ptr(b), self._ptr(y),
-                                      self._ptr(chunk) if mode != APPLY else None,
-                                      self._ptr(plane_part) if mode != APPLY else None, self._stream())
+        rc = self.lib.sedi_slab_sweep(mode, self.n1, self.n2, nloc, a, bb, c, z_lo, z_hi, ctypes.byref(args),
+                                      self._ptr(self._chunk(nloc)) if dots else None,
+                                      self._ptr(plane_part) if dots else None, self._stream())
         if rc != 0:
-            raise RuntimeError(f"sedi_slab_sweep failed ({rc})")
-
-    def p_update(self, r, p, iM, beta, first):
-        n = (r.shape[0] - 2) * self.n1 * self.n2
-        rc = self.lib.sedi_slab_p(n, self._ptr(r[1:-1]), self._ptr(p[1:-1]), iM, beta, int(first), self._stream())
-        if rc != 0:
-            raise RuntimeError(f"sedi_slab_p failed ({rc})")
+            raise RuntimeError(f"sedi_slab_sweep mode {mode} failed ({rc})")
 
     def accumulate(self, x, v, t, q, reset):
         n = (x.shape[0] - 2) * self.n1 * self.n2
@@ -151,16 +180,21 @@ class GpuSlabBackend:
         self.set_interior(buf, host)
 
 
-class SlabCg:
-    """The reference CG (Cg.hpp:70-207) over i3 slabs.
+class _SlabSolver:
+    """Slab storage, halo exchange, plane-ordered dot products and the
+    estimator loop shared by the three solvers.
 
     ``parts`` slabs along i3.  Under torch.distributed (``group``, every
     rank calling with the same arguments) rank r holds slab r and the world
     size must equal ``parts``; with ``loopback=True`` this process holds all
     slabs (one GPU, halos by device copies).  ``mode`` is the reference's
-    sync bit set (Cg.hpp:36-40): bit 0 computes the whole slab after the
-    exchange instead of overlapping the inner planes with it.
+    sync bit set (Cg.hpp:36-40, PipelinedCg.hpp:33-37, BiCgStab.hpp:36-40):
+    bit 0 computes the whole slab after the exchange instead of overlapping
+    the inner planes with it.
     """
+
+    NAME = ""
+    WORK = ()  # names of the work vectors of one solve
 
     def __init__(self, dims, parts, stencil=None, group=None, backend=None, loopback=False, mode=0):
         import torch.distributed as dist
@@ -191,6 +225,10 @@ class SlabCg:
         """One zero slab vector per local slab."""
         return [self.backend.zeros(self.ranges[s][1]) for s in self.local]
 
+    def work(self):
+        """The work vectors of one solve, by name."""
+        return {k: self.zeros() for k in self.WORK}
+
     def _nloc(self, j):
         return self.ranges[self.local[j]][1]
 
@@ -209,7 +247,7 @@ class SlabCg:
                 if nb in owner:
                     jn = owner[nb]
                     src = 1 if nb > s else self._nloc(jn)  # the neighbour's plane next to this slab
-                    buf[ghost].copy_(bufs[jn][src])
+                    self.backend.copy(buf[ghost], bufs[jn][src])
                 else:
                     ops.append(self.dist.P2POp(self.dist.irecv, buf[ghost], nb, self.group))
                     ops.append(self.dist.P2POp(self.dist.isend, buf[mine], nb, self.group))
@@ -222,14 +260,16 @@ class SlabCg:
         self.timers["halo_wait"] += time.perf_counter() - t0
 
     def _dots(self, plane_parts):
-        """Global dot products from the local slabs' per-plane partials:
-        gathered from every rank, added in global plane order."""
+        """The three global dot products of a sweep from the local slabs'
+        per-plane partials: gathered from every rank, added in global plane
+        order (DistrAsyncDotProds.hpp:85-136 sums rank partials with an
+        allreduce instead)."""
         import torch
         t0 = time.perf_counter()
         loc = torch.cat(plane_parts, 0) if len(plane_parts) > 1 else plane_parts[0]
         if self.world > 1:
             most = max(c for _, c in self.ranges)
-            pad = torch.zeros((most, 2), dtype=loc.dtype, device=loc.device)
+            pad = torch.zeros((most, DOTS), dtype=loc.dtype, device=loc.device)
             pad[:loc.shape[0]] = loc
             got = [torch.empty_like(pad) for _ in range(self.world)]
             self.dist.all_gather(got, pad, group=self.group)
@@ -237,90 +277,72 @@ class SlabCg:
         else:
             allp = self.backend.to_numpy(loc)
         self.timers["dot_comm"] += time.perf_counter() - t0
-        return math.fsum(allp[:, 0].tolist()), math.fsum(allp[:, 1].tolist())
+        return tuple(math.fsum(allp[:, d].tolist()) for d in range(DOTS))
 
-    # ---- fused stencil sweeps ----------------------------------------------
-    def _stencil_sweep(self, mode, srcs, outs, **kw):
-        """Exchange srcs' halos and run `mode` on every local slab: the inner
+    # ---- sweeps --------------------------------------------------------------
+    def _args(self, kw, j):
+        return {k: (v[j] if isinstance(v, list) else v) for k, v in kw.items()}
+
+    def _sweep(self, mode, **kw):
+        """`mode` over every plane of every local slab, no exchange (an
+        elementwise mode, or a stencil whose source's ghosts are current).
+        Returns the per-plane partials (None for a mode without dots)."""
+        parts = []
+        for j in range(len(self.local)):
+            nloc = self._nloc(j)
+            pp = self.backend.new_plane_part(nloc) if mode in MODE_DOTS else None
+            self.backend.sweep(mode, nloc, 1, nloc + 1, pp, **self._args(kw, j))
+            parts.append(pp)
+        return parts
+
+    def _stencil_sweep(self, mode, src, **kw):
+        """Exchange src's halos and run `mode` on every local slab: the inner
         planes while the halos move, then the border planes
         (DistrAsyncStencil.hpp:52-100); mode bit 0 = one sweep after the
         exchange (:87-97)."""
-        reqs = self._exchange(srcs)
+        reqs = self._exchange(src)
+        kw["src"] = src
         parts = []
         overlap = not (self.mode & 1)
         for j in range(len(self.local)):
             nloc = self._nloc(j)
-            pp = self.backend.new_plane_part(nloc) if mode != APPLY else None
+            pp = self.backend.new_plane_part(nloc) if mode in MODE_DOTS else None
             parts.append(pp)
             if overlap and nloc > 2:
-                self.backend.sweep(mode, srcs[j], 2, nloc, pp, **{k: (v[j] if isinstance(v, list) else v)
-                                                                  for k, v in kw.items()})
+                self.backend.sweep(mode, nloc, 2, nloc, pp, **self._args(kw, j))
         self._wait(reqs)
         for j in range(len(self.local)):
             nloc = self._nloc(j)
-            args = {k: (v[j] if isinstance(v, list) else v) for k, v in kw.items()}
+            args = self._args(kw, j)
             if overlap and nloc > 2:
-                self.backend.sweep(mode, srcs[j], 1, 2, parts[j], **args)
-                self.backend.sweep(mode, srcs[j], nloc, nloc + 1, parts[j], **args)
+                self.backend.sweep(mode, nloc, 1, 2, parts[j], **args)
+                self.backend.sweep(mode, nloc, nloc, nloc + 1, parts[j], **args)
             else:
-                self.backend.sweep(mode, srcs[j], 1, nloc + 1, parts[j], **args)
+                self.backend.sweep(mode, nloc, 1, nloc + 1, parts[j], **args)
         return parts
 
     def apply(self, x, y):
         """y = A x (Stencil.hpp:38-54 through DistrAsyncStencil)."""
-        self._stencil_sweep(APPLY, x, None, y=y)
+        self._stencil_sweep(APPLY, x, y=y)
 
-    # ---- the solver --------------------------------------------------------
+    def _residual(self, x, b, r):
+        """r = b - A x; returns (<b,b> with 0 taken as 1, <r,r>) -- the common
+        start of the three solvers (Cg.hpp:112-129, PipelinedCg.hpp:104-123,
+        BiCgStab.hpp:122-139)."""
+        bb, rr, _ = self._dots(self._stencil_sweep(SETUP, x, r=r, b=b))
+        return (1.0 if bb == 0.0 else bb), rr
+
     def solve(self, x, b, maxiter, tol, work=None):
-        """Cg::solve (Cg.hpp:70-207) with iM = 1/a: x (in: first guess, out:
-        solution) and b are lists of local slab vectors.  Returns (result_t,
-        final_err, final_iter)."""
-        r, p = work if work is not None else (self.zeros(), self.zeros())
-        hist = []
-        # r = b - A x; <b,b>, <r,r> (:112-129)
-        bb, rr = self._dots(self._stencil_sweep(SETUP, x, None, r=r, b=b))
-        if bb == 0.0:
-            bb = 1.0
-        err = math.sqrt(rr / bb)
-        hist.append(err)
-        self.last_history = hist
-        if err < tol:  # :130-134
-            return 0, err, 0
-        if maxiter < 1:
-            return 1, err, maxiter
-        ru = 0.0
-        beta = 0.0
-        for it in range(1, maxiter + 1):
-            first = it == 1
-            for j in range(len(self.local)):  # p = u + beta p, u = r .* iM (:144-147, :175, :188)
-                self.backend.p_update(r[j], p[j], self.iM, beta, first)
-            sp, ru1 = self._dots(self._stencil_sweep(SP, p, None, r=r, iM=self.iM, first=first))  # :152-165
-            if first:
-                ru = ru1
-            alpha = ru / sp  # :166
-            # x += alpha p, r -= alpha s, u = r .* iM; <r,u>, <r,r> (:169-182); the ghosts of p are current
-            parts = []
-            for j in range(len(self.local)):
-                pp = self.backend.new_plane_part(self._nloc(j))
-                self.backend.sweep(UPDATE, p[j], 1, self._nloc(j) + 1, pp, x=x[j], r=r[j], iM=self.iM,
-                                   alpha=alpha)
-                parts.append(pp)
-            ru_new, rr = self._dots(parts)
-            beta = ru_new / ru  # :185
-            ru = ru_new
-            err = math.sqrt(rr / bb)  # :191
-            hist.append(err)
-            if err <= tol:  # :193
-                return 0, err, it
-        return 1, err, maxiter  # :197-206
+        raise NotImplementedError
 
+    # ---- the estimator -------------------------------------------------------
     def estimate(self, samples, seed=1234, maxiter=1000, tol=1e-4, ignore_errors=True):
         """The estimator loop (stochastic-estimator.cc:155-216) over the slabs:
         probe k is the global std::mt19937(seed + k) probe; x = 0 (:175);
         t += x .* v, q += v .* v (:195, :198); D = t ./ q (:216).  Returns
         dict(D, t, q: lists of local slab vectors, iters, errs, results, rc)."""
         x, b, t, q = self.zeros(), self.zeros(), self.zeros(), self.zeros()
-        work = (self.zeros(), self.zeros())
+        work = self.work()
         iters, errs, results = [], [], []
         rc = 0
         plane = self.n1 * self.n2
@@ -358,3 +380,168 @@ class SlabCg:
         self.dist.all_gather(got, pad, group=self.group)
         return np.concatenate([self.backend.to_numpy(got[s])[:self.ranges[s][1]].reshape(-1)
                                for s in range(self.parts)])
+
+
+class SlabCg(_SlabSolver):
+    """The reference CG (Cg.hpp:70-207) over i3 slabs."""
+
+    NAME = "Cg"
+    WORK = ("r", "p")
+
+    def solve(self, x, b, maxiter, tol, work=None):
+        """Cg::solve with iM = 1/a: x (in: first guess, out: solution) and b
+        are lists of local slab vectors.  Returns (result_t, final_err,
+        final_iter)."""
+        w = work if work is not None else self.work()
+        r, p = w["r"], w["p"]
+        bb, rr = self._residual(x, b, r)
+        err = _sqrt(_fdiv(rr, bb))
+        hist = [err]
+        self.last_history = hist
+        if err < tol:  # :130-134
+            return 0, err, 0
+        if maxiter < 1:
+            return 1, err, maxiter
+        ru = 0.0
+        beta = 0.0
+        for it in range(1, maxiter + 1):
+            first = it == 1
+            self._sweep(CG_P, r=r, p=p, iM=self.iM, beta=beta, first=first)  # p = u + beta p (:144-147, :188)
+            sp, ru1, _ = self._dots(self._stencil_sweep(CG_SP, p, r=r, iM=self.iM, first=first))  # :152-165
+            if first:
+                ru = ru1
+            alpha = _fdiv(ru, sp)  # :166
+            # x += alpha p, r -= alpha s, u = r .* iM; <r,u>, <r,r> (:169-182); the ghosts of p are current
+            ru_new, rr, _ = self._dots(self._sweep(CG_UPDATE, src=p, x=x, r=r, iM=self.iM, alpha=alpha))
+            beta = _fdiv(ru_new, ru)  # :185
+            ru = ru_new
+            err = _sqrt(_fdiv(rr, bb))  # :191
+            hist.append(err)
+            if err <= tol:  # :193
+                return 0, err, it
+        return 1, err, maxiter  # :197-206
+
+
+class SlabPipelinedCg(_SlabSolver):
+    """The reference pipelined CG (PipelinedCg.hpp:75-243) over i3 slabs.
+
+    One fused sweep per iteration: m = w .* iM and n = A m on the fly, the
+    eight vector updates, and the next iteration's <r,u>, <w,u>, <r,r> -- the
+    reference computes those dots at the top of the next iteration from the
+    same vectors (:152-180).  w is double-buffered because the stencil reads
+    the neighbours' w while the update writes it.
+    """
+
+    NAME = "PipelinedCg"
+    WORK = ("r", "u", "w", "wn", "q", "s", "p", "z")
+
+    def solve(self, x, b, maxiter, tol, work=None):
+        W = work if work is not None else self.work()
+        r, u, q, s, p, z = (W[k] for k in ("r", "u", "q", "s", "p", "z"))
+        w, wn = W["w"], W["wn"]
+        bb, rr = self._residual(x, b, r)
+        err = _sqrt(_fdiv(rr, bb))
+        hist = [err]
+        self.last_history = hist
+        if err < tol:  # :124-128
+            return 0, err, 0
+        # u = r .* iM, w = A u, z = q = s = p = 0 (:138-149); dots of iteration 1 (:155, :169-172)
+        gamma, delta, rr = self._dots(self._stencil_sweep(PCG_SETUP, r, u=u, w=w, q=q, s=s, p=p, z=z, iM=self.iM))
+        alpha = beta = 0.0
+        for it in range(1, maxiter + 1):
+            if it > 1:  # :175-181
+                beta = _fdiv(gamma, gamma_old)
+                alpha = _fdiv(1.0, _fdiv(delta, gamma) - _fdiv(beta, alpha))
+            else:
+                beta = 0.0
+                alpha = _fdiv(gamma, delta)
+            gamma_old = gamma
+            rr_it = rr
+            gamma, delta, rr = self._dots(self._stencil_sweep(PCG_ITER, w, x=x, r=r, u=u, wn=wn, q=q, s=s, p=p, z=z,
+                                                              iM=self.iM, alpha=alpha, beta=beta))
+            w, wn = wn, w
+            err = _sqrt(_fdiv(rr_it, bb))  # :227 (the <r,r> of the iteration's start)
+            hist.append(err)
+            if err <= tol:  # :229
+                return 0, err, it
+        return 1, err, maxiter  # :233-242
+
+
+class SlabBiCgStab(_SlabSolver):
+    """The reference BiCGStab (BiCgStab.hpp:75-263) over i3 slabs."""
+
+    NAME = "BiCgStab"
+    WORK = ("r", "rhat", "p", "v", "s", "t")
+
+    def solve(self, x, b, maxiter, tol, work=None):
+        W = work if work is not None else self.work()
+        r, rhat, p, v, s, t = (W[k] for k in self.WORK)
+        iM = self.iM
+        bb, rr = self._residual(x, b, r)
+        err = _sqrt(_fdiv(rr, bb))
+        hist = [err]
+        self.last_history = hist
+        if err < tol:  # :142-146
+            return 0, err, 0
+        omega, alpha, rho_prev = 1.0, 0.0, 0.0  # :148-151
+        for j in range(len(self.local)):
+            self.backend.copy(rhat[j], r[j])  # :154
+        rho_next = rr  # <r, r_hat> with r_hat = r: the same sums as <r,r>
+        s_norm2 = 0.0
+        it = maxiter + 1
+        for k in range(1, maxiter + 1):
+            rho = rho_next  # :160-161
+            if rho == 0.0:  # :163
+                it = k
+                break
+            if k > 1:
+                beta = _fdiv(rho, rho_prev) * _fdiv(alpha, omega)  # :167
+                self._sweep(BICG_P, r=r, p=p, v=v, beta=beta, bo=-beta * omega)  # :169
+            else:
+                self._sweep(BICG_P, r=r, p=p, first=True)  # :172
+            vr, _, _ = self._dots(self._stencil_sweep(BICG_V, p, v=v, rhat=rhat, iM=iM))  # :176-186
+            alpha = _fdiv(rho, vr)  # :187
+            self._sweep(BICG_S, r=r, v=v, s=s, alpha=alpha)  # :190
+            # t = A (s .* iM) with <s,s>, <t,s>, <t,t>: t is computed before the
+            # early-exit test on <s,s> (:193-199) and unused when it exits.
+            ss, ts, tt = self._dots(self._stencil_sweep(BICG_T, s, t=t, iM=iM))
+            s_norm2 = ss
+            if ss < tol * tol:  # :195
+                self._sweep(BICG_X, x=x, p=p, alpha=alpha, iM=iM)  # :197
+                it = k
+                break
+            omega = _fdiv(ts, tt)  # :213
+            rr, rho_next, _ = self._dots(self._sweep(BICG_XR, x=x, p=p, s=s, t=t, r=r, rhat=rhat, alpha=alpha,
+                                                     omega=omega, iM=iM))  # :217-224
+            err = _sqrt(_fdiv(rr, bb))  # :227
+            hist.append(err)
+            if err <= tol:  # :229
+                it = k
+                break
+            if omega == 0.0:  # :230
+                it = k
+                break
+            rho_prev = rho  # :232
+        if err <= tol:  # :236-240
+            return 0, err, it
+        if s_norm2 <= tol * tol:  # :242-246
+            return 0, _sqrt(_fdiv(s_norm2, bb)), it
+        if omega == 0.0:  # :248-252
+            return 3, err, it
+        if rho == 0.0:  # :254-258
+            return 2, err, it
+        return 1, err, maxiter  # :260-263
+
+
+SOLVERS = {"cg": SlabCg, "pcg": SlabPipelinedCg, "pipelined_cg": SlabPipelinedCg, "bicgstab": SlabBiCgStab,
+           2: SlabCg, 3: SlabPipelinedCg, 1: SlabBiCgStab}
+
+
+def slab_solver(solver, dims, parts, **kw):
+    """A slab solver by name ("cg", "pcg", "bicgstab") or the library's
+    solver id (SEDI_CG, SEDI_PIPELINED_CG, SEDI_BICGSTAB)."""
+    try:
+        cls = SOLVERS[solver.lower() if isinstance(solver, str) else int(solver)]
+    except KeyError:
+        raise ValueError(f"unknown solver {solver!r}")
+    return cls(dims, parts, **kw)
