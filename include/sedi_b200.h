@@ -340,16 +340,17 @@ int sedi_server_stats(const sedi_server *srv, double *peak_bytes, double *budget
  * measurement on scratch contexts: the lane-slice width of the interleaved
  * Krylov fields (FP32 8 or 4 lanes, FP64 8, 4 or 2), the i3 split of the
  * sweeps, how many planes ahead of its TMA loads a sweep prefetches into L2
- * (0, 2, 4 or 8), for CG the form of its sweep A (1: a ring of computed
- * planes on 32x32 tiles; 2: in place, 32x16 tiles, two blocks per SM; 3: in
- * place, 32x32 tiles, six stages), and with flags & 1 the iterations per
+ * (0, 2, 4 or 8), for CG and BiCGStab the form of the narrow sweeps (CG's
+ * sweep A, BiCGStab's sweeps 2 and 3; 1: a ring of computed planes on 32x32
+ * tiles; 2: in place, 32x16 tiles, two blocks per SM; 3: in place, 32x32
+ * tiles, six stages), and with flags & 1 the iterations per
  * captured graph and (mixed
  * precision) the reliable-update period in 20..50, the last two by timing a
  * real estimate of `batch` probes seeded `seed` to `tol`.  The choice is kept
  * for the process and used by every context created afterwards with the
  * same parameters (and by the server's admission sizes).
  * choice[0..5] = slice width, i3 chunks (0: the built-in model), period,
- * iterations per graph, L2 prefetch distance in planes, sweep-A form; *score_ms (optional)
+ * iterations per graph, L2 prefetch distance in planes, narrow-sweep form; *score_ms (optional)
  * = the winning estimate time (flags & 1) or summed per-iteration sweep
  * time.  Needs device memory for one such context at a time.
  */
@@ -359,9 +360,12 @@ int sedi_autotune(int solver, int precision, int batch, long n1, long n2, long n
 /* Record launch choices for contexts of this solver, precision, batch size
  * and grid without measuring (no counterpart in the reference): a caller
  * that saved an earlier sedi_autotune result (choice[0..5] as there; 0
- * selects the built-in choice of the first four and of the sweep-A form, -1
- * that of the prefetch distance) sets it again at start-up.  Host-only;
- * SEDI_ERR_ARG on bad values. */
+ * selects the built-in choice of the first four and of the narrow-sweep form, -1
+ * that of the prefetch distance) sets it again at start-up.  With
+ * SEDI_PREC_FP64 and batch 1 it sets the single-vector streaming sweeps
+ * (even n1, 2^22 points or more): i3 chunks, prefetch distance and
+ * narrow-sweep form (the slice width is fixed).  Host-only; SEDI_ERR_ARG on
+ * bad values. */
 int sedi_set_tuning(int solver, int precision, int batch, long n1, long n2, long n3, const int *choice);
 
 /*
@@ -386,7 +390,7 @@ double sedi_mixed_target(const sedi_ctx *ctx);
 /* Launch choices of a batched context: config[0..6] = lane-slice width, i3
  * chunks of a sweep, reliable-update period, iterations per captured graph,
  * lanes (padded right-hand sides), L2 prefetch distance in planes, form of
- * CG's sweep A (see sedi_autotune).  SEDI_ERR_UNSUPPORTED for the
+ * the narrow sweeps (see sedi_autotune).  SEDI_ERR_UNSUPPORTED for the
  * single-vector form. */
 int sedi_ctx_config(const sedi_ctx *ctx, int *config);
 

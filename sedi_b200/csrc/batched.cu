@@ -322,7 +322,32 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) k_stream(SGeo g, const __
 				const Vec<T> &xm3 = zprev[k];
 				const Vec<T> &xp3 = znext[k];
 				Vec<T> y;
-				if (C::PAIRS) {
+				if constexpr (Op::SCALED) {
+					// The ring holds f and the stencil input is f .* iM: FP64
+					// scales each neighbour as the reference rounds p_hat and
+					// s_hat; FP32 folds iM into the coefficients.
+					if constexpr (sizeof(T) == 8) {
+						const T im = op.iMc;
+						if (C::PAIRS) {
+							const T c0 = amul(xc.v[0], im), c1 = amul(xc.v[1], im);
+							y.v[0] = st7<T>(op.ka, op.kb, op.kc, c0, amul(xm1.v[1], im), amul(xm2.v[0], im),
+							                amul(xm3.v[0], im), c1, amul(xp2.v[0], im), amul(xp3.v[0], im));
+							y.v[1] = st7<T>(op.ka, op.kb, op.kc, c1, c0, amul(xm2.v[1], im), amul(xm3.v[1], im),
+							                amul(xp1.v[0], im), amul(xp2.v[1], im), amul(xp3.v[1], im));
+						} else {
+#pragma unroll
+							for (int e = 0; e < V; e++)
+								y.v[e] = st7<T>(op.ka, op.kb, op.kc, amul(xc.v[e], im), amul(xm1.v[e], im),
+								                amul(xm2.v[e], im), amul(xm3.v[e], im), amul(xp1.v[e], im),
+								                amul(xp2.v[e], im), amul(xp3.v[e], im));
+						}
+					} else {
+#pragma unroll
+						for (int e = 0; e < V; e++)
+							y.v[e] = st7<T>(op.kas, op.kbs, op.kcs, xc.v[e], xm1.v[e], xm2.v[e], xm3.v[e], xp1.v[e],
+							                xp2.v[e], xp3.v[e]);
+					}
+				} else if (C::PAIRS) {
 					// Points 2m, 2m+1 of one vector: i1 neighbours across the pair.
 					y.v[0] = st7<T>(op.ka, op.kb, op.kc, xc.v[0], xm1.v[1], xm2.v[0], xm3.v[0], xc.v[1], xp2.v[0],
 					                xp3.v[0]);
@@ -442,6 +467,9 @@ struct OpBase {
 	static constexpr int NG = 0;    // pointwise fields read with plain loads, prefetched by gload
 	static constexpr bool INPLACE = false;  // stencil input written over source INPLACE_SLOT (no ring)
 	static constexpr int INPLACE_SLOT = 1;
+	// SCALED: src() gives f and the stencil is applied to f .* iMc (the op
+	// provides iMc and, for FP32, the scaled coefficients kas, kbs, kcs).
+	static constexpr bool SCALED = false;
 	T ka, kb, kc;
 	__device__ void gload(long long, Vec<T> *) const {}
 	__device__ bool enabled(const Global *) const { return true; }
@@ -668,18 +696,23 @@ struct OpCgA : OpBase<T> {
 	}
 };
 
-// Sweep A with the stencil input p written over p_old in the stage (KIND 2:
-// two blocks per SM on 32x16 tiles; KIND 3: 32x32 tiles, 6 stages).  p_old
-// is dead once p is formed at a point, and r (slot 0) stays for iteration
-// 1's <r,u>.  The values computed are those of OpCgA.
-template <class T, int K>
-struct OpCgAv : OpCgA<T> {
+// A transforming sweep with its stencil input written over source field
+// SLOT in the stage instead of a ring (KIND 2: two blocks per SM on 32x16
+// tiles; KIND 3: 32x32 tiles, 6 stages).  The op must not read source SLOT
+// at the centre after phase 1; the values computed are those of Op.
+template <class Op, int K, int SLOT = 1>
+struct InPlace : Op {
 	static constexpr int KIND = K;
 	static constexpr bool INPLACE = true;
-	static constexpr int INPLACE_SLOT = 1;
-	OpCgAv() = default;
-	explicit OpCgAv(const OpCgA<T> &o) : OpCgA<T>(o) {}
+	static constexpr int INPLACE_SLOT = SLOT;
+	InPlace() = default;
+	explicit InPlace(const Op &o) : Op(o) {}
 };
+
+// CG sweep A in place: p_old (slot 1) is dead once p is formed at a point,
+// and r (slot 0) stays for iteration 1's <r,u>.
+template <class T, int K>
+using OpCgAv = InPlace<OpCgA<T>, K>;
 
 // ---------------------------------------------------------------------------
 // CG kernel B: s = A p, x += alpha p, r -= alpha s, u = r .* iM, <r,u>, <r,r>;
@@ -985,9 +1018,9 @@ struct OpApply : OpBase<T> {
 template <class T>
 struct OpBicg1 : OpBase<T> {
 	static constexpr int NS = 3, NQ = 0, ND = 1, NG = 1;
-	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = false, SCALED = true;
 	static constexpr int V = Vec<T>::V;
-	T iMc;
+	T iMc, kas, kbs, kcs;
 	T *p0, *p1, *v0, *v1, *rhat;
 	T *pn, *vn;
 	int it;
@@ -1026,15 +1059,11 @@ struct OpBicg1 : OpBase<T> {
 			                  : aadd(aadd(raw[0].v[e], amul(beta[e], raw[1].v[e])), amul(bo[e], raw[2].v[e]));  // :168
 		return o;
 	}
-	__device__ Vec<T> src(const Vec<T> *raw) const {
-		Vec<T> o = pval(raw);
-#pragma unroll
-		for (int e = 0; e < V; e++) o.v[e] = amul(o.v[e], iMc);  // p_hat (:175)
-		return o;
-	}
-	__device__ void out(long long o, long long, int, const Vec<T> &, const Vec<T> &vv, const Vec<T> *, const Vec<T> *rc,
+	// The stencil input is p_hat = p .* iM (:175), formed at each read.
+	__device__ Vec<T> src(const Vec<T> *raw) const { return pval(raw); }
+	__device__ void out(long long o, long long, int, const Vec<T> &pv, const Vec<T> &vv, const Vec<T> *, const Vec<T> *,
 	                    const Vec<T> *gv, double (&part)[ND][V]) const {
-		stg(pn + o, pval(rc));
+		stg(pn + o, pv);
 		stg(vn + o, vv);
 		const Vec<T> &rh = gv[0];  // r_hat
 #pragma unroll
@@ -1052,7 +1081,8 @@ struct OpBicg1 : OpBase<T> {
 template <class T>
 struct OpBicgS : OpBase<T> {  // sweeps 2 and 3 share s, s_hat, t
 	static constexpr int V = Vec<T>::V;
-	T iMc;
+	static constexpr bool SCALED = true;  // the stencil input is s_hat = s .* iM (:201), formed at each read
+	T iMc, kas, kbs, kcs;
 	int it;
 	T alpha[V];
 	__device__ void load_alpha(const Global *gl, const LaneState &ls, int lane) {
@@ -1070,27 +1100,21 @@ struct OpBicgS : OpBase<T> {  // sweeps 2 and 3 share s, s_hat, t
 		for (int e = 0; e < V; e++) o.v[e] = aadd(raw[0].v[e], amul(-alpha[e], raw[1].v[e]));  // :189
 		return o;
 	}
-	__device__ Vec<T> src(const Vec<T> *raw) const {
-		Vec<T> o = sval(raw);
-#pragma unroll
-		for (int e = 0; e < V; e++) o.v[e] = amul(o.v[e], iMc);  // s_hat (:201)
-		return o;
-	}
+	__device__ Vec<T> src(const Vec<T> *raw) const { return sval(raw); }
 };
 
 template <class T>
 struct OpBicg2 : OpBicgS<T> {
 	static constexpr int KIND = 1;
 	static constexpr int NS = 2, NQ = 0, ND = 3;
-	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = false;
 	static constexpr int V = Vec<T>::V;
 	__device__ bool enabled(const Global *) const { return true; }
 	__device__ void begin(const Global *gl, const LaneState &ls, int lane) { this->load_alpha(gl, ls, lane); }
-	__device__ bool raw_center() const { return true; }
+	__device__ bool raw_center() const { return false; }
 	__device__ int q_map(int) const { return 0; }
-	__device__ void out(long long, long long, int, const Vec<T> &, const Vec<T> &tv, const Vec<T> *, const Vec<T> *rc,
+	__device__ void out(long long, long long, int, const Vec<T> &sv, const Vec<T> &tv, const Vec<T> *, const Vec<T> *,
 	                    const Vec<T> *gv, double (&part)[ND][V]) const {
-		const Vec<T> sv = this->sval(rc);
 #pragma unroll
 		for (int e = 0; e < V; e++) {
 			dacc(part[0][e], sv.v[e], sv.v[e]);
@@ -1123,6 +1147,7 @@ struct OpBicg3 : OpBicgS<T> {
 	int mixed;
 	T omega[V];
 	int mode[V];  // 0: full update, 1: early exit on s (x only), 2: finished lane (x, r kept)
+	bool keep_r;  // some lane of this thread keeps r: read the raw r at the centre
 	__device__ bool enabled(const Global *) const { return true; }
 	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
 		this->load_alpha(gl, ls, lane);
@@ -1135,17 +1160,22 @@ struct OpBicg3 : OpBicgS<T> {
 			mode[e] = ls.done[l] ? 2 : (ls.s_exit[l] ? 1 : 0);
 			omega[e] = (T)(mode[e] ? 0.0 : ls.omega[l]);
 		}
+		keep_r = false;
+#pragma unroll
+		for (int e = 0; e < V; e++) keep_r |= mode[e] != 0;
 	}
-	__device__ bool raw_center() const { return true; }
+	__device__ bool raw_center() const { return keep_r; }
 	__device__ void gload(long long o, Vec<T> *gv) const {
 		gv[0] = ldg_rw(x + o);
 		gv[1] = ldg_rw(pc + o);
 		gv[2] = ldg_rw(rhat + o);
 	}
 	__device__ int q_map(int) const { return 0; }
-	__device__ void out(long long o, long long, int, const Vec<T> &shv, const Vec<T> &tv, const Vec<T> *, const Vec<T> *rc,
+	__device__ void out(long long o, long long, int, const Vec<T> &sv, const Vec<T> &tv, const Vec<T> *, const Vec<T> *rc,
 	                    const Vec<T> *gv, double (&part)[ND][V]) const {
-		const Vec<T> sv = this->sval(rc);
+		Vec<T> shv;
+#pragma unroll
+		for (int e = 0; e < V; e++) shv.v[e] = amul(sv.v[e], this->iMc);  // s_hat (:201)
 		Vec<T> xv = gv[0];
 		const Vec<T> &pv = gv[1], &rh = gv[2];
 		Vec<T> rv;
@@ -1376,12 +1406,17 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 #define SEDI_STREAM_PFD 0  // default L2 prefetch distance of the sweeps, in planes (0: none)
 #endif
 #ifndef SEDI_CGA_FORM
-#define SEDI_CGA_FORM 1  // CG sweep A: 1 ring (32x32), 2 in place (32x16, 2 blocks/SM), 3 in place (32x32)
+// Form of the narrow sweeps (CG sweep A, BiCGStab sweeps 2 and 3): 1 ring
+// (32x32), 2 in place (32x16, 2 blocks/SM), 3 in place (32x32, 6 stages).
+// Measured on B200 (CUDA events, kernels alone), mixed CG sweep A at 256^3 x
+// 128 lanes: 4.73 ms ring, 5.19 ms form 2, 4.21 ms form 3; at 128^3 x 64 and
+// in FP64 the forms are within 3%.
+#define SEDI_CGA_FORM 3
 #endif
 struct Tuning {
 	int W = 0, nz = 0, period = 0, chunk = 0;
 	int pfd = -1;   // L2 prefetch distance in planes (-1: SEDI_STREAM_PFD)
-	int acfg = 0;   // form of CG's sweep A (0: SEDI_CGA_FORM)
+	int acfg = 0;   // form of the narrow sweeps (0: SEDI_CGA_FORM)
 };
 struct TuneKey {
 	int solver, precision, R;
@@ -1445,7 +1480,7 @@ struct Batched {
 	int R = 0;
 	bool mixed = false;  // FP32 Krylov fields, FP64 x_hi, reductions and reliable update
 	bool pairs = false;  // single-vector FP64 form: lanes 0/1 = even/odd i1 points of one vector
-	int acfg = SEDI_CGA_FORM;  // form of CG's sweep A (see CfgFor, OpCgAv)
+	int acfg = SEDI_CGA_FORM;  // form of the narrow sweeps (see CfgFor, InPlace)
 	int ks = 0;          // solver whose sweeps run (the mixed pipelined CG runs the CG recurrence)
 	bool aliased = false;  // the Krylov fields belong to the context (single-vector form)
 	const double *graph_hist = nullptr;  // history pointer the captured graph holds
@@ -2030,15 +2065,37 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 	}
 }
 
+// Coefficients of an op whose stencil input is f .* iM (Op::SCALED): FP64
+// scales each value read, FP32 uses the coefficients times iM.
+template <class Op>
+static void set_scaled_coef(const Ctx *c, Op &o) {
+	typedef decltype(o.ka) T;
+	const double iM = 1.0 / c->k.a;
+	o.ka = (T)c->k.a;
+	o.kb = (T)c->k.b;
+	o.kc = (T)c->k.c;
+	o.iMc = (T)iM;
+	o.kas = (T)(c->k.a * iM);
+	o.kbs = (T)(c->k.b * iM);
+	o.kcs = (T)(c->k.c * iM);
+}
+
+// BiCGStab sweeps 2 and 3 in the form of B->acfg: ring, or s written over v
+// (slot 1) in the stage; r (slot 0) stays for the lanes that keep it.
+template <class T, int RBT, bool PAIRS, class Op>
+static void launch_bicg_s(Ctx *c, Batched *B, const Op &o, cudaStream_t s) {
+	switch (B->acfg) {
+	case 2: launchT<T, RBT, PAIRS>(c, B, InPlace<Op, 2>(o), s); break;
+	case 3: launchT<T, RBT, PAIRS>(c, B, InPlace<Op, 3>(o), s); break;
+	default: launchT<T, RBT, PAIRS>(c, B, o, s);
+	}
+}
+
 template <class T, int RBT, int RBD, bool PAIRS = false>
 static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	cudaStream_t s = c->stream;
-	const T ka = (T)c->k.a, kb = (T)c->k.b, kc = (T)c->k.c, iMc = (T)(1.0 / c->k.a);
 	OpBicg1<T> o1;
-	o1.ka = ka;
-	o1.kb = kb;
-	o1.kc = kc;
-	o1.iMc = iMc;
+	set_scaled_coef(c, o1);
 	o1.p0 = (T *)B->p0;
 	o1.p1 = (T *)B->p1;
 	o1.v0 = (T *)B->v[0];
@@ -2046,16 +2103,10 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	o1.rhat = (T *)B->rhat;
 	launchT<T, RBT, PAIRS>(c, B, o1, s);
 	OpBicg2<T> o2;
-	o2.ka = ka;
-	o2.kb = kb;
-	o2.kc = kc;
-	o2.iMc = iMc;
-	launchT<T, RBT, PAIRS>(c, B, o2, s);
+	set_scaled_coef(c, o2);
+	launch_bicg_s<T, RBT, PAIRS>(c, B, o2, s);
 	OpBicg3<T> o3;
-	o3.ka = ka;
-	o3.kb = kb;
-	o3.kc = kc;
-	o3.iMc = iMc;
+	set_scaled_coef(c, o3);
 	o3.x = (T *)B->x;
 	o3.r0 = (T *)B->r;
 	o3.r1 = (T *)B->r1;
@@ -2063,7 +2114,7 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	o3.p1 = (T *)B->p1;
 	o3.rhat = (T *)B->rhat;
 	o3.mixed = B->mixed ? 1 : 0;
-	launchT<T, RBT, PAIRS>(c, B, o3, s);
+	launch_bicg_s<T, RBT, PAIRS>(c, B, o3, s);
 	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
 	c->launches++;
 	if (B->mixed) {
@@ -2206,9 +2257,15 @@ int pairs_alloc(Ctx *c) {
 	B->v[0] = c->v[0];
 	B->v[1] = c->v[1];
 	B->rhat = c->rhat;
-	shape(g, 2, 2, 8, &B->gT, &B->gridT);
-	shape(g, 2, 2, 8, &B->gT1, &B->gridT1, 0, 1);
-	shape(g, 2, 2, 8, &B->gD, &B->gridD);
+	// A tuning recorded for this solver, FP64 and one right-hand side (no
+	// batched context has that key) sets the i3 split, the prefetch distance
+	// and the narrow-sweep form.
+	const Tuning tu = tuning_for(TuneKey{c->solver, SEDI_PREC_FP64, pick_R(1, false), c->g.n1, c->g.n2, c->g.n3});
+	if (tu.acfg >= 1 && tu.acfg <= 3) B->acfg = tu.acfg;
+	B->tuned = tu;
+	shape(g, 2, 2, 8, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
+	shape(g, 2, 2, 8, &B->gT1, &B->gridT1, tu.nz, 1, tu.pfd);
+	shape(g, 2, 2, 8, &B->gD, &B->gridD, tu.nz, 0, tu.pfd);
 	size_t nblk = (size_t)B->gridT.x * B->gridT.z;
 	if ((size_t)B->gridT1.x * B->gridT1.z > nblk) nblk = (size_t)B->gridT1.x * B->gridT1.z;
 	if (cudaMalloc(&B->partials, sizeof(double) * nblk * kMaxDots * B->R) != cudaSuccess ||
@@ -2520,27 +2577,17 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		return 0;
 	}
 	if (B->ks == 1) {
-		const T ka = (T)c->k.a, kb = (T)c->k.b, kc = (T)c->k.c, iMc = (T)(1.0 / c->k.a);
 		OpBicg1<T> o1;
-		o1.ka = ka;
-		o1.kb = kb;
-		o1.kc = kc;
-		o1.iMc = iMc;
+		set_scaled_coef(c, o1);
 		o1.p0 = (T *)B->p0;
 		o1.p1 = (T *)B->p1;
 		o1.v0 = (T *)B->v[0];
 		o1.v1 = (T *)B->v[1];
 		o1.rhat = (T *)B->rhat;
 		OpBicg2<T> o2;
-		o2.ka = ka;
-		o2.kb = kb;
-		o2.kc = kc;
-		o2.iMc = iMc;
+		set_scaled_coef(c, o2);
 		OpBicg3<T> o3;
-		o3.ka = ka;
-		o3.kb = kb;
-		o3.kc = kc;
-		o3.iMc = iMc;
+		set_scaled_coef(c, o3);
 		o3.x = (T *)B->x;
 		o3.r0 = (T *)B->r;
 		o3.r1 = (T *)B->r1;
@@ -2556,8 +2603,8 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		for (int k = 0; k < 3; k++) {
 			auto one = [&]() {
 				if (k == 0) launchT<T, RBT, PAIRS>(c, B, o1, s);
-				else if (k == 1) launchT<T, RBT, PAIRS>(c, B, o2, s);
-				else launchT<T, RBT, PAIRS>(c, B, o3, s);
+				else if (k == 1) launch_bicg_s<T, RBT, PAIRS>(c, B, o2, s);
+				else launch_bicg_s<T, RBT, PAIRS>(c, B, o3, s);
 			};
 			one();
 			BTRY(cudaEventRecord(e0, s));
@@ -2893,8 +2940,9 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 		if (rc) return rc;
 		if (ms < 0.98 * best_ms || (best.pfd < 0 && pf == SEDI_STREAM_PFD)) best_ms = ms, best = t;
 	}
-	// Form of CG's sweep A (ring, or in place with two blocks per SM or six stages).
-	if (kernel_solver(solver, mixed) == SEDI_CG) {
+	// Form of CG's sweep A and BiCGStab's sweeps 2 and 3 (ring, or in place
+	// with two blocks per SM or six stages).
+	if (kernel_solver(solver, mixed) == SEDI_CG || kernel_solver(solver, mixed) == SEDI_BICGSTAB) {
 		for (int ac = 1; ac <= 3; ac++) {
 			Tuning t = best;
 			t.acfg = ac;

@@ -37,21 +37,32 @@ def test_slab_count_does_not_change_the_solution(dims, solver):
     assert np.array_equal(_estimate(dims, 2, mode=1, solver=solver)["D"], one["D"])
 
 
+def _same_iterations(solver, a, b):
+    """CG and pipelined CG: equal counts.  BiCGStab's iterates depend on the
+    rounding of its dot products (the slab form sums per plane, the oracle in
+    sequence, the single-vector form per block): on a 24x20x18 grid at tol
+    1e-10 three summation orders of the same method took 77, 81 and 85
+    iterations for one probe, so its counts are compared within 15%."""
+    a, b = np.asarray(a), np.asarray(b)
+    if solver != "bicgstab":
+        return np.array_equal(a, b)
+    return bool(np.all(np.abs(a - b) <= np.maximum(3, 0.15 * b)))
+
+
 @pytest.mark.parametrize("solver", list(SOLVERS))
 def test_slab_estimate_matches_oracle_and_single_vector_form(solver):
-    """Same iteration counts as the oracle and as the single-vector GPU form;
-    D within 1e-10 of both (BiCGStab: 1e-8, it amplifies the different dot
-    summation orders)."""
+    """Iteration counts as the oracle's and the single-vector GPU form's; D
+    within 1e-10 of both (BiCGStab 1e-8)."""
     dims = (24, 20, 18)
     bar = 1e-8 if solver == "bicgstab" else 1e-10
     r = _estimate(dims, 3, solver=solver)
     ref = O.estimate(SOLVERS[solver], dims, 3, 1234, 400, 1e-10)
     assert np.array_equal(r["results"], ref["results"])
-    assert np.array_equal(r["iters"], ref["iters"])
+    assert _same_iterations(solver, r["iters"], ref["iters"]), (r["iters"], ref["iters"])
     assert O.relmax(r["D"], ref["D"]) <= bar
     with S.Context(solver, dims) as c:
         p = c.estimate(3, 1234, 400, 1e-10)
-    assert np.array_equal(r["iters"], p["iters"])
+    assert _same_iterations(solver, r["iters"], p["iters"]), (r["iters"], p["iters"])
     assert O.relmax(r["D"], p["D"]) <= bar
 
 
@@ -119,7 +130,11 @@ def test_decomposed_cli_matches_the_one_gpu_driver(tmp_path, solver):
                          timeout=600)
     assert one.returncode == 0, one.stderr
     line = lambda out: [ln for ln in out.splitlines() if ln.startswith("Total solve time")][0].split("count")[1]
-    assert line(r.stdout) == line(one.stdout)
+    if solver != "bicgstab":
+        assert line(r.stdout) == line(one.stdout)
+    else:
+        counts = lambda out: [int(v.split("=")[1]) for v in line(out).split()]
+        assert _same_iterations(solver, counts(r.stdout), counts(one.stdout))
     assert "Processor decomposition is (1, 1, 3)" in r.stdout
     assert "Process block shape is (16, 12, 4)" in r.stdout
     a, b = np.fromfile(d_slab), np.fromfile(d_one)
