@@ -30,8 +30,20 @@ __device__ __forceinline__ double sub(double x, double y) { return __dsub_rn(x, 
 
 // Stencil::apply_direct term order (Stencil.hpp:43-50):
 //   a*x_c - c*x_{i1-1} - c*x_{i2-1} - c*x_{i3-1} - b*x_{i1+1} - b*x_{i2+1} - b*x_{i3+1}
+// With b = c = 1 (the estimator's stencil) the products by 1.0 are exact and
+// are left out: the same roundings with half the FP64 instructions.
 __device__ __forceinline__ double stencil7(const Coef &k, double xc, double xm1, double xm2, double xm3,
                                            double xp1, double xp2, double xp3) {
+	if (k.b == 1.0 && k.c == 1.0) {
+		double y = mul(k.a, xc);
+		y = sub(y, xm1);
+		y = sub(y, xm2);
+		y = sub(y, xm3);
+		y = sub(y, xp1);
+		y = sub(y, xp2);
+		y = sub(y, xp3);
+		return y;
+	}
 	double y = mul(k.a, xc);
 	y = sub(y, mul(k.c, xm1));
 	y = sub(y, mul(k.c, xm2));
