@@ -71,7 +71,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["sedi", "reference"], default="sedi")
-    ap.add_argument("--workload", choices=["batched256", "dropin", "large512", "accuracy"], default="batched256",
+    ap.add_argument("--workload", choices=["batched256", "dropin", "large512", "accuracy", "sweeps", "slab"],
+                    default="batched256",
                     help="batched256: the benchmark line (256^3 x 128 probes, mixed CG); dropin: 128^3 x 64 "
                          "probes; large512: the 512^3 x 16-probe pipelined-CG configuration (one JSON line); "
                          "accuracy: diagonal error of the mixed forms per in-loop target (JSON lines)")
@@ -515,6 +516,90 @@ def run_accuracy(S, args):
             print(json.dumps(row), flush=True)
 
 
+def run_sweeps(S, args):
+    """Each streaming sweep alone (CUDA events, 10-20 launches after one)
+    across the narrow-sweep forms (1 ring, 2 in place on 32x16 tiles with two
+    blocks per SM, 3 in place on 32x32 tiles with six stages) and L2 prefetch
+    distances: mixed CG and BiCGStab at 128^3 x 64 and 256^3 x 128 lanes,
+    batched FP64 at 256^3 x 64 lanes (slice width 8 and 2), and the
+    single-vector FP64 sweeps of the three solvers at 256^3.  One JSON line
+    per configuration with each sweep's ms, GB/s and fraction of the
+    measured HBM bandwidth."""
+    peak, psrc = _peak()
+
+    def row(tag, ks):
+        tag["kernels"] = [{"kernel": k, "ms": ms, "GB/s": by / ms / 1e6, "frac": by / ms / 1e6 / peak}
+                          for k, ms, by in ks]
+        tag["peak_gbs"], tag["peak_source"] = peak, psrc
+        print(json.dumps(tag), flush=True)
+
+    for g, k in (((128, 128, 128), 64), ((256, 256, 256), 128)):
+        for solver, pfs in (("cg", (0, 2)), ("bicgstab", (0,))):
+            for form in (1, 2, 3):
+                for pf in pfs:
+                    S.set_tuning(solver, g, k, precision=S.MIXED, sweep_a_form=form, prefetch_planes=pf)
+                    with S.Context(solver, g, precision=S.MIXED, batch=k) as c:
+                        row({"grid": list(g), "lanes": k, "solver": solver, "form": "mixed", "sweep_form": form,
+                             "prefetch_planes": pf, "config": c.config()}, c.time_kernels(reps=10))
+    g = (256, 256, 256)
+    for solver in ("cg", "bicgstab"):
+        for W in (8, 2):
+            for form in (1, 3):
+                S.set_tuning(solver, g, 64, precision=S.FP64, slice_width=W, sweep_a_form=form, prefetch_planes=0)
+                with S.Context(solver, g, precision=S.FP64, batch=64) as c:
+                    row({"grid": list(g), "lanes": 64, "solver": solver, "form": "fp64", "sweep_form": form,
+                         "slice_width": W, "config": c.config()}, c.time_kernels(reps=5))
+    for solver in ("cg", "bicgstab", "pcg"):
+        for form in (1, 2, 3):
+            S.set_tuning(solver, g, 1, precision=S.FP64, sweep_a_form=form, prefetch_planes=2)
+            with S.Context(solver, g) as c:
+                row({"grid": list(g), "lanes": 1, "solver": solver, "form": "plain", "sweep_form": form,
+                     "prefetch_planes": 2}, c.time_kernels(reps=20))
+
+
+def run_slab(S, args):
+    """The slab (i3) decomposition on one GPU: P = 1 and P = 2 slabs in one
+    process (halos by device copies), each solver in FP64, 256^3, 2 probes
+    to tol 1e-9, against the single-vector form on the same probes.  Reports
+    probe-solves/s, GPoint-iterations/s, the host time spent in dot-product
+    gathers, and whether D matches across P bit for bit."""
+    import numpy as np
+    import torch
+    from sedi_b200.domain import slab_solver
+    g, samples, tol, maxiter = (256, 256, 256), 2, 1e-9, 5000
+    n = g[0] * g[1] * g[2]
+    for solver in ("cg", "pcg", "bicgstab"):
+        with S.Context(solver, g) as c:
+            c.estimate(1, SEED, 5, tol, ignore_errors=True)
+            t0 = time.perf_counter()
+            rp = c.estimate(samples, SEED, maxiter, tol)
+            dtp = time.perf_counter() - t0
+        row = {"workload": f"slab decomposition on one GPU, {solver}, 256^3, {samples} probes, tol 1e-9, FP64",
+               "single_vector": {"probe_solves_per_s": samples / dtp,
+                                 "gpoint_iterations_per_s": float(np.sum(rp["iters"])) * n / dtp / 1e9,
+                                 "iterations": rp["iters"].tolist()}, "slabs": []}
+        D1 = None
+        for parts in (1, 2):
+            sv = slab_solver(solver, g, parts, loopback=True)
+            sv.estimate(1, SEED, 5, tol)
+            torch.cuda.synchronize()
+            sv.timers = {"halo_wait": 0.0, "dot_comm": 0.0}
+            t0 = time.perf_counter()
+            r = sv.estimate(samples, SEED, maxiter, tol)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            D = sv.gather(r["D"])
+            D1 = D if D1 is None else D1
+            row["slabs"].append({"parts": parts, "probe_solves_per_s": samples / dt,
+                                 "gpoint_iterations_per_s": float(np.sum(r["iters"])) * n / dt / 1e9,
+                                 "iterations": r["iters"].tolist(), "dot_gather_s": sv.timers["dot_comm"],
+                                 "D_equal_to_one_slab": bool(np.array_equal(D, D1)),
+                                 "D_rel_err_vs_single_vector": _relmax(D, rp["D"])})
+            del sv
+            torch.cuda.empty_cache()
+        print(json.dumps(row), flush=True)
+
+
 def traffic_per_launch(kernel, grid, lanes):
     """DRAM bytes per launch of `kernel` at this size, from the committed ncu
     summary (profiles/ncu_traffic.txt lines '<kernel> <n1>x<n2>x<n3> <lanes>
@@ -546,9 +631,10 @@ def run_sedi(args):
 
     rank, world, local = dist_env()
     wl = args.wl
-    if args.workload in ("large512", "accuracy"):
+    aux = {"large512": run_large512, "accuracy": run_accuracy, "sweeps": run_sweeps, "slab": run_slab}
+    if args.workload in aux:
         if rank == 0:
-            (run_large512 if args.workload == "large512" else run_accuracy)(S, args)
+            aux[args.workload](S, args)
         return
     if args.serve_only:
         if rank == 0:

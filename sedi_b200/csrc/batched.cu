@@ -1610,15 +1610,24 @@ static int pick_R(int nrhs, bool mixed) {
 	return (nrhs + full - 1) / full * full;
 }
 
-// Lanes per slice: FP64 fields 8 (64 B per point), FP32 Krylov fields 4
-// (16 B per point, 32x16 tiles).  Measured at 128^3 x 64 lanes on B200: the
-// FP32 sweeps are 2-19% faster with 4 lanes than with 8 (pipelined CG 1418 vs
-// 1685 us), the FP64 ones are not.  The autotuner may override it per shape.
+// Lanes per slice: FP32 Krylov fields 4 (16 B per point); FP64 Krylov fields
+// of CG and BiCGStab 2 (16 B per point), of pipelined CG 8 (64 B per point);
+// the FP64 x and b of the mixed form 8.  16 B per point gets the 32x32 tiles
+// and deep stage rings of the narrow sweeps.  Measured on B200 (kernels
+// alone, 64 lanes): FP64 CG sweep A at 256^3 4.11 ms with 2 lanes against
+// 5.83 ms with 8, BiCGStab sweep 2 3.98 against 5.20 ms, sweep 3 10.79
+// against 12.78 ms; pipelined CG 21.6 ms with 8 against 22.7 ms with 2; the
+// FP32 sweeps 2-19% faster with 4 lanes than with 8 at 128^3.  The
+// autotuner may override it per shape.
 #ifndef SEDI_SLICE_LANES_FP32
 #define SEDI_SLICE_LANES_FP32 4
 #endif
-static int slice_for(int R, bool fp64) {
-	const int w = fp64 ? kSliceLanes : SEDI_SLICE_LANES_FP32;
+#ifndef SEDI_SLICE_LANES_FP64_NARROW
+#define SEDI_SLICE_LANES_FP64_NARROW 2
+#endif
+static int slice_for(int R, bool fp64, int ks = 0) {
+	const int w = !fp64 ? SEDI_SLICE_LANES_FP32
+	                    : ((ks == SEDI_CG || ks == SEDI_BICGSTAB) ? SEDI_SLICE_LANES_FP64_NARROW : kSliceLanes);
 	return R >= w ? w : R;
 }
 
@@ -1635,9 +1644,12 @@ static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int
 	const int t1 = (g.n1 + P1 - 1) / P1, t2 = (g.n2 + P2 - 1) / P2;
 	const int slices = R / rb;
 	// Split i3 into nz chunks of zc planes.  Blocks run in waves of
-	// 148 x SEDI_BLOCKS_PER_SM; a block streams zc + 2 planes plus about one
-	// plane of pipeline fill.  Pick the split with the fewest wave-planes
-	// (the last wave counts in full), the smaller split on ties.
+	// 148 x SEDI_BLOCKS_PER_SM; a block streams zc + 2 planes and costs about
+	// four more in pipeline fill, launch and its share of the reduction
+	// (single-vector CG sweep A at 256^3 on B200: one wave of 128 blocks of
+	// 64 planes, 92 us, beats two waves of 29-plane blocks, 95 us).  Pick the
+	// split with the fewest wave-planes (the last wave counts in full), the
+	// smaller split on ties.
 	const long long per = (long long)t1 * t2 * slices;
 	const long long wave = 148LL * SEDI_BLOCKS_PER_SM;
 	long long best = -1;
@@ -1648,7 +1660,7 @@ static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int
 		if (z < 2 && g.n3 >= 2) break;
 		const int kk = (g.n3 + z - 1) / z;
 		const long long waves = (per * kk + wave - 1) / wave;
-		const long long cost = waves * (z + 3);
+		const long long cost = waves * (z + 6);
 		if (best < 0 || cost < best) {
 			best = cost;
 			zc = z;
@@ -1759,7 +1771,7 @@ int batched_alloc(Ctx *c) {
 	B->elems = (size_t)c->g.n * B->R;
 	const int ebT = B->mixed ? 4 : 8;
 	const Tuning tu = tuning_for(TuneKey{c->solver, c->precision, B->R, c->g.n1, c->g.n2, c->g.n3});
-	B->rbT = slice_for(B->R, !B->mixed);
+	B->rbT = slice_for(B->R, !B->mixed, B->ks);
 	if (tu.W > 0 && tu.W <= B->R && B->R % tu.W == 0) B->rbT = tu.W;
 	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
 	B->tuned = tu;
@@ -1874,7 +1886,7 @@ size_t batched_bytes(int solver, int precision, int batch, long long n1, long lo
 	const int R = pick_R(batch, mixed);
 	const size_t elems = (size_t)g.n * R, ts = mixed ? 4 : 8, xs = mixed ? 4 : 8;
 	const Tuning tu = tuning_for(TuneKey{solver, precision, R, n1, n2, n3});
-	int wT = slice_for(R, !mixed);
+	int wT = slice_for(R, !mixed, kernel_solver(solver, mixed));
 	if (tu.W > 0 && tu.W <= R && R % tu.W == 0) wT = tu.W;
 	SGeo sT, sD;
 	dim3 gT, gD;
@@ -2897,7 +2909,9 @@ static int tune_sweep_ms(sedi_ctx *h, double *ms_sum) {
 	double ms[8], by[8];
 	char names[8 * 32];
 	int cnt = 0;
-	const int rc = batched_time_kernels(&h->c, 5, ms, by, names, &cnt);
+	Ctx *c = &h->c;
+	const int rc = c->batched ? batched_time_kernels(c, 5, ms, by, names, &cnt)
+	                          : (c->pairs ? pairs_time_kernels(c, 10, ms, by, names, &cnt) : SEDI_ERR_UNSUPPORTED);
 	if (rc) return rc;
 	*ms_sum = 0.0;
 	for (int k = 0; k < cnt; k++) *ms_sum += ms[k];
@@ -2907,16 +2921,24 @@ static int tune_sweep_ms(sedi_ctx *h, double *ms_sum) {
 int batched_autotune(int solver, int precision, int batch, long long n1, long long n2, long long n3, int maxiter,
                      double tol, uint32_t seed, int flags, int *out, double *score_ms) {
 	const bool mixed = precision == SEDI_PREC_MIXED;
-	if (batch < 2 && !mixed) return SEDI_ERR_ARG;  // one FP64 lane is the single-vector form
+	// One FP64 right-hand side is the single-vector form: its streaming sweeps
+	// (even n1, 2^22 points or more) take the i3 split, prefetch distance and
+	// narrow-sweep form; the slice width is fixed and there is no graph or
+	// reliable-update choice.
+	const bool single = batch < 2 && !mixed;
+	if (single && (n1 % 2 != 0 || n1 * n2 * n3 < kPairsMinPoints)) return SEDI_ERR_UNSUPPORTED;
+	if (single) flags &= ~1;
 	const int R = pick_R(batch, mixed);
 	const TuneKey key{solver, precision, R, n1, n2, n3};
 	std::vector<int> Ws;
-	if (R >= 8) {
+	if (single) {
+		Ws.push_back(2);
+	} else if (R >= 8) {
 		Ws.push_back(8);
 		Ws.push_back(4);
 		if (!mixed) Ws.push_back(2);
 	} else {
-		Ws.push_back(slice_for(R, !mixed));
+		Ws.push_back(slice_for(R, !mixed, kernel_solver(solver, mixed)));
 	}
 	Tuning best;
 	double best_ms = -1.0;
@@ -2939,9 +2961,13 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 		if (best_ms < 0 || ms < best_ms) best_ms = ms, best = t;
 	}
 	if (best_ms < 0) return SEDI_ERR_NOMEM;
-	const int nzs[] = {1, 2, 3, 4, 6, 8};
+	// i3 splits: a single vector has few tiles per plane, so it tries the
+	// splits around whole waves of blocks too.
+	std::vector<int> nzs = {1, 2, 3, 4, 6, 8};
+	if (single)
+		for (int nz : {5, 9, 10, 12, 14, 16, 18, 24, 32}) nzs.push_back(nz);
 	for (int nz : nzs) {
-		if (nz > n3) break;
+		if (nz > n3) continue;
 		Tuning t = best;
 		t.nz = nz;
 		double ms = 0.0;

@@ -354,3 +354,41 @@ def test_cg_sweep_a_forms_agree(prec):
             assert O.relmax(out[form]["D"], out[1]["D"]) <= 1e-12
         else:
             assert O.relmax(out[form]["D"], out[1]["D"]) <= 1e-9
+
+
+@pytest.mark.parametrize("prec", [S.FP64, S.MIXED])
+def test_bicgstab_sweep_forms_agree(prec):
+    """BiCGStab's sweeps 2 and 3 as a ring of s (form 1) or with s written
+    over v in the stage (forms 2 and 3): the same values summed on other
+    tiles.  At 20 fixed iterations FP64 agrees to 1e-11, mixed to 1e-6 (the
+    FP32 iterates, no reliable-update target at tol 0)."""
+    dims, samples = (40, 36, 30), 16
+    out = {}
+    for form in (1, 2, 3):
+        S.set_tuning("bicgstab", dims, samples, precision=prec, sweep_a_form=form)
+        with S.Context("bicgstab", dims, precision=prec, batch=samples) as c:
+            assert c.config()["sweep_a_form"] == form
+            out[form] = c.estimate(samples, 99, 20, 0.0, ignore_errors=True)
+    S.set_tuning("bicgstab", dims, samples, precision=prec)
+    for form in (2, 3):
+        assert np.array_equal(out[form]["results"], out[1]["results"])
+        assert O.relmax(out[form]["D"], out[1]["D"]) <= (1e-11 if prec == S.FP64 else 1e-6)
+
+
+def test_single_vector_autotune_keeps_results():
+    """The autotuner on one FP64 right-hand side tunes the single-vector
+    streaming sweeps (i3 split, prefetch, sweep form): at 30 fixed CG
+    iterations D stays within 1e-12 of the untuned run.  Odd n1 has no
+    streaming form: SEDI_ERR_UNSUPPORTED."""
+    dims = (256, 128, 128)
+    with S.Context("cg", dims) as c:
+        ref = c.estimate(2, 7, 30, 0.0, ignore_errors=True)
+    choice = S.autotune("cg", dims, 1, precision=S.FP64, maxiter=30, tol=0.0, solve=False)
+    assert choice["slice_width"] == 2 and choice["sweep_a_form"] in (1, 2, 3)
+    with S.Context("cg", dims) as c:
+        got = c.estimate(2, 7, 30, 0.0, ignore_errors=True)
+    S.set_tuning("cg", dims, 1, precision=S.FP64)
+    assert np.array_equal(got["iters"], ref["iters"])
+    assert O.relmax(got["D"], ref["D"]) <= 1e-12
+    with pytest.raises(S.SediError):
+        S.autotune("cg", (255, 128, 130), 1, precision=S.FP64, solve=False)
