@@ -477,7 +477,12 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) k_stream(SGeo g, const __
 		}
 	}
 	__syncthreads();
-	if (t == 0) *ticket = 0u;
+	if (t == 0) {
+		// The sweep that ends an iteration advances the counter unless a
+		// reliable update is due (it advances it after the update).
+		if (Op::ADVANCE && gl->active != 0 && gl->ru_due == 0) gl->iter += 1;
+		*ticket = 0u;
+	}
 }
 
 template <class T>
@@ -489,6 +494,9 @@ struct OpBase {
 	// SCALED: src() gives f and the stencil is applied to f .* iMc (the op
 	// provides iMc and, for FP32, the scaled coefficients kas, kbs, kcs).
 	static constexpr bool SCALED = false;
+	// ADVANCE: the last block ends the iteration (gl->iter += 1 unless a
+	// reliable update is due), so no kernel follows the sweep for that.
+	static constexpr bool ADVANCE = false;
 	T ka, kb, kc;
 	__device__ void gload(long long, Vec<T> *) const {}
 	__device__ bool enabled(const Global *) const { return true; }
@@ -740,7 +748,7 @@ using OpCgAv = InPlace<OpCgA<T>, K>;
 template <class T>
 struct OpCgB : OpBase<T> {
 	static constexpr int NS = 1, NQ = 2, ND = 2;
-	static constexpr bool IDENT = true, USES_RAW_CENTER = false;
+	static constexpr bool IDENT = true, USES_RAW_CENTER = false, ADVANCE = true;
 	static constexpr int V = Vec<T>::V;
 	T iMc;
 	T *x, *r;
@@ -813,7 +821,7 @@ struct OpCgB : OpBase<T> {
 template <class T>
 struct OpPcg : OpBase<T> {
 	static constexpr int NS = 1, NQ = 0, ND = 3;
-	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true, ADVANCE = true;
 	static constexpr int V = Vec<T>::V;
 	T iMc;
 	T *x, *r, *u, *q, *s, *p, *z, *w0, *w1;
@@ -1159,7 +1167,7 @@ template <class T>
 struct OpBicg3 : OpBicgS<T> {
 	static constexpr int KIND = 1;
 	static constexpr int NS = 2, NQ = 0, ND = 2, NG = 3;
-	static constexpr bool IDENT = false, USES_RAW_CENTER = true;
+	static constexpr bool IDENT = false, USES_RAW_CENTER = true, ADVANCE = true;
 	static constexpr int V = Vec<T>::V;
 	T *x, *r0, *r1, *p0, *p1, *rhat;
 	T *rn, *pc;
@@ -1282,11 +1290,6 @@ struct OpBicg3 : OpBicgS<T> {
 };
 
 // Iteration bookkeeping between launches.
-__global__ void kb_next_iter(Global *gl) {
-	if (gl->active == 0) return;
-	if (gl->ru_due == 0) gl->iter += 1;
-}
-
 __global__ void kb_setup_done(Global *gl) { gl->active -= 1; }  // drops the setup sweep's guard
 
 __global__ void kb_ru_done(Global *gl) {
@@ -2012,8 +2015,6 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	bo.r = (T *)B->r;
 	bo.mixed = B->mixed ? 1 : 0;
 	launchT<T, RBT, PAIRS>(c, B, bo, s);
-	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
-	c->launches++;
 	if (B->mixed) {
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
@@ -2064,8 +2065,6 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 	o.w1 = (T *)B->w[1];
 	o.mixed = B->mixed ? 1 : 0;
 	launchT<T, RBT, PAIRS>(c, B, o, s);
-	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
-	c->launches++;
 	if (B->mixed) {
 		// Residual replacement (reliable update) of pipelined CG: x_hi += x_lo;
 		// r = b - A x_hi (FP64); s = A p, q = s .* iM; z = A q; u = r .* iM,
@@ -2146,8 +2145,6 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	o3.rhat = (T *)B->rhat;
 	o3.mixed = B->mixed ? 1 : 0;
 	launch_bicg_s<T, RBT, PAIRS>(c, B, o3, s);
-	kb_next_iter<<<1, 1, 0, s>>>(B->gl);
-	c->launches++;
 	if (B->mixed) {
 		// Reliable update: x_hi += x_lo; r = b - A x_hi (FP64) into the r buffer
 		// the next iteration reads; rho = <r, r_hat> (restarted lanes: r_hat = r).
