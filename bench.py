@@ -521,7 +521,8 @@ def run_sweeps(S, args):
     across the narrow-sweep forms (1 ring, 2 in place on 32x16 tiles with two
     blocks per SM, 3 in place on 32x32 tiles with six stages) and L2 prefetch
     distances: mixed CG and BiCGStab at 128^3 x 64 and 256^3 x 128 lanes,
-    batched FP64 at 256^3 x 64 lanes (slice width 8 and 2), and the
+    batched FP64 (CG, BiCGStab, pipelined CG) at 256^3 x 64 lanes (slice
+    width 8 and 2), and the
     single-vector FP64 sweeps of the three solvers at 256^3.  One JSON line
     per configuration with each sweep's ms, GB/s and fraction of the
     measured HBM bandwidth."""
@@ -542,9 +543,9 @@ def run_sweeps(S, args):
                         row({"grid": list(g), "lanes": k, "solver": solver, "form": "mixed", "sweep_form": form,
                              "prefetch_planes": pf, "config": c.config()}, c.time_kernels(reps=10))
     g = (256, 256, 256)
-    for solver in ("cg", "bicgstab"):
+    for solver in ("cg", "bicgstab", "pcg"):
         for W in (8, 2):
-            for form in (1, 3):
+            for form in ((1, 3) if solver != "pcg" else (1,)):
                 S.set_tuning(solver, g, 64, precision=S.FP64, slice_width=W, sweep_a_form=form, prefetch_planes=0)
                 with S.Context(solver, g, precision=S.FP64, batch=64) as c:
                     row({"grid": list(g), "lanes": 64, "solver": solver, "form": "fp64", "sweep_form": form,

@@ -1427,18 +1427,25 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 #ifndef SEDI_STREAM_PFD
 #define SEDI_STREAM_PFD 0  // default L2 prefetch distance of the sweeps, in planes (0: none)
 #endif
-#ifndef SEDI_CGA_FORM
 // Form of the narrow sweeps (CG sweep A, BiCGStab sweeps 2 and 3): 1 ring
 // (32x32), 2 in place (32x16, 2 blocks/SM), 3 in place (32x32, 6 stages).
-// Measured on B200 (CUDA events, kernels alone), mixed CG sweep A at 256^3 x
-// 128 lanes: 4.73 ms ring, 5.19 ms form 2, 4.21 ms form 3; at 128^3 x 64 and
-// in FP64 the forms are within 3%.
+// Defaults by measurement on B200 (kernels alone, fraction of measured HBM
+// bandwidth, 256^3): batched CG sweep A form 3 (mixed x 128 lanes 4.21 ms,
+// 95%, against 4.78 ms ring; FP64 2-lane slices 97% against 83%); BiCGStab
+// sweep 2 ring (mixed 73% against 71%, FP64 74% against 67%); the
+// single-vector sweeps ring (CG A 68% against 65%, BiCGStab 2 51% against
+// 44%).
+#ifndef SEDI_CGA_FORM
 #define SEDI_CGA_FORM 3
 #endif
+#ifndef SEDI_NARROW_FORM
+#define SEDI_NARROW_FORM 1
+#endif
+static int default_form(int ks, bool single) { return !single && ks == SEDI_CG ? SEDI_CGA_FORM : SEDI_NARROW_FORM; }
 struct Tuning {
 	int W = 0, nz = 0, period = 0, chunk = 0;
 	int pfd = -1;   // L2 prefetch distance in planes (-1: SEDI_STREAM_PFD)
-	int acfg = 0;   // form of the narrow sweeps (0: SEDI_CGA_FORM)
+	int acfg = 0;   // form of the narrow sweeps (0: default_form)
 };
 struct TuneKey {
 	int solver, precision, R;
@@ -1502,7 +1509,7 @@ struct Batched {
 	int R = 0;
 	bool mixed = false;  // FP32 Krylov fields, FP64 x_hi, reductions and reliable update
 	bool pairs = false;  // single-vector FP64 form: lanes 0/1 = even/odd i1 points of one vector
-	int acfg = SEDI_CGA_FORM;  // form of the narrow sweeps (see CfgFor, InPlace)
+	int acfg = SEDI_NARROW_FORM;  // form of the narrow sweeps (see CfgFor, InPlace, default_form)
 	int ks = 0;          // solver whose sweeps run (the mixed pipelined CG runs the CG recurrence)
 	bool aliased = false;  // the Krylov fields belong to the context (single-vector form)
 	const double *graph_hist = nullptr;  // history pointer the captured graph holds
@@ -1779,7 +1786,7 @@ int batched_alloc(Ctx *c) {
 	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
 	B->tuned = tu;
 	if (tu.period > 0) B->period = tu.period;
-	if (tu.acfg >= 1 && tu.acfg <= 3) B->acfg = tu.acfg;
+	B->acfg = tu.acfg >= 1 && tu.acfg <= 3 ? tu.acfg : default_form(B->ks, false);
 	B->theta = default_theta(B->ks);
 	if (tu.chunk > 0) B->chunk = tu.chunk;
 	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
@@ -2289,7 +2296,7 @@ int pairs_alloc(Ctx *c) {
 	// batched context has that key) sets the i3 split, the prefetch distance
 	// and the narrow-sweep form.
 	const Tuning tu = tuning_for(TuneKey{c->solver, SEDI_PREC_FP64, pick_R(1, false), c->g.n1, c->g.n2, c->g.n3});
-	if (tu.acfg >= 1 && tu.acfg <= 3) B->acfg = tu.acfg;
+	B->acfg = tu.acfg >= 1 && tu.acfg <= 3 ? tu.acfg : default_form(B->ks, true);
 	B->tuned = tu;
 	shape(g, 2, 2, 8, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
 	shape(g, 2, 2, 8, &B->gT1, &B->gridT1, tu.nz, 1, tu.pfd);
@@ -2991,7 +2998,8 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 			double ms = 0.0;
 			const int rc = score(t, &ms);
 			if (rc) return rc;
-			if (ms < 0.98 * best_ms || (best.acfg == 0 && ac == SEDI_CGA_FORM)) best_ms = ms, best = t;
+			if (ms < 0.98 * best_ms || (best.acfg == 0 && ac == default_form(kernel_solver(solver, mixed), single)))
+				best_ms = ms, best = t;
 		}
 	}
 	double best_est = -1.0;
@@ -3050,7 +3058,7 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 	out[2] = best.period;
 	out[3] = best.chunk;
 	out[4] = best.pfd >= 0 ? best.pfd : SEDI_STREAM_PFD;
-	out[5] = best.acfg ? best.acfg : SEDI_CGA_FORM;
+	out[5] = best.acfg ? best.acfg : default_form(kernel_solver(solver, mixed), single);
 	if (score_ms) *score_ms = best_est >= 0 ? best_est : best_ms;
 	return 0;
 }

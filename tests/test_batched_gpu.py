@@ -360,8 +360,9 @@ def test_cg_sweep_a_forms_agree(prec):
 def test_bicgstab_sweep_forms_agree(prec):
     """BiCGStab's sweeps 2 and 3 as a ring of s (form 1) or with s written
     over v in the stage (forms 2 and 3): the same values summed on other
-    tiles.  At 20 fixed iterations FP64 agrees to 1e-11, mixed to 1e-6 (the
-    FP32 iterates, no reliable-update target at tol 0)."""
+    tiles.  At 20 fixed iterations FP64 agrees to 1e-9 (BiCGStab amplifies
+    the other summation order: 2.8e-11 measured), mixed to 1e-6 (the FP32
+    iterates, no reliable-update target at tol 0)."""
     dims, samples = (40, 36, 30), 16
     out = {}
     for form in (1, 2, 3):
@@ -372,7 +373,7 @@ def test_bicgstab_sweep_forms_agree(prec):
     S.set_tuning("bicgstab", dims, samples, precision=prec)
     for form in (2, 3):
         assert np.array_equal(out[form]["results"], out[1]["results"])
-        assert O.relmax(out[form]["D"], out[1]["D"]) <= (1e-11 if prec == S.FP64 else 1e-6)
+        assert O.relmax(out[form]["D"], out[1]["D"]) <= (1e-9 if prec == S.FP64 else 1e-6)
 
 
 def test_single_vector_autotune_keeps_results():
