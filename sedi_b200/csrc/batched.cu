@@ -1945,6 +1945,8 @@ int batched_alloc(Ctx *c) {
 
 // Device bytes batched_alloc takes for a context (each allocation rounded
 // up to the 2 MiB granularity of large device allocations).
+int batched_lanes(int precision, int batch) { return pick_R(batch, precision == SEDI_PREC_MIXED); }
+
 size_t batched_bytes(int solver, int precision, int batch, long long n1, long long n2, long long n3) {
 	const bool mixed = precision == SEDI_PREC_MIXED;
 	Geo g;

@@ -137,6 +137,8 @@ int batched_set_theta(Ctx *c, double theta);
 double batched_theta(const Ctx *c);
 // Device bytes a batched context allocates (0 for the single-vector form).
 size_t batched_bytes(int solver, int precision, int batch, long long n1, long long n2, long long n3);
+// Lanes (padded right-hand sides) of a batched context created for `batch`.
+int batched_lanes(int precision, int batch);
 
 // rng.cu
 void host_fill_probe(uint32_t seed, long n, double *out);

@@ -15,13 +15,17 @@
 // than max_active jobs run; when the oldest queued job does not fit, later
 // jobs that do fit may start ahead of it, at most kMaxBypass of them, so a
 // large job is never starved.  Finished contexts stay allocated as idle slots
-// and are reused by later jobs of the same shape (no allocation, no graph
-// instantiation); idle slots are freed oldest first when a new context needs
-// their memory.
+// and are reused by later jobs of the same solver, precision, grid and padded
+// lane count (no allocation, no graph instantiation); idle slots are freed
+// oldest first when a new context needs their memory.
 //
 // A job's lane count depends only on the job and the server's per-job byte
 // cap, never on the load, and every reduction runs in a fixed order, so a
-// job's result is the same alone and in any mix.
+// job's result is the same alone and in any mix.  A context's launch shapes
+// depend only on its padded lane count, so a job whose probes fit one batch
+// may run on any context of its padded lane count with room for them (new
+// contexts are created with every padded lane usable); a job of several
+// batches runs only on contexts of its own batch size.
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -39,7 +43,7 @@ namespace {
 constexpr int kMaxBypass = 4;
 
 struct Key {
-	int solver, precision, lanes;
+	int solver, precision, lanes;  // lanes: padded right-hand sides of the context
 	long long n1, n2, n3;
 	bool operator==(const Key &o) const {
 		return solver == o.solver && precision == o.precision && lanes == o.lanes && n1 == o.n1 && n2 == o.n2 &&
@@ -50,6 +54,7 @@ struct Key {
 struct Slot {
 	sedi_ctx *h = nullptr;
 	Key key;
+	int batch = 0;  // right-hand sides per batch of the context
 	size_t bytes = 0;
 	double *D_host = nullptr;  // pinned, n doubles
 	bool busy = false;
@@ -61,6 +66,7 @@ enum JobState { JOB_QUEUED = 0, JOB_RUNNING = 1, JOB_DONE = 2, JOB_FAILED = 3 };
 struct Job {
 	long id = 0;
 	Key key;
+	int lanes = 0;  // right-hand sides per batch (the job's own context batch)
 	int samples = 0, maxiter = 0;
 	uint32_t seed = 0;
 	double tol = 0.0;
@@ -117,8 +123,9 @@ void free_slot(sedi_server *S, Slot *sl) {
 // slots oldest first).  nullptr when the job cannot start now.
 Slot *acquire(sedi_server *S, const Job &J, int *err) {
 	*err = 0;
+	const bool one_batch = J.lanes >= J.samples;
 	for (Slot *sl : S->slots)
-		if (!sl->busy && sl->key == J.key) {
+		if (!sl->busy && sl->key == J.key && (one_batch ? sl->batch >= J.samples : sl->batch == J.lanes)) {
 			S->reused++;
 			return sl;
 		}
@@ -144,9 +151,10 @@ Slot *acquire(sedi_server *S, const Job &J, int *err) {
 		return nullptr;
 	}
 	sl->key = J.key;
+	sl->batch = one_batch ? J.key.lanes : J.lanes;
 	sl->bytes = J.bytes;
 	sl->h = sedi_create(J.key.solver, (long)J.key.n1, (long)J.key.n2, (long)J.key.n3, 6.0, 1.0, 1.0, 0,
-	                    J.key.precision, J.key.lanes, err);
+	                    J.key.precision, sl->batch, err);
 	if (!sl->h || cudaMallocHost(&sl->D_host, sizeof(double) * (size_t)(J.key.n1 * J.key.n2 * J.key.n3)) != cudaSuccess) {
 		cudaGetLastError();
 		if (!*err) *err = SEDI_ERR_NOMEM;
@@ -290,8 +298,9 @@ long sedi_server_submit(sedi_server *S, int solver, int precision, long n1, long
 	J.key.n1 = n1;
 	J.key.n2 = n2;
 	J.key.n3 = n3;
-	J.key.lanes = job_lanes(S, solver, precision, samples, n1, n2, n3);
-	J.bytes = batched_bytes(solver, precision, J.key.lanes, n1, n2, n3);
+	J.lanes = job_lanes(S, solver, precision, samples, n1, n2, n3);
+	J.key.lanes = batched_lanes(precision, J.lanes);
+	J.bytes = batched_bytes(solver, precision, J.lanes, n1, n2, n3);
 	if (J.bytes > S->budget) return SEDI_ERR_NOMEM;
 	J.samples = samples;
 	J.seed = seed;
@@ -333,7 +342,7 @@ int sedi_server_job_info(sedi_server *S, long id, int *state, int *rc, double *t
 	if (t_submit) *t_submit = J.t_submit;
 	if (t_start) *t_start = J.t_start;
 	if (t_done) *t_done = J.t_done;
-	if (lanes) *lanes = J.key.lanes;
+	if (lanes) *lanes = J.lanes;
 	if (bytes) *bytes = (double)J.bytes;
 	return 0;
 }
