@@ -157,59 +157,46 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) k_stream(SGeo g, const __
 	constexpr int HE = (int)Lay::HALO_ELEMS, IE = (int)Lay::INT_ELEMS;
 
 	const int t = threadIdx.x, lg = t % LG, ps = t / LG;
+	const int tile = blockIdx.x;
+	const int i1_0 = (tile % g.tiles1) * P1, i2_0 = (tile / g.tiles1) * C::P2;
 	const int slice = blockIdx.y, lane0 = slice * RB;
 	const int zoff = slice * g.n3;  // plane offset of this slice in the 4-D map
-	// No planes when the op has no work for this lane slice (the block still
-	// joins the reduction).
-	const bool live = op.slice_live(gl, ls, lane0, RB);
+	const int z0 = blockIdx.z * g.zc, z1 = min(z0 + g.zc, g.n3);
+	// Planes z0-1 .. z1 (relative index j = p - z0 + 1); none when the op has
+	// no work for this lane slice (the block still joins the reduction).
+	const int np = op.slice_live(gl, ls, lane0, RB) ? z1 - z0 + 2 : 0;
 	const int lo = lg * V;
 	op.begin(gl, ls, lane0 + lo);
 
-	// The block's work: one (tile, i3 chunk) per block, or with g.seg an equal
-	// share of the (tile, plane) units in tile-major order, at most two
-	// segments, one block per SM (a single vector has too few tiles per plane
-	// to fill whole waves of blocks).
-	int nseg = 1, seg_tile[2] = {0, 0}, seg_z0[2] = {0, 0}, seg_z1[2] = {0, 0};
-	if (g.seg) {
-		const long long units = (long long)g.ntiles * g.n3;
-		const long long u0 = units * blockIdx.x / gridDim.x, u1 = units * (blockIdx.x + 1) / gridDim.x;
-		const int ta = (int)(u0 / g.n3), tb = (int)((u1 - 1) / g.n3);
-		seg_tile[0] = ta;
-		seg_z0[0] = (int)(u0 - (long long)ta * g.n3);
-		seg_z1[0] = tb == ta ? (int)(u1 - (long long)ta * g.n3) : g.n3;
-		if (tb != ta) {
-			nseg = 2;
-			seg_tile[1] = tb;
-			seg_z1[1] = (int)(u1 - (long long)tb * g.n3);
-		}
-	} else {
-		seg_tile[0] = blockIdx.x;
-		seg_z0[0] = blockIdx.z * g.zc;
-		seg_z1[0] = min(seg_z0[0] + g.zc, g.n3);
-	}
-
-	// Per-thread work, identical in every plane and tile: halo vectors
-	// (stencil input) and output points, with their shared-memory offsets.
+	// Per-thread work, identical in every plane: halo vectors (stencil input)
+	// and output points, with their shared-memory offsets and grid validity.
 	int hoff[KC];
+	unsigned hval = 0;
 #pragma unroll
 	for (int k = 0; k < KC; k++) {
 		const int e = t + k * C::THREADS;
-		hoff[k] = e < HALO * LG ? (e / LG) * RB + lo : -1;
+		const int h = e / LG;
+		const int gi1 = i1_0 - 1 + h % H1, gi2 = i2_0 - 1 + h / H1;
+		hoff[k] = e < HALO * LG ? h * RB + lo : -1;
+		if (e < HALO * LG && gi1 >= 0 && gi1 < g.n1 && gi2 >= 0 && gi2 < g.n2) hval |= 1u << k;
 	}
 	// A thread's KO output points are KO consecutive rows of one column when
 	// the tile allows it (ROWS), so inside the group a point's i2 neighbour
 	// is another point's centre, already in registers.
 	constexpr bool ROWS = (NPS % P1 == 0) && (KO * NPS == INT);
-	int ooff[KO], qoff[KO], oq[KO];
-	unsigned oin = 0;
+	int ooff[KO], qoff[KO];
+	long long obase[KO];
+	unsigned oval = 0, oin = 0;
 #pragma unroll
 	for (int k = 0; k < KO; k++) {
 		const int q = ROWS ? (KO * (ps / P1) + k) * P1 + ps % P1 : ps + k * NPS;
 		const int q1 = q % P1, q2 = q / P1;
-		oq[k] = q;
+		const int gi1 = i1_0 + q1, gi2 = i2_0 + q2;
 		ooff[k] = ((q2 + 1) * H1 + (q1 + 1)) * RB + lo;
 		qoff[k] = q * RB + lo;
+		obase[k] = (long long)gi2 * g.n1 + gi1;
 		if (q < INT) oin |= 1u << k;
+		if (q < INT && gi1 < g.n1 && gi2 < g.n2) oval |= 1u << k;
 	}
 	// Column centres of the stencil input at planes m-1, m, m+1 of the current
 	// output plane m: two of them were read one step earlier (the planes stay
@@ -224,6 +211,36 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) k_stream(SGeo g, const __
 	}
 	__syncthreads();
 
+	auto issue = [&](int j) {  // thread 0
+		const int p = z0 - 1 + j;
+		uint64_t *b = &bar[j % NST];
+		E *st = stage0 + (j % NST) * SE;
+		if (p < 0 || p >= g.n3) {
+			mbar_arrive(b);  // ghost plane: completes the phase without data
+			return;
+		}
+		// Stages are only read by the generic proxy during the sweep (the
+		// reduction scratch that aliases them is written after the last wait),
+		// so no proxy fence is needed before the copy.
+		mbar_arrive_tx(b, Lay::TX);
+#pragma unroll
+		for (int s = 0; s < NS; s++)
+			tma_load3(st + s * HE, &maps.m[op.src_map(s)], b, (i1_0 - 1) * ME, i2_0 - 1, zoff + p);
+#pragma unroll
+		for (int q = 0; q < NQ; q++) tma_load3(st + NS * HE + q * IE, &maps.m[op.q_map(q)], b, i1_0 * ME, i2_0, zoff + p);
+		// The same tiles pfd planes further on, into L2 (within this block's planes).
+		const int pf = p + g.pfd;
+		if (g.pfd > 0 && pf <= z1 && pf < g.n3) {
+#pragma unroll
+			for (int s = 0; s < NS; s++) tma_prefetch3(&maps.m[op.src_map(s)], (i1_0 - 1) * ME, i2_0 - 1, zoff + pf);
+#pragma unroll
+			for (int q = 0; q < NQ; q++) tma_prefetch3(&maps.m[op.q_map(q)], i1_0 * ME, i2_0, zoff + pf);
+		}
+	};
+	int issued = 0;
+	if (t == 0)
+		for (; issued < NST && issued < np; issued++) issue(issued);
+
 	constexpr int NDX = ND > 0 ? ND : 1;
 	double part[NDX][V];
 #pragma unroll
@@ -232,222 +249,158 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) k_stream(SGeo g, const __
 		for (int e = 0; e < V; e++) part[d][e] = 0.0;
 
 	bool failed = false;
-	int G = 0;        // stages of the earlier segments (stage g uses slot g mod NST, parity (g / NST) & 1)
-	int waited = 0;   // planes of this segment whose stage has arrived
-	int issued = 0;   // planes of this segment whose copies were issued
-	for (int sg = 0; sg < nseg; sg++) {
-		const int tile = seg_tile[sg];
-		const int i1_0 = (tile % g.tiles1) * P1, i2_0 = (tile / g.tiles1) * C::P2;
-		const int z0 = seg_z0[sg], z1 = seg_z1[sg];
-		// Planes z0-1 .. z1 (relative index j = p - z0 + 1).
-		const int np = live ? z1 - z0 + 2 : 0;
-		// Grid validity of the halo vectors and output points in this tile.
-		unsigned hval = 0, oval = 0;
-		long long obase[KO];
+	int waited = 0;  // planes whose stage has arrived
+	int sj = 0;      // stage slot of plane j (j mod NST)
+	unsigned par = 0;  // barrier parity of plane j ((j / NST) & 1)
+	for (int j = 0; j <= np; j++, sj = (sj + 1 == NST) ? 0 : sj + 1, par ^= (sj == 0)) {
+		// Each thread waits for plane j's stage itself (the mbarrier's acquire
+		// makes the TMA data visible); a timeout is combined into the one
+		// block barrier at the end of the step.
+		bool ok = true;
+		if (j < np) ok = mbar_wait(&bar[sj], par);
+		// Pointwise fields an op reads with plain loads (Op::NG of them): issue
+		// the loads for this step's outputs (plane j-2) before the halo
+		// transform, so they are in flight during it.
+		Vec<T> gv[KO][NGX];
+		if (Op::NG > 0 && j >= 3) {
+			const long long zb = (long long)(z0 - 1 + j - 2) * plane;
 #pragma unroll
-		for (int k = 0; k < KC; k++) {
-			const int e = t + k * C::THREADS;
-			const int h = e / LG;
-			const int gi1 = i1_0 - 1 + h % H1, gi2 = i2_0 - 1 + h / H1;
-			if (e < HALO * LG && gi1 >= 0 && gi1 < g.n1 && gi2 >= 0 && gi2 < g.n2) hval |= 1u << k;
+			for (int k = 0; k < KO; k++)
+				if (oval >> k & 1u) op.gload(((long long)slice * g.npts + zb + obase[k]) * RB + lo, gv[k]);
 		}
-#pragma unroll
-		for (int k = 0; k < KO; k++) {
-			const int gi1 = i1_0 + oq[k] % P1, gi2 = i2_0 + oq[k] / P1;
-			obase[k] = (long long)gi2 * g.n1 + gi1;
-			if (oq[k] < INT && gi1 < g.n1 && gi2 < g.n2) oval |= 1u << k;
-		}
-
-		auto issue = [&](int j) {  // thread 0
+		// Phase 1: stencil input of plane j (transforming ops only).
+		if (!IDENT && j < np) {
 			const int p = z0 - 1 + j;
-			const int gs = (G + j) % NST;
-			uint64_t *b = &bar[gs];
-			E *st = stage0 + gs * SE;
-			if (p < 0 || p >= g.n3) {
-				mbar_arrive(b);  // ghost plane: completes the phase without data
-				return;
-			}
-			// Stages are only read by the generic proxy during the sweep (the
-			// reduction scratch that aliases them is written after the last wait),
-			// so no proxy fence is needed before the copy.
-			mbar_arrive_tx(b, Lay::TX);
+			E *const st = stage0 + sj * SE;
+			// In place: over the source field INPLACE_SLOT of this plane's stage
+			// (each thread rewrites only the points it read).
+			E *cr = INPLACE ? st + Op::INPLACE_SLOT * HE : ring + (j & 3) * HE;
+			const bool pin = p >= 0 && p < g.n3;
 #pragma unroll
-			for (int s = 0; s < NS; s++)
-				tma_load3(st + s * HE, &maps.m[op.src_map(s)], b, (i1_0 - 1) * ME, i2_0 - 1, zoff + p);
+			for (int k = 0; k < KC; k++) {
+				if (hoff[k] < 0) continue;
+				Vec<T> cv;
+				if (pin && (hval >> k & 1u)) {
+					Vec<T> raw[NS];
 #pragma unroll
-			for (int q = 0; q < NQ; q++)
-				tma_load3(st + NS * HE + q * IE, &maps.m[op.q_map(q)], b, i1_0 * ME, i2_0, zoff + p);
-			// The same tiles pfd planes further on, into L2 (within this segment's planes).
-			const int pf = p + g.pfd;
-			if (g.pfd > 0 && pf <= z1 && pf < g.n3) {
-#pragma unroll
-				for (int s = 0; s < NS; s++)
-					tma_prefetch3(&maps.m[op.src_map(s)], (i1_0 - 1) * ME, i2_0 - 1, zoff + pf);
-#pragma unroll
-				for (int q = 0; q < NQ; q++) tma_prefetch3(&maps.m[op.q_map(q)], i1_0 * ME, i2_0, zoff + pf);
-			}
-		};
-		// Every stage of the previous segment has been waited for and read
-		// (its last step ended with a block barrier), so all slots are free.
-		issued = 0;
-		waited = 0;
-		if (t == 0)
-			for (; issued < NST && issued < np; issued++) issue(issued);
-
-		for (int j = 0; j <= np; j++) {
-			const int sj = (G + j) % NST;                          // stage slot of plane j
-			const unsigned par = (unsigned)(((G + j) / NST) & 1);  // its barrier parity
-			// Each thread waits for plane j's stage itself (the mbarrier's acquire
-			// makes the TMA data visible); a timeout is combined into the one
-			// block barrier at the end of the step.
-			bool ok = true;
-			if (j < np) ok = mbar_wait(&bar[sj], par);
-			// Pointwise fields an op reads with plain loads (Op::NG of them): issue
-			// the loads for this step's outputs (plane j-2) before the halo
-			// transform, so they are in flight during it.
-			Vec<T> gv[KO][NGX];
-			if (Op::NG > 0 && j >= 3) {
-				const long long zb = (long long)(z0 - 1 + j - 2) * plane;
-#pragma unroll
-				for (int k = 0; k < KO; k++)
-					if (oval >> k & 1u) op.gload(((long long)slice * g.npts + zb + obase[k]) * RB + lo, gv[k]);
-			}
-			// Phase 1: stencil input of plane j (transforming ops only).
-			if (!IDENT && j < np) {
-				const int p = z0 - 1 + j;
-				E *const st = stage0 + sj * SE;
-				// In place: over the source field INPLACE_SLOT of this plane's stage
-				// (each thread rewrites only the points it read).
-				E *cr = INPLACE ? st + Op::INPLACE_SLOT * HE : ring + (j & 3) * HE;
-				const bool pin = p >= 0 && p < g.n3;
-#pragma unroll
-				for (int k = 0; k < KC; k++) {
-					if (hoff[k] < 0) continue;
-					Vec<T> cv;
-					if (pin && (hval >> k & 1u)) {
-						Vec<T> raw[NS];
-#pragma unroll
-						for (int s = 0; s < NS; s++) raw[s] = lds(st + s * HE + hoff[k]);
-						cv = op.src(raw);
-					} else {
-						cv = vzero<T>();  // zero ghost layer
-					}
-					sts(cr + hoff[k], cv);
-				}
-				// The stage is refilled by TMA later: order these generic writes
-				// before those async-proxy writes.
-				if (INPLACE) fence_async_smem();
-			}
-			// Phase 2: outputs of plane m = j-2 from planes m-1, m, m+1.
-			if (j >= 3) {
-				const int m = j - 2;
-				const int z = z0 - 1 + m;
-				// Stage slots of planes m-1, m, m+1 (sj is the slot of plane j = m+2).
-				const int sm1 = sj >= 3 ? sj - 3 : sj - 3 + NST;
-				const int s0 = sj >= 2 ? sj - 2 : sj - 2 + NST;
-				const int sp1 = sj >= 1 ? sj - 1 : sj - 1 + NST;
-				const E *stz = stage0 + s0 * SE;
-				const E *cm, *c0, *cp;
-				bool zm = true, zp = true;  // planes m-1, m+1 inside the grid
-				if (STAGED) {
-					const int off = INPLACE ? Op::INPLACE_SLOT * HE : 0;
-					cm = stage0 + sm1 * SE + off;
-					c0 = stz + off;
-					cp = stage0 + sp1 * SE + off;
-					zm = z - 1 >= 0;
-					zp = z + 1 < g.n3;
+					for (int s = 0; s < NS; s++) raw[s] = lds(st + s * HE + hoff[k]);
+					cv = op.src(raw);
 				} else {
-					cm = ring + ((m - 1) & 3) * HE;
-					c0 = ring + (m & 3) * HE;
-					cp = ring + ((m + 1) & 3) * HE;
+					cv = vzero<T>();  // zero ghost layer
 				}
+				sts(cr + hoff[k], cv);
+			}
+			// The stage is refilled by TMA later: order these generic writes
+			// before those async-proxy writes.
+			if (INPLACE) fence_async_smem();
+		}
+		// Phase 2: outputs of plane m = j-2 from planes m-1, m, m+1.
+		if (j >= 3) {
+			const int m = j - 2;
+			const int z = z0 - 1 + m;
+			// Stage slots of planes m-1, m, m+1 (sj is the slot of plane j = m+2).
+			const int sm1 = sj >= 3 ? sj - 3 : sj - 3 + NST;
+			const int s0 = sj >= 2 ? sj - 2 : sj - 2 + NST;
+			const int sp1 = sj >= 1 ? sj - 1 : sj - 1 + NST;
+			const E *stz = stage0 + s0 * SE;
+			const E *cm, *c0, *cp;
+			bool zm = true, zp = true;  // planes m-1, m+1 inside the grid
+			if (STAGED) {
+				const int off = INPLACE ? Op::INPLACE_SLOT * HE : 0;
+				cm = stage0 + sm1 * SE + off;
+				c0 = stz + off;
+				cp = stage0 + sp1 * SE + off;
+				zm = z - 1 >= 0;
+				zp = z + 1 < g.n3;
+			} else {
+				cm = ring + ((m - 1) & 3) * HE;
+				c0 = ring + (m & 3) * HE;
+				cp = ring + ((m + 1) & 3) * HE;
+			}
 #pragma unroll
-				for (int k = 0; k < KO; k++) {
-					if (!(oin >> k & 1u)) continue;
-					if (j > 3) {  // planes m-1 and m were planes m and m+1 of the previous step
-						zprev[k] = zcur[k];
-						zcur[k] = znext[k];
-					} else {
-						zprev[k] = zm ? lds(cm + ooff[k]) : vzero<T>();
-						zcur[k] = lds(c0 + ooff[k]);
-					}
-					znext[k] = zp ? lds(cp + ooff[k]) : vzero<T>();
+			for (int k = 0; k < KO; k++) {
+				if (!(oin >> k & 1u)) continue;
+				if (j > 3) {  // planes m-1 and m were planes m and m+1 of the previous step
+					zprev[k] = zcur[k];
+					zcur[k] = znext[k];
+				} else {
+					zprev[k] = zm ? lds(cm + ooff[k]) : vzero<T>();
+					zcur[k] = lds(c0 + ooff[k]);
 				}
+				znext[k] = zp ? lds(cp + ooff[k]) : vzero<T>();
+			}
 #pragma unroll
-				for (int k = 0; k < KO; k++) {
-					if (!(oval >> k & 1u)) continue;
-					const int hc = ooff[k];
-					const Vec<T> &xc = zcur[k];
-					const Vec<T> xm1 = lds(c0 + hc - RB);
-					const Vec<T> xp1 = lds(c0 + hc + RB);
-					const Vec<T> xm2 = (ROWS && k > 0) ? zcur[k > 0 ? k - 1 : 0] : lds(c0 + hc - H1 * RB);
-					const Vec<T> xp2 = (ROWS && k + 1 < KO) ? zcur[k + 1 < KO ? k + 1 : k] : lds(c0 + hc + H1 * RB);
-					const Vec<T> &xm3 = zprev[k];
-					const Vec<T> &xp3 = znext[k];
-					Vec<T> y;
-					if constexpr (Op::SCALED) {
-						// The ring holds f and the stencil input is f .* iM: FP64
-						// scales each neighbour as the reference rounds p_hat and
-						// s_hat; FP32 folds iM into the coefficients.
-						if constexpr (sizeof(T) == 8) {
-							const T im = op.iMc;
-							if (C::PAIRS) {
-								const T c0 = amul(xc.v[0], im), c1 = amul(xc.v[1], im);
-								y.v[0] = st7x<T>(unit, op.ka, op.kb, op.kc, c0, amul(xm1.v[1], im), amul(xm2.v[0], im),
-								                amul(xm3.v[0], im), c1, amul(xp2.v[0], im), amul(xp3.v[0], im));
-								y.v[1] = st7x<T>(unit, op.ka, op.kb, op.kc, c1, c0, amul(xm2.v[1], im), amul(xm3.v[1], im),
-								                amul(xp1.v[0], im), amul(xp2.v[1], im), amul(xp3.v[1], im));
-							} else {
-#pragma unroll
-								for (int e = 0; e < V; e++)
-									y.v[e] = st7x<T>(unit, op.ka, op.kb, op.kc, amul(xc.v[e], im), amul(xm1.v[e], im),
-									                amul(xm2.v[e], im), amul(xm3.v[e], im), amul(xp1.v[e], im),
-									                amul(xp2.v[e], im), amul(xp3.v[e], im));
-							}
+			for (int k = 0; k < KO; k++) {
+				if (!(oval >> k & 1u)) continue;
+				const int hc = ooff[k];
+				const Vec<T> &xc = zcur[k];
+				const Vec<T> xm1 = lds(c0 + hc - RB);
+				const Vec<T> xp1 = lds(c0 + hc + RB);
+				const Vec<T> xm2 = (ROWS && k > 0) ? zcur[k > 0 ? k - 1 : 0] : lds(c0 + hc - H1 * RB);
+				const Vec<T> xp2 = (ROWS && k + 1 < KO) ? zcur[k + 1 < KO ? k + 1 : k] : lds(c0 + hc + H1 * RB);
+				const Vec<T> &xm3 = zprev[k];
+				const Vec<T> &xp3 = znext[k];
+				Vec<T> y;
+				if constexpr (Op::SCALED) {
+					// The ring holds f and the stencil input is f .* iM: FP64
+					// scales each neighbour as the reference rounds p_hat and
+					// s_hat; FP32 folds iM into the coefficients.
+					if constexpr (sizeof(T) == 8) {
+						const T im = op.iMc;
+						if (C::PAIRS) {
+							const T c0 = amul(xc.v[0], im), c1 = amul(xc.v[1], im);
+							y.v[0] = st7x<T>(unit, op.ka, op.kb, op.kc, c0, amul(xm1.v[1], im), amul(xm2.v[0], im),
+							                amul(xm3.v[0], im), c1, amul(xp2.v[0], im), amul(xp3.v[0], im));
+							y.v[1] = st7x<T>(unit, op.ka, op.kb, op.kc, c1, c0, amul(xm2.v[1], im), amul(xm3.v[1], im),
+							                amul(xp1.v[0], im), amul(xp2.v[1], im), amul(xp3.v[1], im));
 						} else {
 #pragma unroll
 							for (int e = 0; e < V; e++)
-								y.v[e] = st7<T>(op.kas, op.kbs, op.kcs, xc.v[e], xm1.v[e], xm2.v[e], xm3.v[e], xp1.v[e],
-								                xp2.v[e], xp3.v[e]);
+								y.v[e] = st7x<T>(unit, op.ka, op.kb, op.kc, amul(xc.v[e], im), amul(xm1.v[e], im),
+								                amul(xm2.v[e], im), amul(xm3.v[e], im), amul(xp1.v[e], im),
+								                amul(xp2.v[e], im), amul(xp3.v[e], im));
 						}
-					} else if (C::PAIRS) {
-						// Points 2m, 2m+1 of one vector: i1 neighbours across the pair.
-						y.v[0] = st7x<T>(unit, op.ka, op.kb, op.kc, xc.v[0], xm1.v[1], xm2.v[0], xm3.v[0], xc.v[1], xp2.v[0],
-						                xp3.v[0]);
-						y.v[1] = st7x<T>(unit, op.ka, op.kb, op.kc, xc.v[1], xc.v[0], xm2.v[1], xm3.v[1], xp1.v[0], xp2.v[1],
-						                xp3.v[1]);
 					} else {
 #pragma unroll
 						for (int e = 0; e < V; e++)
-							y.v[e] = st7x<T>(unit, op.ka, op.kb, op.kc, xc.v[e], xm1.v[e], xm2.v[e], xm3.v[e], xp1.v[e], xp2.v[e],
-							                xp3.v[e]);
+							y.v[e] = st7<T>(op.kas, op.kbs, op.kcs, xc.v[e], xm1.v[e], xm2.v[e], xm3.v[e], xp1.v[e],
+							                xp2.v[e], xp3.v[e]);
 					}
-					Vec<T> qv[NQ > 0 ? NQ : 1];
+				} else if (C::PAIRS) {
+					// Points 2m, 2m+1 of one vector: i1 neighbours across the pair.
+					y.v[0] = st7x<T>(unit, op.ka, op.kb, op.kc, xc.v[0], xm1.v[1], xm2.v[0], xm3.v[0], xc.v[1], xp2.v[0],
+					                xp3.v[0]);
+					y.v[1] = st7x<T>(unit, op.ka, op.kb, op.kc, xc.v[1], xc.v[0], xm2.v[1], xm3.v[1], xp1.v[0], xp2.v[1],
+					                xp3.v[1]);
+				} else {
 #pragma unroll
-					for (int qq = 0; qq < NQ; qq++) qv[qq] = lds(stz + NS * HE + qq * IE + qoff[k]);
-					Vec<T> rc[NS];
-					if (Op::USES_RAW_CENTER && op.raw_center()) {
-#pragma unroll
-						for (int s = 0; s < NS; s++) rc[s] = lds(stz + s * HE + hc);
-					}
-					const long long pidx = (long long)z * plane + obase[k];
-					const long long o = ((long long)slice * g.npts + pidx) * RB + lo;
-					op.out(o, pidx, lane0 + lo, xc, y, qv, rc, gv[k], part);
+					for (int e = 0; e < V; e++)
+						y.v[e] = st7x<T>(unit, op.ka, op.kb, op.kc, xc.v[e], xm1.v[e], xm2.v[e], xm3.v[e], xp1.v[e], xp2.v[e],
+						                xp3.v[e]);
 				}
-			}
-			if (__syncthreads_or(!ok)) {
-				failed = true;  // outputs of this step may be wrong; the host sees gl->err
-				break;
-			}
-			if (j < np) waited = j + 1;
-			// The stage of plane j-KEEP has been read for the last time.
-			if (t == 0 && j >= KEEP && issued < np) {
-				issue(issued);
-				issued++;
+				Vec<T> qv[NQ > 0 ? NQ : 1];
+#pragma unroll
+				for (int qq = 0; qq < NQ; qq++) qv[qq] = lds(stz + NS * HE + qq * IE + qoff[k]);
+				Vec<T> rc[NS];
+				if (Op::USES_RAW_CENTER && op.raw_center()) {
+#pragma unroll
+					for (int s = 0; s < NS; s++) rc[s] = lds(stz + s * HE + hc);
+				}
+				const long long pidx = (long long)z * plane + obase[k];
+				const long long o = ((long long)slice * g.npts + pidx) * RB + lo;
+				op.out(o, pidx, lane0 + lo, xc, y, qv, rc, gv[k], part);
 			}
 		}
-		if (failed) break;
-		G += np;
+		if (__syncthreads_or(!ok)) {
+			failed = true;  // outputs of this step may be wrong; the host sees gl->err
+			break;
+		}
+		if (j < np) waited = j + 1;
+		// The stage of plane j-KEEP has been read for the last time.
+		if (t == 0 && j >= KEEP && issued < np) {
+			issue(issued);
+			issued++;
+		}
 	}
 	if (failed) {
 		// Timed out: flag the error and wait (bounded) for the copies still in
@@ -456,8 +409,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) k_stream(SGeo g, const __
 		// sees the flag and reports the solve as failed.
 		if (t == 0) {
 			atomicExch(&gl->err, 1);
-			for (int jj = waited; jj < issued; jj++)
-				mbar_wait(&bar[(G + jj) % NST], (unsigned)(((G + jj) / NST) & 1));
+			for (int jj = waited; jj < issued; jj++) mbar_wait(&bar[jj % NST], (unsigned)((jj / NST) & 1));
 		}
 		__syncthreads();
 	}
@@ -1696,7 +1648,7 @@ static void tile_for(int rb, int eb, int *P1, int *P2, int kind = 0) {
 }
 
 static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int nz_force = 0, int kind = 0,
-                  int pfd = -1, bool seg_ok = false) {
+                  int pfd = -1) {
 	int P1, P2;
 	tile_for(rb, eb, &P1, &P2, kind);
 	const int t1 = (g.n1 + P1 - 1) / P1, t2 = (g.n2 + P2 - 1) / P2;
@@ -1739,18 +1691,7 @@ static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int
 	sg->zc = zc;
 	sg->tiles1 = t1;
 	sg->pfd = pfd >= 0 ? pfd : SEDI_STREAM_PFD;
-	sg->ntiles = t1 * t2;
-	sg->seg = 0;
 	*grid = dim3((unsigned)(t1 * t2), (unsigned)slices, (unsigned)nz);
-	// One lane slice with fewer tiles than a wave of blocks (a single vector
-	// in the pair layout: 32 tiles of 32x32 at 256^3): one block per SM, each
-	// an equal share of the (tile, plane) units, so every SM streams the same
-	// number of planes in one wave.
-	const long long units = (long long)t1 * t2 * g.n3;
-	if (seg_ok && nz_force <= 0 && slices == 1 && t1 * t2 < wave && units >= wave) {
-		sg->seg = 1;
-		*grid = dim3((unsigned)wave, 1u, 1u);
-	}
 }
 
 template <class C, class Op>
@@ -2359,9 +2300,9 @@ int pairs_alloc(Ctx *c) {
 	const Tuning tu = tuning_for(TuneKey{c->solver, SEDI_PREC_FP64, pick_R(1, false), c->g.n1, c->g.n2, c->g.n3});
 	B->acfg = tu.acfg >= 1 && tu.acfg <= 3 ? tu.acfg : default_form(B->ks, true);
 	B->tuned = tu;
-	shape(g, 2, 2, 8, &B->gT, &B->gridT, tu.nz, 0, tu.pfd, true);
-	shape(g, 2, 2, 8, &B->gT1, &B->gridT1, tu.nz, 1, tu.pfd, true);
-	shape(g, 2, 2, 8, &B->gD, &B->gridD, tu.nz, 0, tu.pfd, true);
+	shape(g, 2, 2, 8, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
+	shape(g, 2, 2, 8, &B->gT1, &B->gridT1, tu.nz, 1, tu.pfd);
+	shape(g, 2, 2, 8, &B->gD, &B->gridD, tu.nz, 0, tu.pfd);
 	size_t nblk = (size_t)B->gridT.x * B->gridT.z;
 	if ((size_t)B->gridT1.x * B->gridT1.z > nblk) nblk = (size_t)B->gridT1.x * B->gridT1.z;
 	if (cudaMalloc(&B->partials, sizeof(double) * nblk * kMaxDots * B->R) != cudaSuccess ||

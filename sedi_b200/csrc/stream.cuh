@@ -172,8 +172,6 @@ struct SGeo {
 	int tiles1;     // tiles along i1
 	long long npts; // n1*n2*n3
 	int pfd;        // planes the L2 prefetch runs ahead of the TMA loads (0: none)
-	int ntiles;     // point tiles per plane
-	int seg;        // 1: blocks take equal shares of the (tile, plane) units (one lane slice)
 };
 
 __host__ __device__ __forceinline__ long long sliced(long long i, int j, int W, long long npts) {
