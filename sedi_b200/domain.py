@@ -15,9 +15,11 @@ device copies).
   ghost (2 .. nloc-1) while it is in flight, waits, then computes planes 1 and
   nloc -- the reference's inner/border split.
 * Dot products come back per plane, each summed in an order that depends only
-  on (n1, n2); the planes are gathered from all slabs and added in global
-  plane order with ``math.fsum``.  Every vector of the solve is therefore
-  identical bit for bit for every P, including P = 1.
+  on (n1, n2), into one [n3, 3] array of all planes (a slab writes its own
+  rows; across ranks the rows are summed with zeros in an all-reduce, which
+  is exact); that array is then reduced over planes on the device, an order
+  fixed by its shape.  Every vector of the solve is therefore identical bit
+  for bit for every P, including P = 1.
 * The three solvers are the reference's CG (Cg.hpp), pipelined CG
   (PipelinedCg.hpp) and BiCGStab (BiCgStab.hpp) with the constant Jacobi
   preconditioner 1/a; each sweep fuses a stencil with the elementwise updates
@@ -137,8 +139,14 @@ class GpuSlabBackend:
                                                    device=self.device)
         return self._scratch[nloc]
 
-    def new_plane_part(self, nloc):
-        return self.torch.zeros((nloc, DOTS), dtype=self.torch.float64, device=self.device)
+    def plane_sums(self, n3):
+        """The [n3, 3] per-plane dot products of every slab."""
+        return self.torch.zeros((n3, DOTS), dtype=self.torch.float64, device=self.device)
+
+    def totals(self, G):
+        """The three dot products: G summed over planes (device reduction of a
+        fixed shape, so of a fixed order), read back once."""
+        return tuple(G.sum(0).tolist())
 
     def sweep(self, mode, nloc, z_lo, z_hi, plane_part=None, first=False, **kw):
         """sedi_slab_sweep over ghosted planes [z_lo, z_hi): vectors (slab
@@ -219,6 +227,7 @@ class _SlabSolver:
         self.iM = 1.0 / self.stencil.a  # constant Jacobi preconditioner (stochastic-estimator.cc:101-103)
         self.timers = {"halo_wait": 0.0, "dot_comm": 0.0}
         self.last_history = []
+        self._G = self.backend.plane_sums(self.n3)
 
     # ---- vectors -----------------------------------------------------------
     def zeros(self):
@@ -259,25 +268,23 @@ class _SlabSolver:
             q.wait()
         self.timers["halo_wait"] += time.perf_counter() - t0
 
-    def _dots(self, plane_parts):
-        """The three global dot products of a sweep from the local slabs'
-        per-plane partials: gathered from every rank, added in global plane
-        order (DistrAsyncDotProds.hpp:85-136 sums rank partials with an
-        allreduce instead)."""
-        import torch
+    def _plane_part(self, j):
+        """Rows of the global per-plane array that local slab j writes."""
+        first, count = self.ranges[self.local[j]]
+        return self._G[first:first + count]
+
+    def _dots(self, plane_parts=None):
+        """The three global dot products of a sweep from the per-plane array:
+        across ranks the rows of the other slabs are zero here, so an
+        all-reduce assembles it exactly (DistrAsyncDotProds.hpp:85-136 sums
+        rank partials with an allreduce); then one reduction over all n3
+        planes on the device, whose order depends only on n3."""
         t0 = time.perf_counter()
-        loc = torch.cat(plane_parts, 0) if len(plane_parts) > 1 else plane_parts[0]
         if self.world > 1:
-            most = max(c for _, c in self.ranges)
-            pad = torch.zeros((most, DOTS), dtype=loc.dtype, device=loc.device)
-            pad[:loc.shape[0]] = loc
-            got = [torch.empty_like(pad) for _ in range(self.world)]
-            self.dist.all_gather(got, pad, group=self.group)
-            allp = np.concatenate([self.backend.to_numpy(got[s])[:self.ranges[s][1]] for s in range(self.parts)])
-        else:
-            allp = self.backend.to_numpy(loc)
+            self.dist.all_reduce(self._G, group=self.group)
+        tot = self.backend.totals(self._G)
         self.timers["dot_comm"] += time.perf_counter() - t0
-        return tuple(math.fsum(allp[:, d].tolist()) for d in range(DOTS))
+        return tot
 
     # ---- sweeps --------------------------------------------------------------
     def _args(self, kw, j):
@@ -287,13 +294,12 @@ class _SlabSolver:
         """`mode` over every plane of every local slab, no exchange (an
         elementwise mode, or a stencil whose source's ghosts are current).
         Returns the per-plane partials (None for a mode without dots)."""
-        parts = []
+        dots = mode in MODE_DOTS
+        if dots and self.world > 1:
+            self._G.zero_()
         for j in range(len(self.local)):
             nloc = self._nloc(j)
-            pp = self.backend.new_plane_part(nloc) if mode in MODE_DOTS else None
-            self.backend.sweep(mode, nloc, 1, nloc + 1, pp, **self._args(kw, j))
-            parts.append(pp)
-        return parts
+            self.backend.sweep(mode, nloc, 1, nloc + 1, self._plane_part(j) if dots else None, **self._args(kw, j))
 
     def _stencil_sweep(self, mode, src, **kw):
         """Exchange src's halos and run `mode` on every local slab: the inner
@@ -302,14 +308,15 @@ class _SlabSolver:
         exchange (:87-97)."""
         reqs = self._exchange(src)
         kw["src"] = src
-        parts = []
+        dots = mode in MODE_DOTS
+        if dots and self.world > 1:
+            self._G.zero_()
+        parts = [self._plane_part(j) if dots else None for j in range(len(self.local))]
         overlap = not (self.mode & 1)
         for j in range(len(self.local)):
             nloc = self._nloc(j)
-            pp = self.backend.new_plane_part(nloc) if mode in MODE_DOTS else None
-            parts.append(pp)
             if overlap and nloc > 2:
-                self.backend.sweep(mode, nloc, 2, nloc, pp, **self._args(kw, j))
+                self.backend.sweep(mode, nloc, 2, nloc, parts[j], **self._args(kw, j))
         self._wait(reqs)
         for j in range(len(self.local)):
             nloc = self._nloc(j)
@@ -319,7 +326,6 @@ class _SlabSolver:
                 self.backend.sweep(mode, nloc, nloc, nloc + 1, parts[j], **args)
             else:
                 self.backend.sweep(mode, nloc, 1, nloc + 1, parts[j], **args)
-        return parts
 
     def apply(self, x, y):
         """y = A x (Stencil.hpp:38-54 through DistrAsyncStencil)."""

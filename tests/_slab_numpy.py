@@ -2,7 +2,7 @@
 
 It implements the interface of sedi_b200.domain.GpuSlabBackend on CPU torch
 tensors so that the slab decomposition's host logic -- halo exchange, the
-plane-ordered dot reduction, the three solver loops -- runs on gloo ranks
+per-plane dot reduction, the three solver loops -- runs on gloo ranks
 without a GPU.  Elementwise values round as the reference's (numpy evaluates
 one operator at a time, no FMA: Stencil.hpp:43-50, SliceOps.hpp:17-108); a
 plane's dot product is np.sum over the plane, the same whichever slab holds
@@ -42,8 +42,11 @@ class NumpySlabBackend:
     def to_numpy(self, t):
         return t.numpy()
 
-    def new_plane_part(self, nloc):
-        return torch.zeros((nloc, DOTS), dtype=torch.float64)
+    def plane_sums(self, n3):
+        return torch.zeros((n3, DOTS), dtype=torch.float64)
+
+    def totals(self, G):
+        return tuple(G.sum(0).tolist())
 
     def _apply_plane(self, X, z, scale=None):
         f = (lambda k: X[k] * scale) if scale is not None else (lambda k: X[k])
