@@ -2130,6 +2130,15 @@ static void launch_bicg_s(Ctx *c, Batched *B, const Op &o, cudaStream_t s) {
 	}
 }
 
+// BiCGStab sweep 1 (three stencil sources) in form 3: p written over p_old
+// (slot 1) in the stage, on its own 32x16 tiles with six stages instead of
+// five and a ring.
+template <class T, int RBT, bool PAIRS>
+static void launch_bicg_1(Ctx *c, Batched *B, const OpBicg1<T> &o, cudaStream_t s) {
+	if (B->acfg == 3) launchT<T, RBT, PAIRS>(c, B, InPlace<OpBicg1<T>, 0>(o), s);
+	else launchT<T, RBT, PAIRS>(c, B, o, s);
+}
+
 template <class T, int RBT, int RBD, bool PAIRS = false>
 static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	cudaStream_t s = c->stream;
@@ -2140,7 +2149,7 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 	o1.v0 = (T *)B->v[0];
 	o1.v1 = (T *)B->v[1];
 	o1.rhat = (T *)B->rhat;
-	launchT<T, RBT, PAIRS>(c, B, o1, s);
+	launch_bicg_1<T, RBT, PAIRS>(c, B, o1, s);
 	OpBicg2<T> o2;
 	set_scaled_coef(c, o2);
 	launch_bicg_s<T, RBT, PAIRS>(c, B, o2, s);
@@ -2639,7 +2648,7 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		                                          // 3: r, v, x, p, r_hat in, x, r out
 		for (int k = 0; k < 3; k++) {
 			auto one = [&]() {
-				if (k == 0) launchT<T, RBT, PAIRS>(c, B, o1, s);
+				if (k == 0) launch_bicg_1<T, RBT, PAIRS>(c, B, o1, s);
 				else if (k == 1) launch_bicg_s<T, RBT, PAIRS>(c, B, o2, s);
 				else launch_bicg_s<T, RBT, PAIRS>(c, B, o3, s);
 			};

@@ -312,7 +312,9 @@ class _SlabSolver:
         if dots and self.world > 1:
             self._G.zero_()
         parts = [self._plane_part(j) if dots else None for j in range(len(self.local))]
-        overlap = not (self.mode & 1)
+        # Only halos from other ranks are in flight; a process's own slabs get
+        # theirs by copies already queued before the sweep.
+        overlap = not (self.mode & 1) and self.world > 1
         for j in range(len(self.local)):
             nloc = self._nloc(j)
             if overlap and nloc > 2:
