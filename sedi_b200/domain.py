@@ -273,7 +273,7 @@ class _SlabSolver:
         first, count = self.ranges[self.local[j]]
         return self._G[first:first + count]
 
-    def _dots(self, plane_parts=None):
+    def _dots(self):
         """The three global dot products of a sweep from the per-plane array:
         across ranks the rows of the other slabs are zero here, so an
         all-reduce assembles it exactly (DistrAsyncDotProds.hpp:85-136 sums
@@ -293,19 +293,21 @@ class _SlabSolver:
     def _sweep(self, mode, **kw):
         """`mode` over every plane of every local slab, no exchange (an
         elementwise mode, or a stencil whose source's ghosts are current).
-        Returns the per-plane partials (None for a mode without dots)."""
+        Returns the mode's three global dot products (None without dots)."""
         dots = mode in MODE_DOTS
         if dots and self.world > 1:
             self._G.zero_()
         for j in range(len(self.local)):
             nloc = self._nloc(j)
             self.backend.sweep(mode, nloc, 1, nloc + 1, self._plane_part(j) if dots else None, **self._args(kw, j))
+        return self._dots() if dots else None
 
     def _stencil_sweep(self, mode, src, **kw):
         """Exchange src's halos and run `mode` on every local slab: the inner
         planes while the halos move, then the border planes
         (DistrAsyncStencil.hpp:52-100); mode bit 0 = one sweep after the
-        exchange (:87-97)."""
+        exchange (:87-97).  Returns the mode's three global dot products
+        (None without dots)."""
         reqs = self._exchange(src)
         kw["src"] = src
         dots = mode in MODE_DOTS
@@ -328,6 +330,7 @@ class _SlabSolver:
                 self.backend.sweep(mode, nloc, nloc, nloc + 1, parts[j], **args)
             else:
                 self.backend.sweep(mode, nloc, 1, nloc + 1, parts[j], **args)
+        return self._dots() if dots else None
 
     def apply(self, x, y):
         """y = A x (Stencil.hpp:38-54 through DistrAsyncStencil)."""
@@ -337,7 +340,7 @@ class _SlabSolver:
         """r = b - A x; returns (<b,b> with 0 taken as 1, <r,r>) -- the common
         start of the three solvers (Cg.hpp:112-129, PipelinedCg.hpp:104-123,
         BiCgStab.hpp:122-139)."""
-        bb, rr, _ = self._dots(self._stencil_sweep(SETUP, x, r=r, b=b))
+        bb, rr, _ = self._stencil_sweep(SETUP, x, r=r, b=b)
         return (1.0 if bb == 0.0 else bb), rr
 
     def solve(self, x, b, maxiter, tol, work=None):
@@ -415,12 +418,12 @@ class SlabCg(_SlabSolver):
         for it in range(1, maxiter + 1):
             first = it == 1
             self._sweep(CG_P, r=r, p=p, iM=self.iM, beta=beta, first=first)  # p = u + beta p (:144-147, :188)
-            sp, ru1, _ = self._dots(self._stencil_sweep(CG_SP, p, r=r, iM=self.iM, first=first))  # :152-165
+            sp, ru1, _ = self._stencil_sweep(CG_SP, p, r=r, iM=self.iM, first=first)  # :152-165
             if first:
                 ru = ru1
             alpha = _fdiv(ru, sp)  # :166
             # x += alpha p, r -= alpha s, u = r .* iM; <r,u>, <r,r> (:169-182); the ghosts of p are current
-            ru_new, rr, _ = self._dots(self._sweep(CG_UPDATE, src=p, x=x, r=r, iM=self.iM, alpha=alpha))
+            ru_new, rr, _ = self._sweep(CG_UPDATE, src=p, x=x, r=r, iM=self.iM, alpha=alpha)
             beta = _fdiv(ru_new, ru)  # :185
             ru = ru_new
             err = _sqrt(_fdiv(rr, bb))  # :191
@@ -454,7 +457,7 @@ class SlabPipelinedCg(_SlabSolver):
         if err < tol:  # :124-128
             return 0, err, 0
         # u = r .* iM, w = A u, z = q = s = p = 0 (:138-149); dots of iteration 1 (:155, :169-172)
-        gamma, delta, rr = self._dots(self._stencil_sweep(PCG_SETUP, r, u=u, w=w, q=q, s=s, p=p, z=z, iM=self.iM))
+        gamma, delta, rr = self._stencil_sweep(PCG_SETUP, r, u=u, w=w, q=q, s=s, p=p, z=z, iM=self.iM)
         alpha = beta = 0.0
         for it in range(1, maxiter + 1):
             if it > 1:  # :175-181
@@ -465,8 +468,8 @@ class SlabPipelinedCg(_SlabSolver):
                 alpha = _fdiv(gamma, delta)
             gamma_old = gamma
             rr_it = rr
-            gamma, delta, rr = self._dots(self._stencil_sweep(PCG_ITER, w, x=x, r=r, u=u, wn=wn, q=q, s=s, p=p, z=z,
-                                                              iM=self.iM, alpha=alpha, beta=beta))
+            gamma, delta, rr = self._stencil_sweep(PCG_ITER, w, x=x, r=r, u=u, wn=wn, q=q, s=s, p=p, z=z,
+                                                   iM=self.iM, alpha=alpha, beta=beta)
             w, wn = wn, w
             err = _sqrt(_fdiv(rr_it, bb))  # :227 (the <r,r> of the iteration's start)
             hist.append(err)
@@ -507,20 +510,20 @@ class SlabBiCgStab(_SlabSolver):
                 self._sweep(BICG_P, r=r, p=p, v=v, beta=beta, bo=-beta * omega)  # :169
             else:
                 self._sweep(BICG_P, r=r, p=p, first=True)  # :172
-            vr, _, _ = self._dots(self._stencil_sweep(BICG_V, p, v=v, rhat=rhat, iM=iM))  # :176-186
+            vr, _, _ = self._stencil_sweep(BICG_V, p, v=v, rhat=rhat, iM=iM)  # :176-186
             alpha = _fdiv(rho, vr)  # :187
             self._sweep(BICG_S, r=r, v=v, s=s, alpha=alpha)  # :190
             # t = A (s .* iM) with <s,s>, <t,s>, <t,t>: t is computed before the
             # early-exit test on <s,s> (:193-199) and unused when it exits.
-            ss, ts, tt = self._dots(self._stencil_sweep(BICG_T, s, t=t, iM=iM))
+            ss, ts, tt = self._stencil_sweep(BICG_T, s, t=t, iM=iM)
             s_norm2 = ss
             if ss < tol * tol:  # :195
                 self._sweep(BICG_X, x=x, p=p, alpha=alpha, iM=iM)  # :197
                 it = k
                 break
             omega = _fdiv(ts, tt)  # :213
-            rr, rho_next, _ = self._dots(self._sweep(BICG_XR, x=x, p=p, s=s, t=t, r=r, rhat=rhat, alpha=alpha,
-                                                     omega=omega, iM=iM))  # :217-224
+            rr, rho_next, _ = self._sweep(BICG_XR, x=x, p=p, s=s, t=t, r=r, rhat=rhat, alpha=alpha,
+                                            omega=omega, iM=iM)  # :217-224
             err = _sqrt(_fdiv(rr, bb))  # :227
             hist.append(err)
             if err <= tol:  # :229
