@@ -350,7 +350,8 @@ int sedi_server_stats(const sedi_server *srv, double *peak_bytes, double *budget
  * for the process and used by every context created afterwards with the
  * same parameters (and by the server's admission sizes).
  * choice[0..5] = slice width, i3 chunks (0: the built-in model), period,
- * iterations per graph, L2 prefetch distance in planes, narrow-sweep form; *score_ms (optional)
+ * iterations per graph, L2 prefetch distance in planes (-1: the built-in
+ * distance), narrow-sweep form; *score_ms (optional)
  * = the winning estimate time (flags & 1) or summed per-iteration sweep
  * time.  Needs device memory for one such context at a time.
  */

@@ -1424,8 +1424,15 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 // grid): lane-slice width of the Krylov fields, i3 split of the sweeps,
 // reliable-update period and iterations per captured graph.  Zero fields
 // mean "default".  Filled by sedi_autotune, read when a context is created.
+// Default L2 prefetch distance of the sweeps, in planes (-1: 2 when a block
+// streams at most 64 planes, else 0).  Measured on B200: at 128^3 x 64 lanes
+// (32-plane chunks) 2 planes took mixed CG B from 462 to 442 us and the ring
+// form of sweep A from 350 to 318 us, and the single-vector sweeps at 256^3
+// (29-plane chunks) from 102 / 137 to 96 / 131 us; at 256^3 x 128 (whole
+// columns) CG B went from 6.88 to 6.97 ms and in-place sweep A from 4.21 to
+// 4.26 ms.
 #ifndef SEDI_STREAM_PFD
-#define SEDI_STREAM_PFD 0  // default L2 prefetch distance of the sweeps, in planes (0: none)
+#define SEDI_STREAM_PFD -1
 #endif
 // Form of the narrow sweeps (CG sweep A, BiCGStab sweeps 2 and 3): 1 ring
 // (32x32), 2 in place (32x16, 2 blocks/SM), 3 in place (32x32, 6 stages).
@@ -1444,7 +1451,7 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 static int default_form(int ks, bool single) { return !single && ks == SEDI_CG ? SEDI_CGA_FORM : SEDI_NARROW_FORM; }
 struct Tuning {
 	int W = 0, nz = 0, period = 0, chunk = 0;
-	int pfd = -1;   // L2 prefetch distance in planes (-1: SEDI_STREAM_PFD)
+	int pfd = -1;   // L2 prefetch distance in planes (-1: the default, see SEDI_STREAM_PFD)
 	int acfg = 0;   // form of the narrow sweeps (0: default_form)
 };
 struct TuneKey {
@@ -1690,7 +1697,7 @@ static void shape(const Geo &g, int R, int rb, int eb, SGeo *sg, dim3 *grid, int
 	sg->npts = g.n;
 	sg->zc = zc;
 	sg->tiles1 = t1;
-	sg->pfd = pfd >= 0 ? pfd : SEDI_STREAM_PFD;
+	sg->pfd = pfd >= 0 ? pfd : (SEDI_STREAM_PFD >= 0 ? SEDI_STREAM_PFD : (zc <= 64 ? 2 : 0));
 	*grid = dim3((unsigned)(t1 * t2), (unsigned)slices, (unsigned)nz);
 }
 
@@ -2998,7 +3005,7 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 		double ms = 0.0;
 		const int rc = score(t, &ms);
 		if (rc) return rc;
-		if (ms < 0.98 * best_ms || (best.pfd < 0 && pf == SEDI_STREAM_PFD)) best_ms = ms, best = t;
+		if (ms < 0.98 * best_ms) best_ms = ms, best = t;  // a clear win over the default
 	}
 	// Form of CG's sweep A and BiCGStab's sweeps 2 and 3 (ring, or in place
 	// with two blocks per SM or six stages).
@@ -3068,7 +3075,7 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 	out[1] = best.nz;
 	out[2] = best.period;
 	out[3] = best.chunk;
-	out[4] = best.pfd >= 0 ? best.pfd : SEDI_STREAM_PFD;
+	out[4] = best.pfd;  // -1: the default distance
 	out[5] = best.acfg ? best.acfg : default_form(kernel_solver(solver, mixed), single);
 	if (score_ms) *score_ms = best_est >= 0 ? best_est : best_ms;
 	return 0;
