@@ -561,60 +561,74 @@ def run_sweeps(S, args):
 def run_slab(S, args):
     """The slab (i3) decomposition on one GPU, P slabs in one process (halos
     by device copies), FP64, against the single-vector form on the same
-    probe: (1) each solver at 512^3, 200 fixed iterations (tol 0), P = 1, 2,
-    4: GPoint-iterations/s and the host time in dot-product reads; (2) CG at
-    256^3 to tol 1e-9, P = 1 and 2: iteration counts and whether D matches
-    across P bit for bit."""
+    probe: (1) each solver at 512^3, one probe, 200 fixed iterations (tol 0),
+    P = 1, 2, 4: GPoint-iterations/s of the solve alone (probe generation
+    outside the timed region) and the host time spent reading dot products;
+    (2) CG at 256^3 to tol 1e-9, P = 1 and 2: iteration counts and whether D
+    matches across P bit for bit."""
     import numpy as np
     import torch
     from sedi_b200.domain import slab_solver
 
-    def run_sv(solver, g, samples, maxiter, tol):
-        with S.Context(solver, g) as c:
-            c.estimate(1, SEED, 5, tol, ignore_errors=True)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            r = c.estimate(samples, SEED, maxiter, tol, ignore_errors=True)
-            return r, time.perf_counter() - t0
-
-    def run_slabs(solver, g, parts, samples, maxiter, tol):
+    def solve_slabs(solver, g, parts, maxiter, tol):
         sv = slab_solver(solver, g, parts, loopback=True)
-        sv.estimate(1, SEED, 5, tol)
+        x, b = sv.zeros(), sv.zeros()
+        work = sv.work()
+        plane = g[0] * g[1]
+        for j, s_ in enumerate(sv.local):
+            sv.backend.fill_probe(b[j], SEED, sv.ranges[s_][0] * plane)
+        sv.solve(x, b, 3, tol, work)  # warm-up
+        for j in range(len(sv.local)):
+            x[j].zero_()
         torch.cuda.synchronize()
         sv.timers = {"halo_wait": 0.0, "dot_comm": 0.0}
         t0 = time.perf_counter()
-        r = sv.estimate(samples, SEED, maxiter, tol)
+        res, err, it = sv.solve(x, b, maxiter, tol, work)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        D = sv.gather(r["D"])
-        out = (r, dt, D, sv.timers["dot_comm"])
-        del sv
+        out = (it, dt, sv.timers["dot_comm"], err)
+        del sv, x, b, work
         torch.cuda.empty_cache()
         return out
 
     g = (512, 512, 512)
     n = g[0] * g[1] * g[2]
+    probe = torch.empty((1, n), dtype=torch.float64, device="cuda")
+    S.fill_probes_dev(SEED, probe)
+    D = torch.empty(n, dtype=torch.float64, device="cuda")
     for solver in ("cg", "pcg", "bicgstab"):
-        rp, dtp = run_sv(solver, g, 1, 200, 0.0)
+        with S.Context(solver, g) as c:
+            c.estimate_dev(1, probe, D, maxiter=5, tol=0.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rp = c.estimate_dev(1, probe, D, maxiter=200, tol=0.0)
+            torch.cuda.synchronize()
+            dtp = time.perf_counter() - t0
         row = {"workload": f"slab decomposition on one GPU, {solver}, 512^3, 1 probe, 200 fixed iterations, FP64",
-               "single_vector_gpoint_iterations_per_s": float(np.sum(rp["iters"])) * n / dtp / 1e9, "slabs": []}
+               "single_vector_gpoint_iterations_per_s": float(rp["iters"][0]) * n / dtp / 1e9, "slabs": []}
         for parts in (1, 2, 4):
-            r, dt, D, dots = run_slabs(solver, g, parts, 1, 200, 0.0)
-            row["slabs"].append({"parts": parts, "gpoint_iterations_per_s": float(np.sum(r["iters"])) * n / dt / 1e9,
-                                 "s": dt, "dot_read_s": dots,
-                                 "D_rel_err_vs_single_vector": _relmax(D, rp["D"])})
+            it, dt, dots, err = solve_slabs(solver, g, parts, 200, 0.0)
+            row["slabs"].append({"parts": parts, "gpoint_iterations_per_s": it * n / dt / 1e9, "s": dt,
+                                 "dot_read_s": dots, "final_err": err})
         print(json.dumps(row), flush=True)
+    del probe, D
+    torch.cuda.empty_cache()
     g = (256, 256, 256)
-    rp, dtp = run_sv("cg", g, 2, 5000, 1e-9)
+    with S.Context("cg", g) as c:
+        rp = c.estimate(2, SEED, 5000, 1e-9)
     row = {"workload": "slab decomposition on one GPU, cg, 256^3, 2 probes, tol 1e-9, FP64",
            "single_vector_iterations": rp["iters"].tolist(), "slabs": []}
     D1 = None
     for parts in (1, 2):
-        r, dt, D, dots = run_slabs("cg", g, parts, 2, 5000, 1e-9)
-        D1 = D if D1 is None else D1
-        row["slabs"].append({"parts": parts, "iterations": r["iters"].tolist(), "probe_solves_per_s": 2 / dt,
-                             "D_equal_to_one_slab": bool(np.array_equal(D, D1)),
-                             "D_rel_err_vs_single_vector": _relmax(D, rp["D"])})
+        sv = slab_solver("cg", g, parts, loopback=True)
+        r = sv.estimate(2, SEED, 5000, 1e-9)
+        Dg = sv.gather(r["D"])
+        D1 = Dg if D1 is None else D1
+        row["slabs"].append({"parts": parts, "iterations": r["iters"].tolist(),
+                             "D_equal_to_one_slab": bool(np.array_equal(Dg, D1)),
+                             "D_rel_err_vs_single_vector": _relmax(Dg, rp["D"])})
+        del sv
+        torch.cuda.empty_cache()
     print(json.dumps(row), flush=True)
 
 

@@ -141,3 +141,20 @@ def test_burst_of_fresh_contexts_matches_direct():
         got = [srv.take(i) for i in ids]
     for j, l, g in zip(jobs, lanes, got):
         _same(g, _direct(j, l))
+
+
+def test_contexts_reused_across_sample_counts_of_one_padded_lane_count():
+    """Mixed jobs of 9, 20 and 30 probes on one grid all pad to 32 lanes: one
+    context serves them one after another, and each result is bit-identical
+    to the direct estimate on a context created for its own sample count."""
+    jobs = [("cg", (40, 36, 32), k, 50 + k, 2000, 1e-9, S.MIXED) for k in (9, 20, 30)]
+    with S.Server() as srv:
+        got = []
+        for job in jobs:
+            j = _submit(srv, job)
+            srv.wait(j)
+            got.append(srv.take(j))
+        st = srv.stats()
+    assert st["ctx_created"] == 1 and st["ctx_reused"] == 2
+    for job, g in zip(jobs, got):
+        _same(g, _direct(job, job[2]))
