@@ -280,8 +280,12 @@ bool mode_args_ok(int mode, const sedi_slab_args &a) {
 
 template <int MODE>
 void launch_mode(SlabGeo g, Coef k, int z_lo, int z_hi, const sedi_slab_args &a, double *chunk, cudaStream_t s) {
-	const dim3 grid(kSlabChunks, (unsigned)(z_hi - z_lo));
-	k_slab_sweep<MODE><<<grid, kSlabThreads, 0, s>>>(g, k, z_lo, z_hi, a, chunk);
+	constexpr int kMaxPlanes = 65535;  // grid y limit: one block row per plane
+	for (int z = z_lo; z < z_hi; z += kMaxPlanes) {
+		const int ze = z_hi - z > kMaxPlanes ? z + kMaxPlanes : z_hi;
+		const dim3 grid(kSlabChunks, (unsigned)(ze - z));
+		k_slab_sweep<MODE><<<grid, kSlabThreads, 0, s>>>(g, k, z, ze, a, chunk);
+	}
 }
 
 }  // namespace
