@@ -119,3 +119,34 @@ def test_server_and_autotune_argument_checks_without_device():
     timed_out = ctypes.c_int(0)
     assert lib.sedi_selftest_bounded_wait(0.0, ctypes.byref(timed_out), None) == -1
     assert lib.sedi_selftest_bounded_wait(10000.0, ctypes.byref(timed_out), None) == -1
+
+
+def test_slab_sweep_argument_checks_without_device():
+    """sedi_slab_sweep refuses bad modes, plane ranges, grids and missing
+    vectors before any device call; a dot mode needs its scratch buffers."""
+    from sedi_b200.domain import _SlabArgs, APPLY, CG_SP, SETUP
+    lib = sedi_b200.load()
+    vp, c_long, c_double, c_int = ctypes.c_void_p, ctypes.c_long, ctypes.c_double, ctypes.c_int
+    lib.sedi_slab_sweep.argtypes = [c_int, c_long, c_long, c_long, c_double, c_double, c_double, c_long, c_long,
+                                    ctypes.POINTER(_SlabArgs), vp, vp, vp]
+    fake = 0x1000  # never dereferenced: every call below fails its checks first
+    a = _SlabArgs()
+    a.src = a.y = fake
+
+    def call(mode, n1=8, n2=8, nloc=4, z_lo=1, z_hi=5, args=a, chunk=None, plane=None):
+        return lib.sedi_slab_sweep(mode, n1, n2, nloc, 6.0, 1.0, 1.0, z_lo, z_hi, ctypes.byref(args) if args else None,
+                                   chunk, plane, None)
+
+    assert call(13) == -1 and call(-1) == -1              # mode
+    assert call(APPLY, z_lo=0) == -1                      # ghost plane 0 is not swept
+    assert call(APPLY, z_hi=6) == -1                      # past plane nloc
+    assert call(APPLY, z_lo=3, z_hi=2) == -1
+    assert call(APPLY, n1=0) == -1 and call(APPLY, nloc=0) == -1
+    assert call(APPLY, args=None) == -1
+    assert call(SETUP) == -1                              # r and b missing
+    assert call(CG_SP) == -1                              # a dot mode without scratch
+    b = _SlabArgs()
+    b.src = fake
+    assert call(APPLY, args=b) == -1                      # y missing
+    assert call(APPLY, z_lo=3, z_hi=3) == 0               # empty range: nothing to launch
+    assert lib.sedi_slab_chunks() == 8
