@@ -144,10 +144,10 @@ def test_burst_of_fresh_contexts_matches_direct():
 
 
 def test_contexts_reused_across_sample_counts_of_one_padded_lane_count():
-    """Mixed jobs of 9, 20 and 30 probes on one grid all pad to 32 lanes: one
+    """Mixed jobs of 17, 20 and 30 probes on one grid all pad to 32 lanes: one
     context serves them one after another, and each result is bit-identical
     to the direct estimate on a context created for its own sample count."""
-    jobs = [("cg", (40, 36, 32), k, 50 + k, 2000, 1e-9, S.MIXED) for k in (9, 20, 30)]
+    jobs = [("cg", (40, 36, 32), k, 50 + k, 2000, 1e-9, S.MIXED) for k in (17, 20, 30)]
     with S.Server() as srv:
         got = []
         for job in jobs:
