@@ -561,11 +561,11 @@ def run_sweeps(S, args):
 def run_slab(S, args):
     """The slab (i3) decomposition on one GPU, P slabs in one process (halos
     by device copies), FP64, against the single-vector form on the same
-    probe: (1) each solver at 512^3, one probe, 200 fixed iterations (tol 0),
-    P = 1, 2, 4: GPoint-iterations/s of the solve alone (probe generation
-    outside the timed region) and the host time spent reading dot products;
-    (2) CG at 256^3 to tol 1e-9, P = 1 and 2: iteration counts and whether D
-    matches across P bit for bit."""
+    probe: (1) each solver at 512^3 (--grid), one probe, 200 fixed iterations
+    (--maxiter), P = 1, 2, 4: GPoint-iterations/s of the solve alone (probe
+    generation outside the timed region) and the host time spent reading dot
+    products; (2) unless --no-extras, CG at 256^3 to tol 1e-9, P = 1 and 2:
+    iteration counts and whether D matches across P bit for bit."""
     import numpy as np
     import torch
     from sedi_b200.domain import slab_solver
@@ -591,7 +591,8 @@ def run_slab(S, args):
         torch.cuda.empty_cache()
         return out
 
-    g = (512, 512, 512)
+    g = tuple(int(v) for v in args.grid.split("x")) if args.grid else (512, 512, 512)
+    iters = args.maxiter if args.maxiter else 200
     n = g[0] * g[1] * g[2]
     probe = torch.empty((1, n), dtype=torch.float64, device="cuda")
     S.fill_probes_dev(SEED, probe)
@@ -601,18 +602,21 @@ def run_slab(S, args):
             c.estimate_dev(1, probe, D, maxiter=5, tol=0.0)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            rp = c.estimate_dev(1, probe, D, maxiter=200, tol=0.0)
+            rp = c.estimate_dev(1, probe, D, maxiter=iters, tol=0.0)
             torch.cuda.synchronize()
             dtp = time.perf_counter() - t0
-        row = {"workload": f"slab decomposition on one GPU, {solver}, 512^3, 1 probe, 200 fixed iterations, FP64",
+        row = {"workload": f"slab decomposition on one GPU, {solver}, {g[0]}x{g[1]}x{g[2]}, 1 probe, {iters} fixed "
+                           f"iterations, FP64",
                "single_vector_gpoint_iterations_per_s": float(rp["iters"][0]) * n / dtp / 1e9, "slabs": []}
         for parts in (1, 2, 4):
-            it, dt, dots, err = solve_slabs(solver, g, parts, 200, 0.0)
+            it, dt, dots, err = solve_slabs(solver, g, parts, iters, 0.0)
             row["slabs"].append({"parts": parts, "gpoint_iterations_per_s": it * n / dt / 1e9, "s": dt,
                                  "dot_read_s": dots, "final_err": err})
         print(json.dumps(row), flush=True)
     del probe, D
     torch.cuda.empty_cache()
+    if args.no_extras:
+        return
     g = (256, 256, 256)
     with S.Context("cg", g) as c:
         rp = c.estimate(2, SEED, 5000, 1e-9)
