@@ -121,94 +121,101 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_sweep(SlabGeo g, Coef k, 
 #pragma unroll
 	for (int d = 0; d < ND; d++) v[d] = 0.0;
 	const double iM = a.iM;
-	const long long n_in = (long long)(r1 - r0) * g.n1;
-	for (long long t = threadIdx.x; t < n_in; t += kSlabThreads) {
-		const int i2 = r0 + (int)(t / g.n1), i1 = (int)(t % g.n1);
-		const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + i1;
-		double st = 0.0;
-		if (mode_stencil(MODE)) st = slab_stencil(g, k, a.src, mode_scaled(MODE), iM, z, i2, i1);
-		if (MODE == SLAB_SETUP) {
-			const double bi = a.b[i];
-			const double ri = add(bi, mul(-1.0, st));  // combine2(1.0, b, -1.0, Ax, r)
-			a.r[i] = ri;
-			v[0] = fma(bi, bi, v[0]);
-			v[1] = fma(ri, ri, v[1]);
-		} else if (MODE == SLAB_CG_SP) {
-			const double pi = a.src[i];
-			v[0] = fma(st, pi, v[0]);
-			if (a.first) {
+	// Rows of the chunk, each by tpr threads (the smallest power of two >= n1,
+	// at most the block), the block's other threads on the next rows; the row
+	// loop is unrolled so each thread has several rows' loads in flight.
+	int tpr = 32;
+	while (tpr < g.n1 && tpr < kSlabThreads) tpr <<= 1;
+	const int rpi = kSlabThreads / tpr, tc = (int)threadIdx.x % tpr;
+	for (int i1 = tc; i1 < g.n1; i1 += tpr) {
+#pragma unroll 4
+		for (int i2 = r0 + (int)threadIdx.x / tpr; i2 < r1; i2 += rpi) {
+			const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + i1;
+			double st = 0.0;
+			if (mode_stencil(MODE)) st = slab_stencil(g, k, a.src, mode_scaled(MODE), iM, z, i2, i1);
+			if (MODE == SLAB_SETUP) {
+				const double bi = a.b[i];
+				const double ri = add(bi, mul(-1.0, st));  // combine2(1.0, b, -1.0, Ax, r)
+				a.r[i] = ri;
+				v[0] = fma(bi, bi, v[0]);
+				v[1] = fma(ri, ri, v[1]);
+			} else if (MODE == SLAB_CG_SP) {
+				const double pi = a.src[i];
+				v[0] = fma(st, pi, v[0]);
+				if (a.first) {
+					const double ri = a.r[i];
+					v[1] = fma(ri, mul(ri, iM), v[1]);
+				}
+			} else if (MODE == SLAB_CG_UPDATE) {
+				const double pi = a.src[i];
+				a.x[i] = add(a.x[i], mul(a.alpha, pi));          // :169
+				const double ri = add(a.r[i], mul(-a.alpha, st));  // :172
+				a.r[i] = ri;
+				const double ui = mul(ri, iM);                     // :175
+				v[0] = fma(ri, ui, v[0]);
+				v[1] = fma(ri, ri, v[1]);
+			} else if (MODE == SLAB_APPLY) {
+				a.y[i] = st;
+			} else if (MODE == SLAB_PCG_SETUP) {
+				const double ri = a.src[i];
+				const double ui = mul(ri, iM);  // :138
+				a.u[i] = ui;
+				a.w[i] = st;                    // :141-143
+				a.q[i] = a.s[i] = a.p[i] = a.z[i] = 0.0;  // :146-149
+				v[0] = fma(ri, ui, v[0]);
+				v[1] = fma(st, ui, v[1]);
+				v[2] = fma(ri, ri, v[2]);
+			} else if (MODE == SLAB_PCG_ITER) {
+				const double wi = a.src[i];
+				const double mi = mul(wi, iM);                            // :158
+				const double qi = add(mi, mul(a.beta, a.q[i]));          // :200
+				const double si = add(wi, mul(a.beta, a.s[i]));          // :203
+				const double ui0 = a.u[i];
+				const double pi = add(ui0, mul(a.beta, a.p[i]));         // :206
+				const double zi = add(st, mul(a.beta, a.z[i]));          // :209
+				const double ri = add(a.r[i], mul(-a.alpha, si));        // :212
+				const double xi = add(a.x[i], mul(a.alpha, pi));         // :215
+				const double ui = add(ui0, mul(-a.alpha, qi));           // :218
+				const double wni = add(wi, mul(-a.alpha, zi));           // :221
+				a.q[i] = qi;
+				a.s[i] = si;
+				a.p[i] = pi;
+				a.z[i] = zi;
+				a.r[i] = ri;
+				a.x[i] = xi;
+				a.u[i] = ui;
+				a.wn[i] = wni;
+				v[0] = fma(ri, ui, v[0]);   // next <r,u>
+				v[1] = fma(wni, ui, v[1]);  // next <w,u>
+				v[2] = fma(ri, ri, v[2]);   // next <r,r>
+			} else if (MODE == SLAB_BICG_P) {
 				const double ri = a.r[i];
-				v[1] = fma(ri, mul(ri, iM), v[1]);
+				a.p[i] = a.first ? ri : add(add(ri, mul(a.beta, a.p[i])), mul(a.bo, a.v[i]));  // :168, :171
+			} else if (MODE == SLAB_BICG_V) {
+				a.v[i] = st;  // v = A p_hat (:178-180)
+				v[0] = fma(st, a.rhat[i], v[0]);
+			} else if (MODE == SLAB_BICG_S) {
+				a.s[i] = add(a.r[i], mul(-a.alpha, a.v[i]));  // :189
+			} else if (MODE == SLAB_BICG_T) {
+				const double si = a.src[i];
+				a.t[i] = st;  // t = A s_hat (:204-206)
+				v[0] = fma(si, si, v[0]);
+				v[1] = fma(st, si, v[1]);
+				v[2] = fma(st, st, v[2]);
+			} else if (MODE == SLAB_BICG_XR) {
+				const double si = a.s[i];
+				const double phi = mul(a.p[i], iM), shi = mul(si, iM);
+				a.x[i] = add(add(a.x[i], mul(a.alpha, phi)), mul(a.omega, shi));  // :216
+				const double ri = add(si, mul(-a.omega, a.t[i]));                   // :219
+				a.r[i] = ri;
+				v[0] = fma(ri, ri, v[0]);
+				v[1] = fma(ri, a.rhat[i], v[1]);
+			} else if (MODE == SLAB_BICG_X) {
+				a.x[i] = add(a.x[i], mul(a.alpha, mul(a.p[i], iM)));  // :196
+			} else {  // SLAB_CG_P
+				const double ui = mul(a.r[i], iM);
+				a.p[i] = a.first ? ui : add(ui, mul(a.beta, a.p[i]));
 			}
-		} else if (MODE == SLAB_CG_UPDATE) {
-			const double pi = a.src[i];
-			a.x[i] = add(a.x[i], mul(a.alpha, pi));          // :169
-			const double ri = add(a.r[i], mul(-a.alpha, st));  // :172
-			a.r[i] = ri;
-			const double ui = mul(ri, iM);                     // :175
-			v[0] = fma(ri, ui, v[0]);
-			v[1] = fma(ri, ri, v[1]);
-		} else if (MODE == SLAB_APPLY) {
-			a.y[i] = st;
-		} else if (MODE == SLAB_PCG_SETUP) {
-			const double ri = a.src[i];
-			const double ui = mul(ri, iM);  // :138
-			a.u[i] = ui;
-			a.w[i] = st;                    // :141-143
-			a.q[i] = a.s[i] = a.p[i] = a.z[i] = 0.0;  // :146-149
-			v[0] = fma(ri, ui, v[0]);
-			v[1] = fma(st, ui, v[1]);
-			v[2] = fma(ri, ri, v[2]);
-		} else if (MODE == SLAB_PCG_ITER) {
-			const double wi = a.src[i];
-			const double mi = mul(wi, iM);                            // :158
-			const double qi = add(mi, mul(a.beta, a.q[i]));          // :200
-			const double si = add(wi, mul(a.beta, a.s[i]));          // :203
-			const double ui0 = a.u[i];
-			const double pi = add(ui0, mul(a.beta, a.p[i]));         // :206
-			const double zi = add(st, mul(a.beta, a.z[i]));          // :209
-			const double ri = add(a.r[i], mul(-a.alpha, si));        // :212
-			const double xi = add(a.x[i], mul(a.alpha, pi));         // :215
-			const double ui = add(ui0, mul(-a.alpha, qi));           // :218
-			const double wni = add(wi, mul(-a.alpha, zi));           // :221
-			a.q[i] = qi;
-			a.s[i] = si;
-			a.p[i] = pi;
-			a.z[i] = zi;
-			a.r[i] = ri;
-			a.x[i] = xi;
-			a.u[i] = ui;
-			a.wn[i] = wni;
-			v[0] = fma(ri, ui, v[0]);   // next <r,u>
-			v[1] = fma(wni, ui, v[1]);  // next <w,u>
-			v[2] = fma(ri, ri, v[2]);   // next <r,r>
-		} else if (MODE == SLAB_BICG_P) {
-			const double ri = a.r[i];
-			a.p[i] = a.first ? ri : add(add(ri, mul(a.beta, a.p[i])), mul(a.bo, a.v[i]));  // :168, :171
-		} else if (MODE == SLAB_BICG_V) {
-			a.v[i] = st;  // v = A p_hat (:178-180)
-			v[0] = fma(st, a.rhat[i], v[0]);
-		} else if (MODE == SLAB_BICG_S) {
-			a.s[i] = add(a.r[i], mul(-a.alpha, a.v[i]));  // :189
-		} else if (MODE == SLAB_BICG_T) {
-			const double si = a.src[i];
-			a.t[i] = st;  // t = A s_hat (:204-206)
-			v[0] = fma(si, si, v[0]);
-			v[1] = fma(st, si, v[1]);
-			v[2] = fma(st, st, v[2]);
-		} else if (MODE == SLAB_BICG_XR) {
-			const double si = a.s[i];
-			const double phi = mul(a.p[i], iM), shi = mul(si, iM);
-			a.x[i] = add(add(a.x[i], mul(a.alpha, phi)), mul(a.omega, shi));  // :216
-			const double ri = add(si, mul(-a.omega, a.t[i]));                   // :219
-			a.r[i] = ri;
-			v[0] = fma(ri, ri, v[0]);
-			v[1] = fma(ri, a.rhat[i], v[1]);
-		} else if (MODE == SLAB_BICG_X) {
-			a.x[i] = add(a.x[i], mul(a.alpha, mul(a.p[i], iM)));  // :196
-		} else {  // SLAB_CG_P
-			const double ui = mul(a.r[i], iM);
-			a.p[i] = a.first ? ui : add(ui, mul(a.beta, a.p[i]));
 		}
 	}
 	if (mode_dots(MODE) == 0) return;
