@@ -122,13 +122,15 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_sweep(SlabGeo g, Coef k, 
 	for (int d = 0; d < ND; d++) v[d] = 0.0;
 	const double iM = a.iM;
 	// Rows of the chunk, each by tpr threads (the smallest power of two >= n1,
-	// at most the block), the block's other threads on the next rows; the row
-	// loop is unrolled so each thread has several rows' loads in flight.
+	// at most the block), the block's other threads on the next rows.  Not
+	// unrolled: these sweeps hide latency with resident warps, and unrolling
+	// by 4 cost more in occupancy (registers) than it gained (512^3 CG 55 ->
+	// 51, pipelined CG 46 -> 37 GPoint-it/s on B200).
 	int tpr = 32;
 	while (tpr < g.n1 && tpr < kSlabThreads) tpr <<= 1;
 	const int rpi = kSlabThreads / tpr, tc = (int)threadIdx.x % tpr;
 	for (int i1 = tc; i1 < g.n1; i1 += tpr) {
-#pragma unroll 4
+#pragma unroll 1
 		for (int i2 = r0 + (int)threadIdx.x / tpr; i2 < r1; i2 += rpi) {
 			const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + i1;
 			double st = 0.0;
