@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["sedi", "reference"], default="sedi")
-    ap.add_argument("--workload", choices=["batched256", "dropin", "large512", "accuracy", "sweeps", "slab"],
+    ap.add_argument("--workload", choices=["batched256", "dropin", "large512", "accuracy", "sweeps", "slab", "periods"],
                     default="batched256",
                     help="batched256: the benchmark line (256^3 x 128 probes, mixed CG); dropin: 128^3 x 64 "
                          "probes; large512: the 512^3 x 16-probe pipelined-CG configuration (one JSON line); "
@@ -636,6 +636,36 @@ def run_slab(S, args):
     print(json.dumps(row), flush=True)
 
 
+def run_periods(S, args):
+    """Reliable-update period of the mixed forms: BiCGStab and CG at 128^3 x
+    64 probes, tol 1e-9, periods 8 to 50.  Per period: mean iterations,
+    seconds per estimate, D error against the FP64 form on the same probes
+    and against the converged diagonal (FP64 CG to 1e-13).  One JSON line
+    per solver."""
+    g, k, tol = (128, 128, 128), 64, 1e-9
+
+    def est(solver, prec, period=0, t=tol):
+        S.set_tuning(solver, g, k, precision=prec, period=period)
+        with S.Context(solver, g, precision=prec, batch=k) as c:
+            c.estimate(k, SEED, 20, t, ignore_errors=True)  # graph capture
+            t0 = time.perf_counter()
+            r = c.estimate(k, SEED, 20000, t)
+            return r, time.perf_counter() - t0
+
+    ex, _ = est("cg", S.FP64, t=1e-13)
+    for solver in ("bicgstab", "cg"):
+        r64, dt64 = est(solver, S.FP64)
+        row = {"workload": f"reliable-update period, mixed {solver}, 128^3 x 64 probes, tol 1e-9",
+               "fp64": {"iterations": float(r64["iters"].mean()), "s": dt64,
+                        "vs_converged": _relmax(r64["D"], ex["D"])}, "mixed": []}
+        for period in (8, 12, 16, 24, 32, 50):
+            rm, dtm = est(solver, S.MIXED, period)
+            row["mixed"].append({"period": period, "iterations": float(rm["iters"].mean()), "s": dtm,
+                                 "vs_fp64": _relmax(rm["D"], r64["D"]), "vs_converged": _relmax(rm["D"], ex["D"])})
+        S.set_tuning(solver, g, k, precision=S.MIXED)
+        print(json.dumps(row), flush=True)
+
+
 def traffic_per_launch(kernel, grid, lanes):
     """DRAM bytes per launch of `kernel` at this size, from the committed ncu
     summary (profiles/ncu_traffic.txt lines '<kernel> <n1>x<n2>x<n3> <lanes>
@@ -667,7 +697,8 @@ def run_sedi(args):
 
     rank, world, local = dist_env()
     wl = args.wl
-    aux = {"large512": run_large512, "accuracy": run_accuracy, "sweeps": run_sweeps, "slab": run_slab}
+    aux = {"large512": run_large512, "accuracy": run_accuracy, "sweeps": run_sweeps, "slab": run_slab,
+           "periods": run_periods}
     if args.workload in aux:
         if rank == 0:
             aux[args.workload](S, args)
