@@ -372,9 +372,11 @@ def estimate(solver, dims, samples, seed=1234, maxiter=1000, tol=1e-4, ignore_er
 
 
 def autotune(solver, dims, batch, precision=MIXED, maxiter=5000, tol=1e-9, seed=1234, solve=True):
-    """Pick the batched form's launch choices for this shape by measurement
-    (sedi_autotune); contexts created afterwards use them.  Returns
-    {"slice_width", "z_chunks", "period", "chunk", "score_ms"}."""
+    """Pick the launch choices for this shape by measurement (sedi_autotune);
+    contexts created afterwards use them.  With precision FP64 and batch 1 it
+    tunes the single-vector streaming sweeps.  Returns {"slice_width",
+    "z_chunks", "period", "chunk", "prefetch_planes" (-1: the built-in
+    distance), "sweep_a_form" (narrow-sweep form 1, 2 or 3), "score_ms"}."""
     sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
     ch = np.zeros(6, np.int32)
     ms = ctypes.c_double(0.0)
@@ -389,7 +391,8 @@ def autotune(solver, dims, batch, precision=MIXED, maxiter=5000, tol=1e-9, seed=
 def set_tuning(solver, dims, batch, precision=MIXED, slice_width=0, z_chunks=0, period=0, chunk=0,
                prefetch_planes=-1, sweep_a_form=0):
     """Record launch choices for contexts of this shape without measuring
-    (sedi_set_tuning), e.g. an earlier autotune result."""
+    (sedi_set_tuning), e.g. an earlier autotune result.  0 (-1 for
+    prefetch_planes) keeps the built-in choice."""
     sid = SOLVER_IDS[solver] if isinstance(solver, str) else int(solver)
     ch = np.array([slice_width, z_chunks, period, chunk, prefetch_planes, sweep_a_form], np.int32)
     rc = load().sedi_set_tuning(sid, int(precision), int(batch), *[int(d) for d in dims], _ptr(ch))
