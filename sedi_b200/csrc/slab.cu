@@ -58,30 +58,6 @@ __device__ __forceinline__ double slab_stencil(const SlabGeo &g, const Coef &k, 
 	return stencil7(k, xc, xm1, xm2, xm3, xp1, xp2, xp3);
 }
 
-// The same stencil at columns i1 and i1+1 (i1 even, n1 even, src 16-byte
-// aligned): the centre, row and plane neighbours as 16-byte pairs, the
-// outer column neighbours as single values.  Same roundings as slab_stencil.
-__device__ __forceinline__ void slab_stencil2(const SlabGeo &g, const Coef &k, const double *__restrict__ src,
-                                              bool scaled, double scale, int z, int i2, int i1, double *y0,
-                                              double *y1) {
-	const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + i1;
-	const double2 zero = make_double2(0.0, 0.0);
-	auto f2 = [&](long long j) {
-		double2 v = __ldg(reinterpret_cast<const double2 *>(src + j));
-		if (scaled) v = make_double2(mul(v.x, scale), mul(v.y, scale));
-		return v;
-	};
-	auto f = [&](long long j) { return scaled ? mul(__ldg(src + j), scale) : __ldg(src + j); };
-	const double2 c = f2(i);
-	const double2 ym = i2 > 0 ? f2(i - g.n1) : zero;
-	const double2 yp = i2 < g.n2 - 1 ? f2(i + g.n1) : zero;
-	const double2 zm = f2(i - g.plane), zp = f2(i + g.plane);
-	const double xl = i1 > 0 ? f(i - 1) : 0.0;
-	const double xr = i1 + 2 < g.n1 ? f(i + 2) : 0.0;
-	*y0 = stencil7(k, c.x, xl, ym.x, zm.x, c.y, yp.x, zp.x);
-	*y1 = stencil7(k, c.y, c.x, ym.y, zm.y, xr, yp.y, zp.y);
-}
-
 // Block-level sum of ND values in a fixed tree; result in thread 0.
 template <int ND>
 __device__ __forceinline__ void block_total(double (&v)[ND]) {
@@ -145,117 +121,102 @@ __global__ void __launch_bounds__(kSlabThreads) k_slab_sweep(SlabGeo g, Coef k, 
 #pragma unroll
 	for (int d = 0; d < ND; d++) v[d] = 0.0;
 	const double iM = a.iM;
-	// Rows of the chunk, each by tpr threads (the smallest power of two >= the
-	// row's work items, at most the block), the block's other threads on the
-	// next rows.  A work item is a pair of columns whose stencil input is read
-	// with 16-byte loads when n1 is even and src is 16-byte aligned, else one
-	// column.
-	const bool pairs = g.n1 % 2 == 0 && reinterpret_cast<uintptr_t>(a.src) % 16 == 0;
-	const int items = pairs ? g.n1 / 2 : g.n1;
+	// Rows of the chunk, each by tpr threads (the smallest power of two >= n1,
+	// at most the block), the block's other threads on the next rows.  Not
+	// unrolled: these sweeps hide latency with resident warps, and unrolling
+	// by 4 cost more in occupancy (registers) than it gained (512^3 CG 55 ->
+	// 51, pipelined CG 46 -> 37 GPoint-it/s on B200).
 	int tpr = 32;
-	while (tpr < items && tpr < kSlabThreads) tpr <<= 1;
+	while (tpr < g.n1 && tpr < kSlabThreads) tpr <<= 1;
 	const int rpi = kSlabThreads / tpr, tc = (int)threadIdx.x % tpr;
-	// One point of the sweep: i its ghosted index, st the stencil there.
-	auto point = [&](long long i, double st) {
-		if (MODE == SLAB_SETUP) {
-			const double bi = a.b[i];
-			const double ri = add(bi, mul(-1.0, st));  // combine2(1.0, b, -1.0, Ax, r)
-			a.r[i] = ri;
-			v[0] = fma(bi, bi, v[0]);
-			v[1] = fma(ri, ri, v[1]);
-		} else if (MODE == SLAB_CG_SP) {
-			const double pi = a.src[i];
-			v[0] = fma(st, pi, v[0]);
-			if (a.first) {
-				const double ri = a.r[i];
-				v[1] = fma(ri, mul(ri, iM), v[1]);
-			}
-		} else if (MODE == SLAB_CG_UPDATE) {
-			const double pi = a.src[i];
-			a.x[i] = add(a.x[i], mul(a.alpha, pi));          // :169
-			const double ri = add(a.r[i], mul(-a.alpha, st));  // :172
-			a.r[i] = ri;
-			const double ui = mul(ri, iM);                     // :175
-			v[0] = fma(ri, ui, v[0]);
-			v[1] = fma(ri, ri, v[1]);
-		} else if (MODE == SLAB_APPLY) {
-			a.y[i] = st;
-		} else if (MODE == SLAB_PCG_SETUP) {
-			const double ri = a.src[i];
-			const double ui = mul(ri, iM);  // :138
-			a.u[i] = ui;
-			a.w[i] = st;                    // :141-143
-			a.q[i] = a.s[i] = a.p[i] = a.z[i] = 0.0;  // :146-149
-			v[0] = fma(ri, ui, v[0]);
-			v[1] = fma(st, ui, v[1]);
-			v[2] = fma(ri, ri, v[2]);
-		} else if (MODE == SLAB_PCG_ITER) {
-			const double wi = a.src[i];
-			const double mi = mul(wi, iM);                            // :158
-			const double qi = add(mi, mul(a.beta, a.q[i]));          // :200
-			const double si = add(wi, mul(a.beta, a.s[i]));          // :203
-			const double ui0 = a.u[i];
-			const double pi = add(ui0, mul(a.beta, a.p[i]));         // :206
-			const double zi = add(st, mul(a.beta, a.z[i]));          // :209
-			const double ri = add(a.r[i], mul(-a.alpha, si));        // :212
-			const double xi = add(a.x[i], mul(a.alpha, pi));         // :215
-			const double ui = add(ui0, mul(-a.alpha, qi));           // :218
-			const double wni = add(wi, mul(-a.alpha, zi));           // :221
-			a.q[i] = qi;
-			a.s[i] = si;
-			a.p[i] = pi;
-			a.z[i] = zi;
-			a.r[i] = ri;
-			a.x[i] = xi;
-			a.u[i] = ui;
-			a.wn[i] = wni;
-			v[0] = fma(ri, ui, v[0]);   // next <r,u>
-			v[1] = fma(wni, ui, v[1]);  // next <w,u>
-			v[2] = fma(ri, ri, v[2]);   // next <r,r>
-		} else if (MODE == SLAB_BICG_P) {
-			const double ri = a.r[i];
-			a.p[i] = a.first ? ri : add(add(ri, mul(a.beta, a.p[i])), mul(a.bo, a.v[i]));  // :168, :171
-		} else if (MODE == SLAB_BICG_V) {
-			a.v[i] = st;  // v = A p_hat (:178-180)
-			v[0] = fma(st, a.rhat[i], v[0]);
-		} else if (MODE == SLAB_BICG_S) {
-			a.s[i] = add(a.r[i], mul(-a.alpha, a.v[i]));  // :189
-		} else if (MODE == SLAB_BICG_T) {
-			const double si = a.src[i];
-			a.t[i] = st;  // t = A s_hat (:204-206)
-			v[0] = fma(si, si, v[0]);
-			v[1] = fma(st, si, v[1]);
-			v[2] = fma(st, st, v[2]);
-		} else if (MODE == SLAB_BICG_XR) {
-			const double si = a.s[i];
-			const double phi = mul(a.p[i], iM), shi = mul(si, iM);
-			a.x[i] = add(add(a.x[i], mul(a.alpha, phi)), mul(a.omega, shi));  // :216
-			const double ri = add(si, mul(-a.omega, a.t[i]));                   // :219
-			a.r[i] = ri;
-			v[0] = fma(ri, ri, v[0]);
-			v[1] = fma(ri, a.rhat[i], v[1]);
-		} else if (MODE == SLAB_BICG_X) {
-			a.x[i] = add(a.x[i], mul(a.alpha, mul(a.p[i], iM)));  // :196
-		} else {  // SLAB_CG_P
-			const double ui = mul(a.r[i], iM);
-			a.p[i] = a.first ? ui : add(ui, mul(a.beta, a.p[i]));
-		}
-	};
-	for (int w = tc; w < items; w += tpr) {
+	for (int i1 = tc; i1 < g.n1; i1 += tpr) {
 #pragma unroll 1
 		for (int i2 = r0 + (int)threadIdx.x / tpr; i2 < r1; i2 += rpi) {
-			if (pairs) {
-				const int i1 = 2 * w;
-				const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + i1;
-				double s0 = 0.0, s1 = 0.0;
-				if (mode_stencil(MODE)) slab_stencil2(g, k, a.src, mode_scaled(MODE), iM, z, i2, i1, &s0, &s1);
-				point(i, s0);
-				point(i + 1, s1);
-			} else {
-				const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + w;
-				double st = 0.0;
-				if (mode_stencil(MODE)) st = slab_stencil(g, k, a.src, mode_scaled(MODE), iM, z, i2, w);
-				point(i, st);
+			const long long i = (long long)z * g.plane + (long long)i2 * g.n1 + i1;
+			double st = 0.0;
+			if (mode_stencil(MODE)) st = slab_stencil(g, k, a.src, mode_scaled(MODE), iM, z, i2, i1);
+			if (MODE == SLAB_SETUP) {
+				const double bi = a.b[i];
+				const double ri = add(bi, mul(-1.0, st));  // combine2(1.0, b, -1.0, Ax, r)
+				a.r[i] = ri;
+				v[0] = fma(bi, bi, v[0]);
+				v[1] = fma(ri, ri, v[1]);
+			} else if (MODE == SLAB_CG_SP) {
+				const double pi = a.src[i];
+				v[0] = fma(st, pi, v[0]);
+				if (a.first) {
+					const double ri = a.r[i];
+					v[1] = fma(ri, mul(ri, iM), v[1]);
+				}
+			} else if (MODE == SLAB_CG_UPDATE) {
+				const double pi = a.src[i];
+				a.x[i] = add(a.x[i], mul(a.alpha, pi));          // :169
+				const double ri = add(a.r[i], mul(-a.alpha, st));  // :172
+				a.r[i] = ri;
+				const double ui = mul(ri, iM);                     // :175
+				v[0] = fma(ri, ui, v[0]);
+				v[1] = fma(ri, ri, v[1]);
+			} else if (MODE == SLAB_APPLY) {
+				a.y[i] = st;
+			} else if (MODE == SLAB_PCG_SETUP) {
+				const double ri = a.src[i];
+				const double ui = mul(ri, iM);  // :138
+				a.u[i] = ui;
+				a.w[i] = st;                    // :141-143
+				a.q[i] = a.s[i] = a.p[i] = a.z[i] = 0.0;  // :146-149
+				v[0] = fma(ri, ui, v[0]);
+				v[1] = fma(st, ui, v[1]);
+				v[2] = fma(ri, ri, v[2]);
+			} else if (MODE == SLAB_PCG_ITER) {
+				const double wi = a.src[i];
+				const double mi = mul(wi, iM);                            // :158
+				const double qi = add(mi, mul(a.beta, a.q[i]));          // :200
+				const double si = add(wi, mul(a.beta, a.s[i]));          // :203
+				const double ui0 = a.u[i];
+				const double pi = add(ui0, mul(a.beta, a.p[i]));         // :206
+				const double zi = add(st, mul(a.beta, a.z[i]));          // :209
+				const double ri = add(a.r[i], mul(-a.alpha, si));        // :212
+				const double xi = add(a.x[i], mul(a.alpha, pi));         // :215
+				const double ui = add(ui0, mul(-a.alpha, qi));           // :218
+				const double wni = add(wi, mul(-a.alpha, zi));           // :221
+				a.q[i] = qi;
+				a.s[i] = si;
+				a.p[i] = pi;
+				a.z[i] = zi;
+				a.r[i] = ri;
+				a.x[i] = xi;
+				a.u[i] = ui;
+				a.wn[i] = wni;
+				v[0] = fma(ri, ui, v[0]);   // next <r,u>
+				v[1] = fma(wni, ui, v[1]);  // next <w,u>
+				v[2] = fma(ri, ri, v[2]);   // next <r,r>
+			} else if (MODE == SLAB_BICG_P) {
+				const double ri = a.r[i];
+				a.p[i] = a.first ? ri : add(add(ri, mul(a.beta, a.p[i])), mul(a.bo, a.v[i]));  // :168, :171
+			} else if (MODE == SLAB_BICG_V) {
+				a.v[i] = st;  // v = A p_hat (:178-180)
+				v[0] = fma(st, a.rhat[i], v[0]);
+			} else if (MODE == SLAB_BICG_S) {
+				a.s[i] = add(a.r[i], mul(-a.alpha, a.v[i]));  // :189
+			} else if (MODE == SLAB_BICG_T) {
+				const double si = a.src[i];
+				a.t[i] = st;  // t = A s_hat (:204-206)
+				v[0] = fma(si, si, v[0]);
+				v[1] = fma(st, si, v[1]);
+				v[2] = fma(st, st, v[2]);
+			} else if (MODE == SLAB_BICG_XR) {
+				const double si = a.s[i];
+				const double phi = mul(a.p[i], iM), shi = mul(si, iM);
+				a.x[i] = add(add(a.x[i], mul(a.alpha, phi)), mul(a.omega, shi));  // :216
+				const double ri = add(si, mul(-a.omega, a.t[i]));                   // :219
+				a.r[i] = ri;
+				v[0] = fma(ri, ri, v[0]);
+				v[1] = fma(ri, a.rhat[i], v[1]);
+			} else if (MODE == SLAB_BICG_X) {
+				a.x[i] = add(a.x[i], mul(a.alpha, mul(a.p[i], iM)));  // :196
+			} else {  // SLAB_CG_P
+				const double ui = mul(a.r[i], iM);
+				a.p[i] = a.first ? ui : add(ui, mul(a.beta, a.p[i]));
 			}
 		}
 	}
