@@ -519,8 +519,7 @@ def run_accuracy(S, args):
 def run_sweeps(S, args):
     """Each streaming sweep alone (CUDA events, 10-20 launches after one)
     across the narrow-sweep forms (1 ring, 2 in place on 32x16 tiles with two
-    blocks per SM, 3 in place on 32x32 tiles with six stages, 4 for CG sweep
-    A a ring on 32x16 tiles) and L2 prefetch
+    blocks per SM, 3 in place on 32x32 tiles with six stages) and L2 prefetch
     distances: mixed CG and BiCGStab at 128^3 x 64 and 256^3 x 128 lanes,
     batched FP64 (CG, BiCGStab, pipelined CG) at 256^3 x 64 lanes (slice
     width 8 and 2), and the
@@ -537,7 +536,7 @@ def run_sweeps(S, args):
 
     for g, k in (((128, 128, 128), 64), ((256, 256, 256), 128)):
         for solver, pfs in (("cg", (0, 2)), ("bicgstab", (0,))):
-            for form in ((1, 2, 3, 4) if solver == "cg" else (1, 2, 3)):
+            for form in (1, 2, 3):
                 for pf in pfs:
                     S.set_tuning(solver, g, k, precision=S.MIXED, sweep_a_form=form, prefetch_planes=pf)
                     with S.Context(solver, g, precision=S.MIXED, batch=k) as c:
@@ -552,7 +551,7 @@ def run_sweeps(S, args):
                     row({"grid": list(g), "lanes": 64, "solver": solver, "form": "fp64", "sweep_form": form,
                          "slice_width": W, "config": c.config()}, c.time_kernels(reps=5))
     for solver in ("cg", "bicgstab", "pcg"):
-        for form in ((1, 2, 3, 4) if solver == "cg" else (1, 2, 3)):
+        for form in (1, 2, 3):
             S.set_tuning(solver, g, 1, precision=S.FP64, sweep_a_form=form, prefetch_planes=2)
             with S.Context(solver, g) as c:
                 row({"grid": list(g), "lanes": 1, "solver": solver, "form": "plain", "sweep_form": form,

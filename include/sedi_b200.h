@@ -343,8 +343,7 @@ int sedi_server_stats(const sedi_server *srv, double *peak_bytes, double *budget
  * (0, 2, 4 or 8), for CG and BiCGStab the form of the narrow sweeps (CG's
  * sweep A, BiCGStab's sweeps 2 and 3; 1: a ring of computed planes on 32x32
  * tiles; 2: in place, 32x16 tiles, two blocks per SM; 3: in place, 32x32
- * tiles, six stages; 4, CG only: a ring on 32x16 tiles), and with flags & 1
- * the iterations per
+ * tiles, six stages), and with flags & 1 the iterations per
  * captured graph and (mixed
  * precision) the reliable-update period in 20..50, the last two by timing a
  * real estimate of `batch` probes seeded `seed` to `tol`.  The choice is kept

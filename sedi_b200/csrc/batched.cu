@@ -741,15 +741,6 @@ struct InPlace : Op {
 template <class T, int K>
 using OpCgAv = InPlace<OpCgA<T>, K>;
 
-// A sweep on the tiles of another KIND, with its ring (CG sweep A form 4:
-// 32x16 tiles, five stages, the tile count of sweep B).
-template <class Op, int K>
-struct Tiled : Op {
-	static constexpr int KIND = K;
-	Tiled() = default;
-	explicit Tiled(const Op &o) : Op(o) {}
-};
-
 // ---------------------------------------------------------------------------
 // CG kernel B: s = A p, x += alpha p, r -= alpha s, u = r .* iM, <r,u>, <r,r>;
 // beta, err, stop test (Cg.hpp:169-193).
@@ -1444,8 +1435,7 @@ static bool make_map(CUtensorMap *m, void *base, int eb, const Geo &g, int R, in
 #define SEDI_STREAM_PFD -1
 #endif
 // Form of the narrow sweeps (CG sweep A, BiCGStab sweeps 2 and 3): 1 ring
-// (32x32), 2 in place (32x16, 2 blocks/SM), 3 in place (32x32, 6 stages),
-// 4 (CG sweep A only) ring on 32x16 tiles.
+// (32x32), 2 in place (32x16, 2 blocks/SM), 3 in place (32x32, 6 stages).
 // Defaults by measurement on B200 (kernels alone, fraction of measured HBM
 // bandwidth, 256^3): batched CG sweep A form 3 (mixed x 128 lanes 4.21 ms,
 // 95%, against 4.78 ms ring; FP64 2-lane slices 97% against 83%); BiCGStab
@@ -1803,7 +1793,7 @@ int batched_alloc(Ctx *c) {
 	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
 	B->tuned = tu;
 	if (tu.period > 0) B->period = tu.period;
-	B->acfg = tu.acfg >= 1 && tu.acfg <= 4 ? tu.acfg : default_form(B->ks, false);
+	B->acfg = tu.acfg >= 1 && tu.acfg <= 3 ? tu.acfg : default_form(B->ks, false);
 	B->theta = default_theta(B->ks);
 	if (tu.chunk > 0) B->chunk = tu.chunk;
 	shape(c->g, B->R, B->rbT, ebT, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
@@ -2016,7 +2006,6 @@ static void launch_cg_a(Ctx *c, Batched *B, const OpCgA<T> &a, cudaStream_t s) {
 	switch (B->acfg) {
 	case 2: launchT<T, RBT, PAIRS>(c, B, OpCgAv<T, 2>(a), s); break;
 	case 3: launchT<T, RBT, PAIRS>(c, B, OpCgAv<T, 3>(a), s); break;
-	case 4: launchT<T, RBT, PAIRS>(c, B, Tiled<OpCgA<T>, 0>(a), s); break;
 	default: launchT<T, RBT, PAIRS>(c, B, a, s);
 	}
 }
@@ -2325,7 +2314,7 @@ int pairs_alloc(Ctx *c) {
 	// batched context has that key) sets the i3 split, the prefetch distance
 	// and the narrow-sweep form.
 	const Tuning tu = tuning_for(TuneKey{c->solver, SEDI_PREC_FP64, pick_R(1, false), c->g.n1, c->g.n2, c->g.n3});
-	B->acfg = tu.acfg >= 1 && tu.acfg <= 4 ? tu.acfg : default_form(B->ks, true);
+	B->acfg = tu.acfg >= 1 && tu.acfg <= 3 ? tu.acfg : default_form(B->ks, true);
 	B->tuned = tu;
 	shape(g, 2, 2, 8, &B->gT, &B->gridT, tu.nz, 0, tu.pfd);
 	shape(g, 2, 2, 8, &B->gT1, &B->gridT1, tu.nz, 1, tu.pfd);
@@ -3021,8 +3010,7 @@ int batched_autotune(int solver, int precision, int batch, long long n1, long lo
 	// Form of CG's sweep A and BiCGStab's sweeps 2 and 3 (ring, or in place
 	// with two blocks per SM or six stages).
 	if (kernel_solver(solver, mixed) == SEDI_CG || kernel_solver(solver, mixed) == SEDI_BICGSTAB) {
-		const int forms = kernel_solver(solver, mixed) == SEDI_CG ? 4 : 3;  // form 4: CG sweep A only
-		for (int ac = 1; ac <= forms; ac++) {
+		for (int ac = 1; ac <= 3; ac++) {
 			Tuning t = best;
 			t.acfg = ac;
 			double ms = 0.0;
@@ -3103,7 +3091,7 @@ int batched_set_tuning(int solver, int precision, int batch, long long n1, long 
 	t.chunk = choice[3];
 	t.pfd = choice[4];
 	t.acfg = choice[5];
-	if (t.W < 0 || t.nz < 0 || t.period < 0 || t.chunk < 0 || t.pfd < -1 || t.pfd > 64 || t.acfg < 0 || t.acfg > 4 ||
+	if (t.W < 0 || t.nz < 0 || t.period < 0 || t.chunk < 0 || t.pfd < -1 || t.pfd > 64 || t.acfg < 0 || t.acfg > 3 ||
 	    (t.period > 0 && (t.period < 1 || t.period > 1000)) || t.chunk > 256)
 		return SEDI_ERR_ARG;
 	set_tuning(TuneKey{solver, precision, pick_R(batch, mixed), n1, n2, n3}, t);
