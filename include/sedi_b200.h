@@ -373,7 +373,7 @@ int sedi_set_tuning(int solver, int precision, int batch, long n1, long n2, long
  * In-loop stop target of the mixed-precision batched form (no counterpart in
  * the reference, whose FP64 method needs none).  A mixed lane leaves its loop
  * when its FP64 true residual sqrt(<b - A x, b - A x>/<b,b>) <= theta * tol,
- * 0 < theta <= 1; result codes and final_err are still judged against tol
+ * 0 < theta <= 1; result codes and final_err are still checked against tol
  * as the reference does (Cg.hpp:191-206), and the initial test stays
  * err < tol (Cg.hpp:130-134).  Two solutions that both meet tol differ by
  * the error each leaves behind the residual bound.  The FP32 CG iterates
