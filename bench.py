@@ -666,6 +666,13 @@ def run_periods(S, args):
         print(json.dumps(row), flush=True)
 
 
+def per_iteration(name, kern):
+    """Launches of a timed kernel per iteration: the mixed CG's second sweep
+    alternates between cg_b (odd iterations) and cg_bx (even ones)."""
+    deferred = any(k[0].startswith("cg_bx") for k in kern)
+    return 0.5 if deferred and name.startswith("cg_b") else 1.0
+
+
 def traffic_per_launch(kernel, grid, lanes):
     """DRAM bytes per launch of `kernel` at this size, from the committed ncu
     summary (profiles/ncu_traffic.txt lines '<kernel> <n1>x<n2>x<n3> <lanes>
@@ -823,7 +830,7 @@ def run_sedi(args):
         if kern:
             dom = max(kern, key=lambda k: k[1])
             ach = dom[2] / (dom[1] * 1e-3) / 1e9
-            it_ms = sum(k[1] for k in kern)
+            it_ms = sum(k[1] * per_iteration(k[0], kern) for k in kern)
             it_bytes = CG_BYTES[form] * n * SAMPLES
             roofline = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": peak, "unit": "GB/s",
                         "frac": ach / peak, "peak_source": peak_src,

@@ -52,6 +52,7 @@ struct LaneState {
 	double *bb, *rr, *err, *ru, *ru_new, *sp, *alpha, *beta;  // CG
 	double *gamma, *gamma_old, *delta, *rr_top;                 // pipelined CG
 	double *rho, *rho_prev, *omega, *s_norm2, *ts, *tt;         // BiCGStab
+	double *xa;  // mixed CG: alpha of the x step an odd iteration leaves to the next even one
 	int *done, *exit_iter, *reason, *pending, *s_exit;
 	double *hist;  // single-vector form: err after each iteration (lane 0), else null
 };
@@ -60,7 +61,7 @@ struct LaneState {
 // and carries the same scalars.
 __device__ __forceinline__ void mirror_lane0(const LaneState &ls) {
 	double *const d[] = {ls.bb, ls.rr, ls.err, ls.ru, ls.ru_new, ls.sp, ls.alpha, ls.beta, ls.gamma, ls.gamma_old,
-	                     ls.delta, ls.rr_top, ls.rho, ls.rho_prev, ls.omega, ls.s_norm2, ls.ts, ls.tt};
+	                     ls.delta, ls.rr_top, ls.rho, ls.rho_prev, ls.omega, ls.s_norm2, ls.ts, ls.tt, ls.xa};
 	for (double *a : d) a[1] = a[0];
 	int *const n[] = {ls.done, ls.exit_iter, ls.reason, ls.pending, ls.s_exit};
 	for (int *a : n) a[1] = a[0];
@@ -77,6 +78,7 @@ struct Global {
 	int err;        // a bounded wait timed out
 	int ru_all;     // the pending reliable update covers every lane (periodic)
 	double tol_in;  // in-loop stop target: tol (FP64 form), theta * tol (mixed lanes)
+	int b_iter;     // iteration of the last CG sweep A (gates the parity forms of sweep B)
 };
 
 // Arithmetic: FP64 keeps the reference's operator-by-operator rounding (no
@@ -126,7 +128,7 @@ __device__ __forceinline__ void dacc(double &acc, T a, T b) {
 // Map slots (Maps::m) for the per-type descriptor sets.
 enum {
 	MT_R_HALO = 0, MT_P0_HALO, MT_P1_HALO, MT_X_INT, MT_R_INT, MT_W0_HALO, MT_W1_HALO, MT_Q_HALO,
-	MT_R1_HALO, MT_V0_HALO, MT_V1_HALO
+	MT_R1_HALO, MT_V0_HALO, MT_V1_HALO, MT_P1_INT
 };  // fields of type T
 enum { MD_X_HALO = 0, MD_B_INT };                                     // FP64 fields
 
@@ -478,6 +480,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) k_stream(SGeo g, const __
 	}
 	__syncthreads();
 	if (t == 0) {
+		op.after(gl);
 		// The sweep that ends an iteration advances the counter unless a
 		// reliable update is due (it advances it after the update).
 		if (Op::ADVANCE && gl->active != 0 && gl->ru_due == 0) gl->iter += 1;
@@ -500,6 +503,7 @@ struct OpBase {
 	T ka, kb, kc;
 	__device__ void gload(long long, Vec<T> *) const {}
 	__device__ bool enabled(const Global *) const { return true; }
+	__device__ void after(Global *) const {}  // last block, after every lane's fin
 	__device__ bool slice_live(const Global *, const LaneState &, int, int) const { return true; }
 };
 
@@ -575,6 +579,7 @@ struct OpResid : OpBase<double> {
 		if (ru) {
 			if (ls.done[lane]) return;
 			if (!pcg && !gl->ru_all && !ls.pending[lane]) return;  // not part of this update
+			ls.xa[lane] = 0.0;  // a deferred x step was folded into x_hi
 			// The FP32 recurrence's <r,r> before the replacement: when it sits
 			// far below the true one (squared norms 1e-6 apart: the recurrence
 			// converged in FP32 arithmetic, as small systems do exactly), its
@@ -626,6 +631,7 @@ struct OpResid : OpBase<double> {
 		ls.pending[lane] = 0;
 		ls.gamma[lane] = 0.0;
 		ls.gamma_old[lane] = 0.0;
+		ls.xa[lane] = 0.0;
 		int done = 0, reason = STOP_NONE, ex = 0;
 		if (lane >= gl->nrhs) {
 			done = 1;
@@ -700,6 +706,7 @@ struct OpCgA : OpBase<T> {
 			for (int e = 0; e < V; e++) dacc(part[1][e], rc[0].v[e], amul(rc[0].v[e], iMc));
 		}
 	}
+	__device__ void after(Global *gl) const { gl->b_iter = gl->iter; }
 	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
 		if (ls.done[lane]) {
 			ls.alpha[lane] = 0.0;
@@ -744,10 +751,20 @@ using OpCgAv = InPlace<OpCgA<T>, K>;
 // ---------------------------------------------------------------------------
 // CG kernel B: s = A p, x += alpha p, r -= alpha s, u = r .* iM, <r,u>, <r,r>;
 // beta, err, stop test (Cg.hpp:169-193).
+// XS (mixed form only) defers x: XS_R runs on odd iterations and updates r
+// alone, leaving its x step (alpha in xa) to XS_X on the next even
+// iteration, which applies both, x = (x + xa p_old) + alpha p, with p_old
+// the previous iteration's direction (still in the other p buffer).  Two
+// iterations move 3 + 6 instead of 5 + 5 words per point and lane; r, the
+// scalars and every iteration count are those of the undeferred sweep, and
+// a reliable update after an odd iteration folds the pending step.
 // ---------------------------------------------------------------------------
-template <class T>
+enum { XS_EVERY = 0, XS_R = 1, XS_X = 2 };
+template <class T, int XS = XS_EVERY>
 struct OpCgB : OpBase<T> {
-	static constexpr int NS = 1, NQ = 2, ND = 2;
+	// XS_R streams two words like sweep A and takes its 32x32 tiles (KIND 1).
+	static constexpr int KIND = XS == XS_R ? 1 : 0;
+	static constexpr int NS = 1, NQ = XS == XS_EVERY ? 2 : (XS == XS_R ? 1 : 3), ND = 2;
 	static constexpr bool IDENT = true, USES_RAW_CENTER = false, ADVANCE = true;
 	static constexpr int V = Vec<T>::V;
 	T iMc;
@@ -755,30 +772,45 @@ struct OpCgB : OpBase<T> {
 	int mixed;
 	int it;
 	T alpha[V];
+	T xap[V];  // XS_X: the odd iteration's deferred alpha
+	// The parity forms run once per sweep A: the one that ran advances the
+	// iteration, so the other sees b_iter != iter and leaves.
+	__device__ bool enabled(const Global *gl) const {
+		return XS == XS_EVERY || (gl->b_iter == gl->iter && (gl->iter & 1) == (XS == XS_R ? 1 : 0));
+	}
 	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
 		it = gl->iter;
 #pragma unroll
-		for (int e = 0; e < V; e++) alpha[e] = (T)ls.alpha[lane + e];
+		for (int e = 0; e < V; e++) {
+			alpha[e] = (T)ls.alpha[lane + e];
+			xap[e] = XS == XS_X ? (T)ls.xa[lane + e] : T(0);
+		}
 	}
 	__device__ int src_map(int) const { return (it & 1) ? MT_P1_HALO : MT_P0_HALO; }
-	__device__ int q_map(int q) const { return q == 0 ? MT_X_INT : MT_R_INT; }
+	__device__ int q_map(int q) const {
+		if (XS == XS_R) return MT_R_INT;
+		return q == 0 ? MT_X_INT : (q == 1 ? MT_R_INT : MT_P1_INT);  // XS_X: p_old of an odd iteration is P1
+	}
 	__device__ bool raw_center() const { return false; }
 	__device__ Vec<T> src(const Vec<T> *raw) const { return raw[0]; }
 	__device__ void out(long long o, long long, int, const Vec<T> &pc, const Vec<T> &s, const Vec<T> *q,
 	                    const Vec<T> *, const Vec<T> *gv, double (&part)[ND][V]) const {
-		Vec<T> xv = q[0], rv = q[1];
+		Vec<T> xv, rv = q[XS == XS_R ? 0 : 1];
+		if (XS != XS_R) xv = q[0];
 #pragma unroll
 		for (int e = 0; e < V; e++) {
-			xv.v[e] = aadd(xv.v[e], amul(alpha[e], pc.v[e]));  // :169
+			if (XS == XS_X) xv.v[e] = aadd(xv.v[e], amul(xap[e], q[2].v[e]));
+			if (XS != XS_R) xv.v[e] = aadd(xv.v[e], amul(alpha[e], pc.v[e]));  // :169
 			rv.v[e] = aadd(rv.v[e], amul(-alpha[e], s.v[e]));  // :172
 			const T u = amul(rv.v[e], iMc);                                // :175
 			dacc(part[0][e], rv.v[e], u);
 			dacc(part[1][e], rv.v[e], rv.v[e]);
 		}
-		stg(x + o, xv);
+		if (XS != XS_R) stg(x + o, xv);
 		stg(r + o, rv);
 	}
 	__device__ void fin(int lane, const double *tot, Global *gl, const LaneState &ls) const {
+		if (XS == XS_R) ls.xa[lane] = ls.alpha[lane];  // this iteration's x step, applied by the next
 		if (ls.done[lane]) return;
 		ls.ru_new[lane] = tot[0];
 		ls.rr[lane] = tot[1];
@@ -1303,12 +1335,17 @@ __global__ void kb_ru_done(Global *gl) {
 // Reliable update (MIXED): x_hi += x_lo, x_lo = 0.  x_hi uses FP64 slices
 // of width WD, x_lo FP32 slices of width WT.  An update triggered by single
 // lanes (convergence claims, maxiter, breakdowns) folds only those lanes;
-// a periodic one (or any pipelined-CG one) folds every lane.
+// a periodic one (or any pipelined-CG one) folds every lane.  With CG's
+// deferred x step (p_odd non-null) an update after an odd iteration also
+// adds that iteration's step xa * p (its direction is in p_odd); the
+// residual sweep that follows clears xa of the folded lanes.
 __global__ void __launch_bounds__(256) kb_ru_fold(long long npts, int R, int WD, int WT, double *__restrict__ xh,
-                                                  float *__restrict__ xl, const int *__restrict__ pending, int all,
-                                                  Global *gl) {
+                                                  float *__restrict__ xl, const float *__restrict__ p_odd,
+                                                  const double *__restrict__ xa, const int *__restrict__ pending,
+                                                  int all, Global *gl) {
 	if (gl->active == 0 || gl->ru_due == 0) return;
 	all = all || gl->ru_all;
+	const bool step = p_odd != nullptr && (gl->iter & 1);
 	const long long pairs = npts * R / 2;
 	for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < pairs;
 	     u += (long long)gridDim.x * blockDim.x) {
@@ -1317,12 +1354,21 @@ __global__ void __launch_bounds__(256) kb_ru_fold(long long npts, int R, int WD,
 		const long long rem = od - sd * WD * npts;
 		const long long i = rem / WD;
 		const int j = (int)(sd * WD + rem % WD);
-		if (!all && !pending[j] && !pending[j + 1]) continue;  // lanes j, j+1 share the pair
+		const bool f0 = all || pending[j], f1 = all || pending[j + 1];  // lanes j, j+1 share the pair
+		if (!f0 && !f1) continue;
+		// Both lanes of the pair fold x_lo (x_hi + x_lo is unchanged for a
+		// lane outside the update); only the lanes in the update take their
+		// pending x step.
 		const long long ot = sliced(i, j, WT, npts);
 		const float2 lo = *reinterpret_cast<const float2 *>(xl + ot);
 		double2 hi = *reinterpret_cast<double2 *>(xh + od);
 		hi.x += (double)lo.x;
 		hi.y += (double)lo.y;
+		if (step) {
+			const float2 pv = *reinterpret_cast<const float2 *>(p_odd + ot);
+			if (f0) hi.x += xa[j] * (double)pv.x;
+			if (f1) hi.y += xa[j + 1] * (double)pv.y;
+		}
 		*reinterpret_cast<double2 *>(xh + od) = hi;
 		*reinterpret_cast<float2 *>(xl + ot) = make_float2(0.f, 0.f);
 	}
@@ -1480,13 +1526,17 @@ static void set_tuning(const TuneKey &k, const Tuning &t) {
 	g_tune[k] = t;
 }
 
-constexpr int kLaneDoubles = 18, kLaneInts = 5;  // LaneState arrays
+constexpr int kLaneDoubles = 19, kLaneInts = 5;  // LaneState arrays
 
 #ifndef SEDI_MIXED_THETA_CG
 #define SEDI_MIXED_THETA_CG 1.0
 #endif
 #ifndef SEDI_MIXED_THETA_PCG
 #define SEDI_MIXED_THETA_PCG 1.0
+#endif
+// Mixed CG defers the x step of odd iterations to the next even one (OpCgB).
+#ifndef SEDI_MIXED_DEFER_X
+#define SEDI_MIXED_DEFER_X 1
 #endif
 #ifndef SEDI_MIXED_THETA_BICGSTAB
 #define SEDI_MIXED_THETA_BICGSTAB 0.1
@@ -1516,6 +1566,7 @@ struct Batched {
 	int R = 0;
 	bool mixed = false;  // FP32 Krylov fields, FP64 x_hi, reductions and reliable update
 	bool pairs = false;  // single-vector FP64 form: lanes 0/1 = even/odd i1 points of one vector
+	bool defer_x = false;  // mixed CG: x steps of odd iterations deferred to the next even one (OpCgB XS)
 	int acfg = SEDI_NARROW_FORM;  // form of the narrow sweeps (see CfgFor, InPlace, default_form)
 	int ks = 0;          // solver whose sweeps run (the mixed pipelined CG runs the CG recurrence)
 	bool aliased = false;  // the Krylov fields belong to the context (single-vector form)
@@ -1776,6 +1827,7 @@ int batched_alloc(Ctx *c) {
 	c->batched = B;
 	B->mixed = c->precision == SEDI_PREC_MIXED;
 	B->ks = kernel_solver(c->solver, B->mixed);
+	B->defer_x = SEDI_MIXED_DEFER_X && B->mixed && B->ks == SEDI_CG;
 	if (c->batch > (B->mixed ? 256 : 128)) {
 		c->error = "batch too large for one context (max 256 FP32 / 128 FP64 right-hand sides)";
 		return SEDI_ERR_ARG;
@@ -1850,7 +1902,7 @@ int batched_alloc(Ctx *c) {
 	LaneState &ls = B->ls;
 	double **dp[] = {&ls.bb, &ls.rr, &ls.err, &ls.ru, &ls.ru_new, &ls.sp, &ls.alpha, &ls.beta, &ls.gamma,
 	                 &ls.gamma_old, &ls.delta, &ls.rr_top, &ls.rho, &ls.rho_prev, &ls.omega, &ls.s_norm2, &ls.ts,
-	                 &ls.tt};
+	                 &ls.tt, &ls.xa};
 	static_assert(sizeof(dp) / sizeof(dp[0]) == kLaneDoubles, "lane arrays");
 	for (size_t i = 0; i < sizeof(dp) / sizeof(dp[0]); i++) *dp[i] = B->lane_mem + i * R;
 	int **ip[] = {&ls.done, &ls.exit_iter, &ls.reason, &ls.pending, &ls.s_exit};
@@ -1864,7 +1916,8 @@ int batched_alloc(Ctx *c) {
 		         make_map(&M.m[MT_P0_HALO], B->p0, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_P1_HALO], B->p1, ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_X_INT], B->x, ebT, c->g, R, B->rbT, Q1, Q2) &&
-		         make_map(&M.m[MT_R_INT], B->r, ebT, c->g, R, B->rbT, Q1, Q2);
+		         make_map(&M.m[MT_R_INT], B->r, ebT, c->g, R, B->rbT, Q1, Q2) &&
+		         make_map(&M.m[MT_P1_INT], B->p1, ebT, c->g, R, B->rbT, Q1, Q2);
 		if (B->ks == 3)
 			k = k && make_map(&M.m[MT_W0_HALO], B->w[0], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_W1_HALO], B->w[1], ebT, c->g, R, B->rbT, Q1 + 2, Q2 + 2) &&
@@ -2010,6 +2063,19 @@ static void launch_cg_a(Ctx *c, Batched *B, const OpCgA<T> &a, cudaStream_t s) {
 	}
 }
 
+template <int XS, class T>
+static OpCgB<T, XS> cg_b_as(const OpCgB<T> &o) {
+	OpCgB<T, XS> d;
+	d.ka = o.ka;
+	d.kb = o.kb;
+	d.kc = o.kc;
+	d.iMc = o.iMc;
+	d.x = o.x;
+	d.r = o.r;
+	d.mixed = o.mixed;
+	return d;
+}
+
 template <class T, int RBT, int RBD, bool PAIRS = false>
 static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	cudaStream_t s = c->stream;
@@ -2030,12 +2096,18 @@ static void enqueue_cg_iteration(Ctx *c, Batched *B) {
 	bo.x = (T *)B->x;
 	bo.r = (T *)B->r;
 	bo.mixed = B->mixed ? 1 : 0;
-	launchT<T, RBT, PAIRS>(c, B, bo, s);
+	if (B->defer_x) {
+		// Both are captured; each runs only on its iteration parity.
+		launchT<T, RBT, PAIRS>(c, B, cg_b_as<XS_R>(bo), s);
+		launchT<T, RBT, PAIRS>(c, B, cg_b_as<XS_X>(bo), s);
+	} else {
+		launchT<T, RBT, PAIRS>(c, B, bo, s);
+	}
 	if (B->mixed) {
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
-		                                                                 (float *)B->x, B->ls.pending,
-		                                                                 B->ks == 3 ? 1 : 0, B->gl);
+		                                                                 (float *)B->x, B->defer_x ? (const float *)B->p1 : nullptr,
+		                                                                 B->ls.xa, B->ls.pending, B->ks == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD, PAIRS>(c, B, true);
 		kb_ru_done<<<1, 1, 0, s>>>(B->gl);
@@ -2087,7 +2159,7 @@ static void enqueue_pcg_iteration(Ctx *c, Batched *B) {
 		// w = A u and the next iteration's dots.
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
-		                                                                 (float *)B->x, B->ls.pending,
+		                                                                 (float *)B->x, nullptr, B->ls.xa, B->ls.pending,
 		                                                                 B->ks == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD, PAIRS>(c, B, true);
@@ -2175,7 +2247,7 @@ static void enqueue_bicg_iteration(Ctx *c, Batched *B) {
 		// the next iteration reads; rho = <r, r_hat> (restarted lanes: r_hat = r).
 		const long long nb = ((long long)B->elems / 2 + 255) / 256;
 		kb_ru_fold<<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(c->g.n, B->R, B->rbD, B->rbT, B->xh,
-		                                                                 (float *)B->x, B->ls.pending,
+		                                                                 (float *)B->x, nullptr, B->ls.xa, B->ls.pending,
 		                                                                 B->ks == 3 ? 1 : 0, B->gl);
 		c->launches++;
 		enqueue_resid<RBD, PAIRS>(c, B, true);
@@ -2340,7 +2412,7 @@ int pairs_alloc(Ctx *c) {
 	LaneState &ls = B->ls;
 	double **dp[] = {&ls.bb, &ls.rr, &ls.err, &ls.ru, &ls.ru_new, &ls.sp, &ls.alpha, &ls.beta, &ls.gamma,
 	                 &ls.gamma_old, &ls.delta, &ls.rr_top, &ls.rho, &ls.rho_prev, &ls.omega, &ls.s_norm2, &ls.ts,
-	                 &ls.tt};
+	                 &ls.tt, &ls.xa};
 	for (size_t i = 0; i < sizeof(dp) / sizeof(dp[0]); i++) *dp[i] = B->lane_mem + i * B->R;
 	int **ip[] = {&ls.done, &ls.exit_iter, &ls.reason, &ls.pending, &ls.s_exit};
 	for (size_t i = 0; i < 5; i++) *ip[i] = B->lane_int + i * B->R;
@@ -2676,22 +2748,37 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		BTRY(cudaGetLastError());
 		return 0;
 	}
-	for (int k = 0; k < 2; k++) {
-		if (k == 0) launch_cg_a<T, RBT, PAIRS>(c, B, a, s);
-		else launchT<T, RBT, PAIRS>(c, B, bo, s);
-		BTRY(cudaEventRecord(e0, s));
-		for (int i = 0; i < reps; i++) {
-			if (k == 0) launch_cg_a<T, RBT, PAIRS>(c, B, a, s);
-			else launchT<T, RBT, PAIRS>(c, B, bo, s);
+	// With the deferred x step, sweep B runs as cg_b (odd iterations: r only)
+	// and cg_bx (even: both x steps); each is timed on its own parity.
+	const int nk = B->defer_x ? 3 : 2;
+	for (int k = 0; k < nk; k++) {
+		if (B->defer_x) {
+			// Each form on its own parity; ru_due holds the counter (no advance).
+			g.iter = g.b_iter = k == 1 ? 3 : 2;
+			g.ru_due = 1;
+			*B->gl_host = g;
+			BTRY(cudaMemcpyAsync(B->gl, B->gl_host, sizeof(Global), cudaMemcpyHostToDevice, s));
 		}
+		auto one = [&]() {
+			if (k == 0) launch_cg_a<T, RBT, PAIRS>(c, B, a, s);
+			else if (!B->defer_x) launchT<T, RBT, PAIRS>(c, B, bo, s);
+			else if (k == 1) launchT<T, RBT, PAIRS>(c, B, cg_b_as<XS_R>(bo), s);
+			else launchT<T, RBT, PAIRS>(c, B, cg_b_as<XS_X>(bo), s);
+		};
+		one();
+		BTRY(cudaEventRecord(e0, s));
+		for (int i = 0; i < reps; i++) one();
 		BTRY(cudaEventRecord(e1, s));
 		BTRY(cudaEventSynchronize(e1));
 		float t = 0.f;
 		BTRY(cudaEventElapsedTime(&t, e0, e1));
 		ms[k] = (double)t / reps;
-		bytes[k] = (k == 0 ? 3.0 : 5.0) * ts;  // A: r, p_old in, p out; B: p, x, r in, x, r out
-		snprintf(names + 32 * k, 32, "%s%s", k == 0 ? (B->mixed ? "cg_a_fp32" : "cg_a_fp64")
-		                                             : (B->mixed ? "cg_b_fp32" : "cg_b_fp64"), PAIRS ? "_sv" : "");
+		// A: r, p_old in, p out; B: p, x, r in, x, r out; deferred: cg_b p, r in, r out,
+		// cg_bx p, p_old, x, r in, x, r out.
+		const double words = k == 0 ? 3.0 : (!B->defer_x ? 5.0 : (k == 1 ? 3.0 : 6.0));
+		bytes[k] = words * ts;
+		const char *nm = k == 0 ? "cg_a" : (k == 1 ? "cg_b" : "cg_bx");
+		snprintf(names + 32 * k, 32, "%s_%s%s", nm, B->mixed ? "fp32" : "fp64", PAIRS ? "_sv" : "");
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
@@ -2701,7 +2788,7 @@ static int time_cg_kernels(Ctx *c, Batched *B, int reps, double *ms, double *byt
 		c->error = "batched sweep timed out waiting for its data";
 		return SEDI_ERR_CUDA;
 	}
-	*count = 2;
+	*count = nk;
 	return 0;
 }
 

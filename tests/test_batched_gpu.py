@@ -291,14 +291,43 @@ def test_mixed_estimator_within_1e8_of_fp64_256cube(solver):
     assert O.relmax(rm["D"], r64["D"]) <= 1e-8, O.relmax(rm["D"], r64["D"])
 
 
-@pytest.mark.parametrize("solver,prec,nk", [("cg", S.MIXED, 2), ("pcg", S.MIXED, 2), ("bicgstab", S.MIXED, 3),
-                                            ("pcg", S.FP64, 1)])
+@pytest.mark.parametrize("period", [7, 32])
+def test_mixed_cg_deferred_x_steps_with_odd_updates(period):
+    """The mixed CG applies the x step of an odd iteration together with the
+    next even one's; a reliable update after an odd iteration (period 7:
+    every other update; lane-triggered ones at any iteration) folds the
+    pending step into x_hi.  A lost or doubled step would show as a true
+    residual off the recurrence and extra iterations: the iteration counts
+    stay within one of the FP64 form's and D within 1e-8 of it."""
+    dims, samples = (48, 48, 48), 16
+    with S.Context("cg", dims, batch=samples) as c64:
+        r64 = c64.estimate(samples, 99, 5000, 1e-9)
+    S.set_tuning("cg", dims, samples, precision=S.MIXED, period=period)
+    try:
+        with S.Context("cg", dims, precision=S.MIXED, batch=samples) as cm:
+            assert cm.config()["period"] == period
+            rm = cm.estimate(samples, 99, 5000, 1e-9)
+    finally:
+        S.set_tuning("cg", dims, samples, precision=S.MIXED)
+    assert np.all(rm["results"] == 0) and np.all(r64["results"] == 0)
+    assert np.abs(rm["iters"] - r64["iters"]).max() <= 1, (rm["iters"], r64["iters"])
+    assert O.relmax(rm["D"], r64["D"]) <= 1e-8, O.relmax(rm["D"], r64["D"])
+
+
+@pytest.mark.parametrize("solver,prec,nk", [("cg", S.MIXED, 3), ("pcg", S.MIXED, 3), ("bicgstab", S.MIXED, 3),
+                                            ("pcg", S.FP64, 1), ("cg", S.FP64, 2)])
 def test_time_kernels_lists_solver_sweeps(solver, prec, nk):
-    """Per-iteration sweeps: CG 2, BiCGStab 3, pipelined CG 1 in FP64 (its
-    mixed form runs the CG recurrence: 2)."""
+    """Per-iteration sweeps: CG 2 in FP64, BiCGStab 3, pipelined CG 1 in FP64.
+    The mixed CG (and the mixed pipelined CG, which runs the CG recurrence)
+    lists sweep A and the two parity forms of sweep B: cg_b on odd
+    iterations (r only, 3 words) and cg_bx on even ones (both x steps, 6)."""
     with S.Context(solver, (64, 64, 64), precision=prec, batch=16) as c:
         ks = c.time_kernels(reps=2)
     assert len(ks) == nk and all(ms > 0 and by > 0 for _, ms, by in ks)
+    if prec == S.MIXED and solver != "bicgstab":
+        names = [k[0] for k in ks]
+        assert names == ["cg_a_fp32", "cg_b_fp32", "cg_bx_fp32"], names
+        assert ks[2][2] == 2 * ks[1][2] == 2 * ks[0][2]
 
 
 @pytest.mark.parametrize("solver,prec", [("cg", S.FP64), ("cg", S.MIXED), ("pcg", S.MIXED), ("bicgstab", S.FP64)])
