@@ -1680,7 +1680,7 @@ static int pick_R(int nrhs, bool mixed) {
 
 // Lanes per slice: FP32 Krylov fields 4 (16 B per point); FP64 Krylov fields
 // of CG and BiCGStab 2 (16 B per point), of pipelined CG 8 (64 B per point);
-// the FP64 x and b of the mixed form 8.  16 B per point gets the 32x32 tiles
+// the FP64 x and b of the mixed form 2 (mixed_slice_fp64).  16 B per point gets the 32x32 tiles
 // and deep stage rings of the narrow sweeps.  Measured on B200 (kernels
 // alone, 64 lanes): FP64 CG sweep A at 256^3 4.11 ms with 2 lanes against
 // 5.83 ms with 8, BiCGStab sweep 2 3.98 against 5.20 ms, sweep 3 10.79
@@ -1698,6 +1698,13 @@ static int slice_for(int R, bool fp64, int ks = 0) {
 	                    : ((ks == SEDI_CG || ks == SEDI_BICGSTAB) ? SEDI_SLICE_LANES_FP64_NARROW : kSliceLanes);
 	return R >= w ? w : R;
 }
+
+// FP64 fields of the mixed form (x_hi, b), streamed by the setup and
+// reliable-update residual sweep: 2-lane slices (16 B per point: 32x16
+// tiles, six stages), like the FP64 CG sweeps.  With 8-lane slices (64 B per
+// point, 16x8 tiles) that sweep took about 13 ms at 256^3 x 128 (55% of
+// measured HBM) in an ncu launch list.
+static int mixed_slice_fp64(int R) { return R >= 2 ? 2 : R; }
 
 static void tile_for(int rb, int eb, int *P1, int *P2, int kind = 0) {
 	const int lg = rb * eb / 16;
@@ -1842,7 +1849,7 @@ int batched_alloc(Ctx *c) {
 	const Tuning tu = tuning_for(TuneKey{c->solver, c->precision, B->R, c->g.n1, c->g.n2, c->g.n3});
 	B->rbT = slice_for(B->R, !B->mixed, B->ks);
 	if (tu.W > 0 && tu.W <= B->R && B->R % tu.W == 0) B->rbT = tu.W;
-	B->rbD = B->mixed ? slice_for(B->R, true) : B->rbT;  // FP64 x is read through the FP64 maps
+	B->rbD = B->mixed ? mixed_slice_fp64(B->R) : B->rbT;  // FP64 x is read through the FP64 maps
 	B->tuned = tu;
 	if (tu.period > 0) B->period = tu.period;
 	B->acfg = tu.acfg >= 1 && tu.acfg <= 3 ? tu.acfg : default_form(B->ks, false);
@@ -1963,7 +1970,7 @@ size_t batched_bytes(int solver, int precision, int batch, long long n1, long lo
 	SGeo sT, sD;
 	dim3 gT, gD;
 	shape(g, R, wT, (int)ts, &sT, &gT, tu.nz);
-	shape(g, R, mixed ? slice_for(R, true) : wT, 8, &sD, &gD, tu.nz);
+	shape(g, R, mixed ? mixed_slice_fp64(R) : wT, 8, &sD, &gD, tu.nz);
 	SGeo sT1;
 	dim3 gT1;
 	shape(g, R, wT, (int)ts, &sT1, &gT1, tu.nz, 1);
@@ -2312,16 +2319,13 @@ struct Impl {
 };
 
 static void bind_impl(Batched *B) {
-	if (B->mixed) {
-		if (B->rbT == 4 && B->rbD == 4) {
-			B->setup_fn = Impl<float, 4, 4>::setup;
-			B->chunk_fn = Impl<float, 4, 4>::chunk;
-		} else if (B->rbT == 4) {
-			B->setup_fn = Impl<float, 4, 8>::setup;
-			B->chunk_fn = Impl<float, 4, 8>::chunk;
+	if (B->mixed) {  // FP64 fields in 2-lane slices (mixed_slice_fp64)
+		if (B->rbT == 4) {
+			B->setup_fn = Impl<float, 4, 2>::setup;
+			B->chunk_fn = Impl<float, 4, 2>::chunk;
 		} else {
-			B->setup_fn = Impl<float, 8, 8>::setup;
-			B->chunk_fn = Impl<float, 8, 8>::chunk;
+			B->setup_fn = Impl<float, 8, 2>::setup;
+			B->chunk_fn = Impl<float, 8, 2>::chunk;
 		}
 		return;
 	}
