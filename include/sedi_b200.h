@@ -149,9 +149,9 @@ int sedi_set_stream(sedi_ctx *ctx, void *stream);
  * A single-vector FP64 context (batch 1) times its streaming sweeps (names
  * ending in _sv), which serve grids with n1 even and at least 2^22 points;
  * SEDI_ERR_UNSUPPORTED for other grids, which use column-march kernels.
- * The mixed CG form lists three kernels: cg_a every iteration, and its
- * second sweep in two forms that alternate, cg_b on odd iterations (r only)
- * and cg_bx on even ones (the x steps of both iterations).
+ * CG lists three kernels: cg_a every iteration, and its second sweep in two
+ * forms that alternate, cg_b on odd iterations (r only) and cg_bx on even
+ * ones (the x steps of both iterations).
  */
 int sedi_time_kernels(sedi_ctx *ctx, int reps, double *ms, double *bytes, char *names, int *count);
 

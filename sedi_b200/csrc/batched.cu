@@ -79,6 +79,7 @@ struct Global {
 	int ru_all;     // the pending reliable update covers every lane (periodic)
 	double tol_in;  // in-loop stop target: tol (FP64 form), theta * tol (mixed lanes)
 	int b_iter;     // iteration of the last CG sweep A (gates the parity forms of sweep B)
+	int x_pending;  // the last CG sweep B was the odd form: its x step is still pending
 };
 
 // Arithmetic: FP64 keeps the reference's operator-by-operator rounding (no
@@ -778,6 +779,9 @@ struct OpCgB : OpBase<T> {
 	__device__ bool enabled(const Global *gl) const {
 		return XS == XS_EVERY || (gl->b_iter == gl->iter && (gl->iter & 1) == (XS == XS_R ? 1 : 0));
 	}
+	__device__ void after(Global *gl) const {
+		if (XS != XS_EVERY) gl->x_pending = XS == XS_R ? 1 : 0;
+	}
 	__device__ void begin(const Global *gl, const LaneState &ls, int lane) {
 		it = gl->iter;
 #pragma unroll
@@ -1374,6 +1378,28 @@ __global__ void __launch_bounds__(256) kb_ru_fold(long long npts, int R, int WD,
 	}
 }
 
+// FP64 CG with the deferred x step: a batch whose last iteration was odd
+// (every lane stopped in the odd form of sweep B) still owes that
+// iteration's step, x += alpha p (lanes stopped earlier have alpha 0).  The
+// step rounds as the reference's x update (Cg.hpp:169).  Runs at the end of
+// every graph chunk; kb_x_flush_done clears the flag so it applies once.
+template <class T>
+__global__ void __launch_bounds__(256) kb_x_flush(long long npts, int R, int W, T *__restrict__ x,
+                                                  const T *__restrict__ p_odd, const double *__restrict__ xa,
+                                                  const Global *gl) {
+	if (gl->active != 0 || !gl->x_pending) return;
+	const long long total = npts * R;
+	for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < total;
+	     u += (long long)gridDim.x * blockDim.x) {
+		const int j = (int)(u / ((long long)W * npts)) * W + (int)(u % W);  // lane of element u
+		x[u] = aadd(x[u], amul((T)xa[j], p_odd[u]));
+	}
+}
+
+__global__ void kb_x_flush_done(Global *gl) {
+	if (gl->active == 0) gl->x_pending = 0;
+}
+
 // ---------------------------------------------------------------------------
 // Estimator accumulation over a batch: t += x .* v, q += v .* v per point,
 // lanes in probe order (stochastic-estimator.cc:195, :198).  x and v are FP64
@@ -1534,9 +1560,9 @@ constexpr int kLaneDoubles = 19, kLaneInts = 5;  // LaneState arrays
 #ifndef SEDI_MIXED_THETA_PCG
 #define SEDI_MIXED_THETA_PCG 1.0
 #endif
-// Mixed CG defers the x step of odd iterations to the next even one (OpCgB).
-#ifndef SEDI_MIXED_DEFER_X
-#define SEDI_MIXED_DEFER_X 1
+// CG defers the x step of odd iterations to the next even one (OpCgB).
+#ifndef SEDI_DEFER_X
+#define SEDI_DEFER_X 1
 #endif
 #ifndef SEDI_MIXED_THETA_BICGSTAB
 #define SEDI_MIXED_THETA_BICGSTAB 0.1
@@ -1566,7 +1592,7 @@ struct Batched {
 	int R = 0;
 	bool mixed = false;  // FP32 Krylov fields, FP64 x_hi, reductions and reliable update
 	bool pairs = false;  // single-vector FP64 form: lanes 0/1 = even/odd i1 points of one vector
-	bool defer_x = false;  // mixed CG: x steps of odd iterations deferred to the next even one (OpCgB XS)
+	bool defer_x = false;  // CG: x steps of odd iterations deferred to the next even one (OpCgB XS)
 	int acfg = SEDI_NARROW_FORM;  // form of the narrow sweeps (see CfgFor, InPlace, default_form)
 	int ks = 0;          // solver whose sweeps run (the mixed pipelined CG runs the CG recurrence)
 	bool aliased = false;  // the Krylov fields belong to the context (single-vector form)
@@ -1680,7 +1706,7 @@ static int pick_R(int nrhs, bool mixed) {
 
 // Lanes per slice: FP32 Krylov fields 4 (16 B per point); FP64 Krylov fields
 // of CG and BiCGStab 2 (16 B per point), of pipelined CG 8 (64 B per point);
-// the FP64 x and b of the mixed form 2 (mixed_slice_fp64).  16 B per point gets the 32x32 tiles
+// the FP64 x and b of the mixed form 8 (mixed_slice_fp64).  16 B per point gets the 32x32 tiles
 // and deep stage rings of the narrow sweeps.  Measured on B200 (kernels
 // alone, 64 lanes): FP64 CG sweep A at 256^3 4.11 ms with 2 lanes against
 // 5.83 ms with 8, BiCGStab sweep 2 3.98 against 5.20 ms, sweep 3 10.79
@@ -1700,11 +1726,12 @@ static int slice_for(int R, bool fp64, int ks = 0) {
 }
 
 // FP64 fields of the mixed form (x_hi, b), streamed by the setup and
-// reliable-update residual sweep: 2-lane slices (16 B per point: 32x16
-// tiles, six stages), like the FP64 CG sweeps.  With 8-lane slices (64 B per
-// point, 16x8 tiles) that sweep took about 13 ms at 256^3 x 128 (55% of
-// measured HBM) in an ncu launch list.
-static int mixed_slice_fp64(int R) { return R >= 2 ? 2 : R; }
+// reliable-update residual sweep and the fold: 8-lane slices, so a block's
+// FP32 r (and the fold's x_lo) covers whole 4-lane vectors.  With 2-lane
+// slices (32x16 tiles instead of 16x8) the residual sweep kept its 12.8 ms
+// at 256^3 x 128 (each block wrote half of every FP32 r vector), setup took
+// 16.7 against 12.6 ms and the fold 11.1 against 9.6 ms (ncu launch lists).
+static int mixed_slice_fp64(int R) { return slice_for(R, true); }
 
 static void tile_for(int rb, int eb, int *P1, int *P2, int kind = 0) {
 	const int lg = rb * eb / 16;
@@ -1834,7 +1861,7 @@ int batched_alloc(Ctx *c) {
 	c->batched = B;
 	B->mixed = c->precision == SEDI_PREC_MIXED;
 	B->ks = kernel_solver(c->solver, B->mixed);
-	B->defer_x = SEDI_MIXED_DEFER_X && B->mixed && B->ks == SEDI_CG;
+	B->defer_x = SEDI_DEFER_X && B->ks == SEDI_CG;
 	if (c->batch > (B->mixed ? 256 : 128)) {
 		c->error = "batch too large for one context (max 256 FP32 / 128 FP64 right-hand sides)";
 		return SEDI_ERR_ARG;
@@ -2302,6 +2329,14 @@ struct Impl {
 				else if (B->ks == 1) enqueue_bicg_iteration<T, RBT, RBD, PAIRS>(c, B);
 				else enqueue_cg_iteration<T, RBT, RBD, PAIRS>(c, B);
 			}
+			if (B->defer_x && !B->mixed) {  // the mixed form folds pending steps in its reliable update
+				const long long npts = PAIRS ? c->g.n / 2 : c->g.n;
+				const long long nb = ((long long)B->elems + 255) / 256;
+				kb_x_flush<T><<<(int)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, s>>>(npts, B->R, RBT, (T *)B->x,
+				                                                                    (const T *)B->p1, B->ls.xa, B->gl);
+				kb_x_flush_done<<<1, 1, 0, s>>>(B->gl);
+				c->launches += 2;
+			}
 			BTRY(cudaStreamEndCapture(s, &graph));
 			B->graph_kernels = c->launches - before;
 			c->launches = before;
@@ -2319,13 +2354,16 @@ struct Impl {
 };
 
 static void bind_impl(Batched *B) {
-	if (B->mixed) {  // FP64 fields in 2-lane slices (mixed_slice_fp64)
-		if (B->rbT == 4) {
-			B->setup_fn = Impl<float, 4, 2>::setup;
-			B->chunk_fn = Impl<float, 4, 2>::chunk;
+	if (B->mixed) {  // FP64 fields in slices of mixed_slice_fp64 lanes
+		if (B->rbT == 4 && B->rbD == 4) {
+			B->setup_fn = Impl<float, 4, 4>::setup;
+			B->chunk_fn = Impl<float, 4, 4>::chunk;
+		} else if (B->rbT == 4) {
+			B->setup_fn = Impl<float, 4, 8>::setup;
+			B->chunk_fn = Impl<float, 4, 8>::chunk;
 		} else {
-			B->setup_fn = Impl<float, 8, 2>::setup;
-			B->chunk_fn = Impl<float, 8, 2>::chunk;
+			B->setup_fn = Impl<float, 8, 8>::setup;
+			B->chunk_fn = Impl<float, 8, 8>::chunk;
 		}
 		return;
 	}
@@ -2365,6 +2403,7 @@ int pairs_alloc(Ctx *c) {
 	if (!B) return SEDI_ERR_NOMEM;
 	B->pairs = B->aliased = true;
 	B->ks = c->solver;
+	B->defer_x = SEDI_DEFER_X && B->ks == SEDI_CG;
 	B->R = 2;
 	B->rbT = B->rbD = 2;
 	B->elems = (size_t)c->g.n;
@@ -2428,7 +2467,8 @@ int pairs_alloc(Ctx *c) {
 		         make_map(&M.m[MT_P0_HALO], B->p0, 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_P1_HALO], B->p1, 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
 		         make_map(&M.m[MT_X_INT], B->x, 8, g, 2, 2, Q1, Q2) &&
-		         make_map(&M.m[MT_R_INT], B->r, 8, g, 2, 2, Q1, Q2);
+		         make_map(&M.m[MT_R_INT], B->r, 8, g, 2, 2, Q1, Q2) &&
+		         make_map(&M.m[MT_P1_INT], B->p1, 8, g, 2, 2, Q1, Q2);
 		if (B->ks == 3)
 			k = k && make_map(&M.m[MT_W0_HALO], B->w[0], 8, g, 2, 2, Q1 + 2, Q2 + 2) &&
 			    make_map(&M.m[MT_W1_HALO], B->w[1], 8, g, 2, 2, Q1 + 2, Q2 + 2) &&

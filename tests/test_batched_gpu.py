@@ -335,18 +335,19 @@ def test_mixed_cg_deferred_x_steps_with_odd_updates(period):
 
 
 @pytest.mark.parametrize("solver,prec,nk", [("cg", S.MIXED, 3), ("pcg", S.MIXED, 3), ("bicgstab", S.MIXED, 3),
-                                            ("pcg", S.FP64, 1), ("cg", S.FP64, 2)])
+                                            ("pcg", S.FP64, 1), ("cg", S.FP64, 3)])
 def test_time_kernels_lists_solver_sweeps(solver, prec, nk):
-    """Per-iteration sweeps: CG 2 in FP64, BiCGStab 3, pipelined CG 1 in FP64.
-    The mixed CG (and the mixed pipelined CG, which runs the CG recurrence)
-    lists sweep A and the two parity forms of sweep B: cg_b on odd
-    iterations (r only, 3 words) and cg_bx on even ones (both x steps, 6)."""
+    """Per-iteration sweeps: BiCGStab 3, pipelined CG 1 in FP64.  CG (and the
+    mixed pipelined CG, which runs the CG recurrence) lists sweep A and the
+    two parity forms of sweep B: cg_b on odd iterations (r only, 3 words)
+    and cg_bx on even ones (both x steps, 6)."""
     with S.Context(solver, (64, 64, 64), precision=prec, batch=16) as c:
         ks = c.time_kernels(reps=2)
     assert len(ks) == nk and all(ms > 0 and by > 0 for _, ms, by in ks)
-    if prec == S.MIXED and solver != "bicgstab":
+    if solver == "cg" or (prec == S.MIXED and solver == "pcg"):
+        t = "fp32" if prec == S.MIXED else "fp64"
         names = [k[0] for k in ks]
-        assert names == ["cg_a_fp32", "cg_b_fp32", "cg_bx_fp32"], names
+        assert names == [f"cg_a_{t}", f"cg_b_{t}", f"cg_bx_{t}"], names
         assert ks[2][2] == 2 * ks[1][2] == 2 * ks[0][2]
 
 
