@@ -752,13 +752,16 @@ using OpCgAv = InPlace<OpCgA<T>, K>;
 // ---------------------------------------------------------------------------
 // CG kernel B: s = A p, x += alpha p, r -= alpha s, u = r .* iM, <r,u>, <r,r>;
 // beta, err, stop test (Cg.hpp:169-193).
-// XS (mixed form only) defers x: XS_R runs on odd iterations and updates r
-// alone, leaving its x step (alpha in xa) to XS_X on the next even
-// iteration, which applies both, x = (x + xa p_old) + alpha p, with p_old
-// the previous iteration's direction (still in the other p buffer).  Two
-// iterations move 3 + 6 instead of 5 + 5 words per point and lane; r, the
-// scalars and every iteration count are those of the undeferred sweep, and
-// a reliable update after an odd iteration folds the pending step.
+// XS defers x (no sweep reads x during the solve): XS_R runs on odd
+// iterations and updates r alone, leaving its x step (alpha in xa) to XS_X
+// on the next even iteration, which applies both in order,
+// x = (x + xa p_old) + alpha p, with p_old the previous iteration's
+// direction (still in the other p buffer).  In FP64 that rounds exactly as
+// two reference updates (Cg.hpp:169).  Two iterations move 3 + 6 instead of
+// 5 + 5 words per point and lane; r, the scalars and every iteration count
+// are those of the undeferred sweep.  A pending step after an odd iteration
+// is folded by the mixed form's reliable update (kb_ru_fold) and applied by
+// kb_x_flush when an FP64 batch ends there.
 // ---------------------------------------------------------------------------
 enum { XS_EVERY = 0, XS_R = 1, XS_X = 2 };
 template <class T, int XS = XS_EVERY>
