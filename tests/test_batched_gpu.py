@@ -41,16 +41,19 @@ def test_fp64_batch_matches_single_vector(nrhs):
         assert abs(fe[k] - fe0) <= 1e-10 * fe0 + 1e-15
 
 
-def test_fp64_batch_fixed_iterations():
+@pytest.mark.parametrize("K", [200, 31])
+def test_fp64_batch_fixed_iterations(K):
+    """K odd: the batch ends on an odd iteration, whose deferred x step is
+    applied after the last sweep (kb_x_flush)."""
     dims = (24, 20, 16)
     n = int(np.prod(dims))
     B = np.stack([O.fill_probe(99 + k, n) for k in range(5)])
     X = np.zeros_like(B)
     with S.Context("cg", dims, batch=8) as c:
-        res, fe, fi = c.solve_batch(X, B, maxiter=200, tol=0.0)
+        res, fe, fi = c.solve_batch(X, B, maxiter=K, tol=0.0)
     for k in range(5):
-        rc0, fe0, fi0, x0, _ = O.solve(2, dims, B[k], maxiter=200, tol=0.0)
-        assert (res[k], fi[k]) == (rc0, fi0) == (1, 200)
+        rc0, fe0, fi0, x0, _ = O.solve(2, dims, B[k], maxiter=K, tol=0.0)
+        assert (res[k], fi[k]) == (rc0, fi0) == (1, K)
         assert O.relmax(X[k], x0) <= 1e-10
 
 
