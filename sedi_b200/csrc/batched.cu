@@ -52,7 +52,7 @@ struct LaneState {
 	double *bb, *rr, *err, *ru, *ru_new, *sp, *alpha, *beta;  // CG
 	double *gamma, *gamma_old, *delta, *rr_top;                 // pipelined CG
 	double *rho, *rho_prev, *omega, *s_norm2, *ts, *tt;         // BiCGStab
-	double *xa;  // mixed CG: alpha of the x step an odd iteration leaves to the next even one
+	double *xa;  // CG: alpha of the x step an odd iteration leaves to the next even one
 	int *done, *exit_iter, *reason, *pending, *s_exit;
 	double *hist;  // single-vector form: err after each iteration (lane 0), else null
 };
