@@ -355,8 +355,9 @@ int sedi_server_stats(const sedi_server *srv, double *peak_bytes, double *budget
  * choice[0..5] = slice width, i3 chunks (0: the built-in model), period,
  * iterations per graph, L2 prefetch distance in planes (-1: the built-in
  * distance), narrow-sweep form; *score_ms (optional)
- * = the winning estimate time (flags & 1) or summed per-iteration sweep
- * time.  Needs device memory for one such context at a time.
+ * = the winning estimate time (flags & 1) or the sweep time of one
+ * iteration (CG's two parity forms of sweep B count half each).  Needs
+ * device memory for one such context at a time.
  */
 int sedi_autotune(int solver, int precision, int batch, long n1, long n2, long n3, int maxiter, double tol,
                   uint32_t seed, int flags, int *choice, double *score_ms);

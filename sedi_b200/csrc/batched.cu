@@ -3050,7 +3050,8 @@ namespace sedi {
 // Autotuner.  For one (solver, precision, lanes, grid):
 //   1. lane-slice width W of the Krylov fields (FP32: 8 or 4 lanes; FP64: 8,
 //      4 or 2), each on a scratch context with the model's i3 split, scored
-//      by the summed per-iteration sweep time (CUDA events, kernels alone);
+//      by the sweep time of one iteration (CUDA events, kernels alone; CG's
+//      two parity forms of sweep B count half each);
 //   2. the i3 split of the sweeps (the model's choice and 1, 2, 3, 4, 6, 8
 //      chunks) with the best W, same score;
 //   3. with flags & 1: iterations per captured graph (8, 16, 32) and, for the
@@ -3069,8 +3070,13 @@ static int tune_sweep_ms(sedi_ctx *h, double *ms_sum) {
 	const int rc = c->batched ? batched_time_kernels(c, 5, ms, by, names, &cnt)
 	                          : (c->pairs ? pairs_time_kernels(c, 10, ms, by, names, &cnt) : SEDI_ERR_UNSUPPORTED);
 	if (rc) return rc;
+	// Time per iteration: the two parity forms of CG sweep B (cg_b, cg_bx)
+	// each run every other iteration.
+	bool deferred = false;
+	for (int k = 0; k < cnt; k++) deferred = deferred || strncmp(names + 32 * k, "cg_bx", 5) == 0;
 	*ms_sum = 0.0;
-	for (int k = 0; k < cnt; k++) *ms_sum += ms[k];
+	for (int k = 0; k < cnt; k++)
+		*ms_sum += (deferred && strncmp(names + 32 * k, "cg_b", 4) == 0) ? 0.5 * ms[k] : ms[k];
 	return 0;
 }
 
